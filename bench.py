@@ -1,0 +1,321 @@
+"""Benchmark of the integral hot path on B200.
+
+Workload (the metric's configuration): ERIDA classes of a "32^3" grid at
+spacing 0.5 bohr -- the reference's symmetry-reduced path needs the odd
+rotationally symmetric grid, so the 33^3 grid (-16, 33)^3 with its 6,545
+symmetry-reduced classes stands in for it; G10 gausslet coefficients, tol
+1e-16, values scaled by 1/spacing = 2 to Hartree.  Synthetic: the inputs are
+the coefficients and the grid.
+
+One step = one evaluation of every class value from the class list already
+resident in HBM (tables, staged contraction, write-back), i.e. one
+gli_b200_sparse_values_dev call.  The class enumeration is measured apart.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|mixed] [--impl ours|reference]
+
+Timing: W >= 3 untimed warm-up steps; each timed step is bracketed by CUDA
+events on the stream the library launches on; L2 (126 MB) is flushed by
+writing a 256 MB buffer between timed steps (outside the events); the K steps
+are bracketed by a barrier and device synchronisation, and the slowest rank's
+time counts.  N > 1 (torchrun, one process per GPU): every rank evaluates its
+own copy of the workload (weak scaling, no data-path collective).
+
+--impl reference times the reference's own CPU implementation (the reference C
+core compiled under oracle/_ref, OpenMP on all host cores) on the same
+workload and prints the same JSON line with "impl": "reference".
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "ERI classes/sec on 1 B200, mixed vs FP64 form at <=1e-8 Ha max abs err"
+L_GRID = 33          # odd symmetric stand-in for 32^3
+SPACING = 0.5        # bohr
+TOL = 1e-16
+WORKLOAD = "ERIDA 32^3 grid (odd stand-in 33^3, 6545 classes), spacing 0.5 bohr, G10, tol 1e-16"
+
+
+def g10():
+    return np.load(os.path.join(REPO, "tests", "golden", "reference_fixtures.npz"))["g10"]
+
+
+def grid_spec():
+    return [(-(L_GRID // 2), L_GRID)] * 3
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, device):
+        self.path = tempfile.mktemp(suffix=".csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(b, spec, idx, tol, min_seconds=8.0):
+    """Reference C core (oracle/_ref) on all host cores over the full class list,
+    repeated until about min_seconds of CPU work; returns (classes/s, sample)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from ref_binding import RefLib
+    r = RefLib()
+    reps, t0 = 0, time.perf_counter()
+    vals = None
+    while True:
+        vals = r.sparse_values("erida", b, spec, idx, tol)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= 50:
+            break
+    return reps * idx.size / el, f"full {idx.size}-class list x {reps} passes ({el:.1f} s)", vals
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from ref_binding import RefLib
+    r = RefLib()
+    b = g10()
+    spec = grid_spec()
+    idx = r.enumerate("erida", spec)
+    for _ in range(min(args.warmup, 1)):
+        r.sparse_values("erida", b, spec, idx, TOL)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r.sparse_values("erida", b, spec, idx, TOL)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = args.steps * idx.size / tot
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "classes/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "classes": int(idx.size), "form": "fp64 (reference C core)"},
+            "cpu_baseline": {"value": value, "unit": "classes/s", "cores": cores, "kind": "reference",
+                             "sample": f"full {idx.size}-class list per step, {args.steps} steps"},
+            "e2e": {"value": value, "unit": "classes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import gausslectronitegrate_b200 as gli
+    from gausslectronitegrate_b200 import _abi
+    L = gli.lib()
+    L.gli_b200_set_device(local)
+    form = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}[args.form]
+    b = np.ascontiguousarray(g10())
+    spec = grid_spec()
+    gs = gli._grid_struct(spec)
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    # class list on the device (enumeration timed apart)
+    d_idx = C.c_void_p()
+    num = _abi.glong()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        rc = L.gli_b200_enumerate_dev(0, C.byref(gs), C.byref(d_idx), C.byref(num), sptr)
+        e1.record(stream)
+    if rc:
+        raise RuntimeError(L.gli_b200_last_error_message().decode())
+    stream.synchronize()
+    enum_ms = e0.elapsed_time(e1)
+    m = num.value
+    out = torch.empty(m, dtype=torch.float64, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    coeff_p = b.ctypes.data_as(_abi.dptr)
+
+    def step(f):
+        rc = L.gli_b200_sparse_values_dev(0, coeff_p, b.size, C.byref(gs), d_idx, m, TOL, f,
+                                          C.c_void_p(out.data_ptr()), sptr)
+        if rc:
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+
+    # accuracy of the chosen form against the FP64 form (max abs error in Ha)
+    step(_abi.GLI_FORM_FP64)
+    stream.synchronize()
+    ref64 = out.cpu().numpy().copy()
+    step(form)
+    stream.synchronize()
+    got = out.cpu().numpy().copy()
+    scale = 1.0 / SPACING
+    max_abs_err_ha = float(np.max(np.abs(got - ref64)) * scale)
+
+    for _ in range(max(args.warmup, 3)):
+        step(form)
+    stream.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            starts[k].record(stream)
+        step(form)
+        with torch.cuda.stream(stream):
+            ends[k].record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    my_ms = sum(step_ms)
+    t = torch.tensor([my_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    total_ms = float(t.item())
+    value = ws * m * args.steps / (total_ms * 1e-3)
+
+    # per-stage device times of one step (library events on the same stream)
+    L.gli_b200_set_timing(1)
+    step(form)
+    stream.synchronize()
+    ms4 = (C.c_float * 4)()
+    sz3 = (_abi.glong * 3)()
+    L.gli_b200_last_stage_times(ms4, sz3)
+    L.gli_b200_set_timing(0)
+    nA, nP, U = int(sz3[0]), int(sz3[1]), int(sz3[2])
+    flops_a = 2.0 * nA * U * U * U
+    peak = C.c_double()
+    L.gli_b200_measure_fp64_peak(C.byref(peak))
+
+    # e2e: the reference-facing C call with host buffers (copies inside); the
+    # host class list comes from the reference-facing enumeration call
+    idx_s = _abi.SparseIndices()
+    L.enumerate_symmetry_reduced_erida_indices(C.byref(gs), C.byref(idx_s))
+    idx_np = np.ctypeslib.as_array(idx_s.indices, shape=(idx_s.num,)).copy()
+    L.delete_sparse_erida_indices(C.byref(idx_s))
+    gd, keep = gli._parse_coeffs(b, "")
+    e2e_times = []
+    for k in range(max(3, args.steps)):
+        res = _abi.SparseIntegrals()
+        t0 = time.perf_counter()
+        L.compute_sparse_erida_gausslet_integrals(C.byref(gd), C.byref(gs), idx_np.ctypes.data_as(_abi.lptr), m, TOL,
+                                                  C.byref(res))
+        vals = np.ctypeslib.as_array(res.integral_values, shape=(m,)).copy()
+        e2e_times.append(time.perf_counter() - t0)
+        L.delete_sparse_erida_gausslet_integrals(C.byref(res))
+    e2e_s = statistics.median(e2e_times[1:]) if len(e2e_times) > 1 else e2e_times[0]
+
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        L.gli_b200_free_dev(d_idx, sptr)
+        return 0
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            rate, sample, ref_vals = cpu_reference_rate(b, spec, idx_np, TOL)
+            cpu = {"value": rate, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": sample, "max_abs_err_ha_vs_gpu_fp64": float(np.max(np.abs(ref_vals - ref64)) * scale)}
+        except Exception as ex:  # the reference core must be prebuilt (make -C oracle ref)
+            cpu = {"value": None, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+    ms_a = float(ms4[1])
+    achieved = flops_a / (ms_a * 1e-3) / 1e12 if ms_a > 0 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "classes": m, "form": args.form, "tol": TOL, "spacing_bohr": SPACING,
+                   "l2": "flushed between timed steps (256 MB write)", "max_abs_err_ha_vs_fp64": max_abs_err_ha,
+                   "enumeration_ms": enum_ms, "stage_ms": {"tables": float(ms4[0]), "A": ms_a, "B": float(ms4[2]),
+                                                          "C": float(ms4[3])},
+                   "stage_sizes": {"keys_A": nA, "key_pairs": nP, "lattice_U": U},
+                   "wall_s_timed_region": wall},
+        "roofline": {"bound": "fp64", "kernel": "k_stage_a", "achieved": achieved, "peak": peak.value,
+                     "unit": "TFLOP/s", "frac": (achieved / peak.value) if (achieved and peak.value) else None,
+                     "peak_source": "measured FP64 FMA probe on this device (gli_b200_measure_fp64_peak)",
+                     "algorithmic_flops_per_launch": flops_a, "traffic": None},
+        "e2e": {"value": m / e2e_s, "unit": "classes/s", "h2d_bytes_per_step": 8 * m + 8 * b.size,
+                "d2h_bytes_per_step": 8 * m},
+        "gpu_launches": None,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    L.gli_b200_free_dev(d_idx, sptr)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,128 @@
+"""ctypes view of libgli_b200's C ABI (include/gli_b200.h).
+
+The struct layouts are those of the reference headers (include/range.h,
+grid.h, gausslet.h, nuclear_integrals.h, kinetic_integrals.h,
+eri_integrals.h, erida_integrals.h), which libgli_b200 keeps unchanged.
+Loading fails loudly when the shared library has not been built.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgli_b200.so")
+
+glong = C.c_int64
+dptr = C.POINTER(C.c_double)
+lptr = C.POINTER(glong)
+
+GLI_FORM_FP64 = 0
+GLI_FORM_MIXED = 1
+GLI_KIND_ERIDA = 0
+GLI_KIND_ERI = 1
+
+
+class Range(C.Structure):
+    _fields_ = [("istart", glong), ("num", glong)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("coord_range", Range * 3)]
+
+
+class Point(C.Structure):
+    _fields_ = [("c", glong * 3)]
+
+
+class GaussletData(C.Structure):
+    _fields_ = [("coefficients", dptr), ("indices", Range)]
+
+
+class Nucleus(C.Structure):
+    _fields_ = [("pos", C.c_double * 3), ("charge", C.c_int)]
+
+
+class Kinetic(C.Structure):
+    _fields_ = [("integral_values", dptr), ("grid", Grid)]
+
+
+class Nuclear(C.Structure):
+    _fields_ = [("integral_values", dptr), ("grid", Grid), ("nuclei", C.POINTER(Nucleus)), ("num_nuclei", C.c_int)]
+
+
+class SparseIndices(C.Structure):
+    """struct sparse_eri_indices / sparse_erida_indices (same layout)."""
+    _fields_ = [("indices", lptr), ("num", glong), ("grid", Grid)]
+
+
+class SparseIntegrals(C.Structure):
+    """struct sparse_eri_gausslet_integrals / sparse_erida_gausslet_integrals."""
+    _fields_ = [("integral_values", dptr), ("indices", lptr), ("num_entries", glong), ("grid", Grid)]
+
+
+EXPORTS = [
+    # reference API (include/{kinetic,nuclear,eri,erida}_integrals.h, symmetry.h)
+    "compute_kinetic_gausslet_integral", "compute_kinetic_gausslet_integrals", "delete_kinetic_gausslet_integrals",
+    "compute_nuclear_gausslet_integral", "compute_nuclear_gausslet_integrals", "delete_nuclear_gausslet_integrals",
+    "compute_eri_gausslet_integral", "minimum_octahedral_orbit_eri_tensor_index",
+    "enumerate_symmetry_reduced_eri_indices", "delete_sparse_eri_indices", "compute_sparse_eri_gausslet_integrals",
+    "sparse_eri_gausslet_integrals_get_value", "project_sparse_eri_gausslet_integrals", "fill_dense_eri_tensor",
+    "apply_sparse_eri_tensor", "delete_sparse_eri_gausslet_integrals",
+    "compute_erida_gausslet_integral", "minimum_octahedral_orbit_erida_tensor_index",
+    "enumerate_symmetry_reduced_erida_indices", "delete_sparse_erida_indices",
+    "compute_sparse_erida_gausslet_integrals", "sparse_erida_gausslet_integrals_get_value",
+    "project_sparse_erida_gausslet_integrals", "fill_dense_erida_matrix", "delete_sparse_erida_gausslet_integrals",
+    "evaluate_octahedral_grid_permutations",
+    # extensions
+    "gli_b200_last_error", "gli_b200_last_error_message", "gli_b200_device_count", "gli_b200_set_device",
+    "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
+    "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_measure_fp64_peak",
+]
+
+
+def load(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(f"libgli_b200.so not built ({path}); run python -m gausslectronitegrate_b200.build")
+    L = C.CDLL(path)
+    P = C.POINTER
+    L.compute_kinetic_gausslet_integral.argtypes = [P(GaussletData), P(Point)]
+    L.compute_kinetic_gausslet_integral.restype = C.c_double
+    L.compute_kinetic_gausslet_integrals.argtypes = [P(GaussletData), P(Grid), P(Kinetic)]
+    L.delete_kinetic_gausslet_integrals.argtypes = [P(Kinetic)]
+    L.compute_nuclear_gausslet_integral.argtypes = [P(GaussletData), P(Point), P(Nucleus), C.c_int, C.c_double]
+    L.compute_nuclear_gausslet_integral.restype = C.c_double
+    L.compute_nuclear_gausslet_integrals.argtypes = [P(GaussletData), P(Grid), P(Nucleus), C.c_int, C.c_double,
+                                                     P(Nuclear)]
+    L.delete_nuclear_gausslet_integrals.argtypes = [P(Nuclear)]
+    for kind in ("eri", "erida"):
+        getattr(L, f"compute_{kind}_gausslet_integral").argtypes = [P(GaussletData), P(Point), C.c_double]
+        getattr(L, f"compute_{kind}_gausslet_integral").restype = C.c_double
+        getattr(L, f"enumerate_symmetry_reduced_{kind}_indices").argtypes = [P(Grid), P(SparseIndices)]
+        getattr(L, f"delete_sparse_{kind}_indices").argtypes = [P(SparseIndices)]
+        getattr(L, f"compute_sparse_{kind}_gausslet_integrals").argtypes = [
+            P(GaussletData), P(Grid), lptr, glong, C.c_double, P(SparseIntegrals)]
+        getattr(L, f"sparse_{kind}_gausslet_integrals_get_value").argtypes = [P(SparseIntegrals), glong]
+        getattr(L, f"sparse_{kind}_gausslet_integrals_get_value").restype = C.c_double
+        getattr(L, f"project_sparse_{kind}_gausslet_integrals").argtypes = [P(SparseIntegrals), dptr, glong, dptr]
+        getattr(L, f"delete_sparse_{kind}_gausslet_integrals").argtypes = [P(SparseIntegrals)]
+    L.minimum_octahedral_orbit_eri_tensor_index.argtypes = [glong, P(lptr), glong, glong, glong, glong]
+    L.minimum_octahedral_orbit_eri_tensor_index.restype = glong
+    L.minimum_octahedral_orbit_erida_tensor_index.argtypes = [glong, P(lptr), glong, glong]
+    L.minimum_octahedral_orbit_erida_tensor_index.restype = glong
+    L.fill_dense_eri_tensor.argtypes = [P(SparseIntegrals), P(Grid), dptr]
+    L.fill_dense_erida_matrix.argtypes = [P(SparseIntegrals), P(Grid), dptr]
+    L.apply_sparse_eri_tensor.argtypes = [P(SparseIntegrals), dptr, glong, dptr]
+    L.evaluate_octahedral_grid_permutations.argtypes = [P(Grid), P(lptr)]
+    L.gli_b200_last_error.restype = C.c_int
+    L.gli_b200_last_error_message.restype = C.c_char_p
+    L.gli_b200_device_count.restype = C.c_int
+    L.gli_b200_set_device.argtypes = [C.c_int]
+    L.gli_b200_version.restype = C.c_char_p
+    L.gli_b200_sparse_values_dev.argtypes = [C.c_int, dptr, glong, P(Grid), C.c_void_p, glong, C.c_double, C.c_int,
+                                             C.c_void_p, C.c_void_p]
+    L.gli_b200_sparse_values.argtypes = [C.c_int, P(GaussletData), P(Grid), lptr, glong, C.c_double, C.c_int, dptr]
+    L.gli_b200_enumerate_dev.argtypes = [C.c_int, P(Grid), P(C.c_void_p), P(glong), C.c_void_p]
+    L.gli_b200_free_dev.argtypes = [C.c_void_p, C.c_void_p]
+    L.gli_b200_set_timing.argtypes = [C.c_int]
+    L.gli_b200_last_stage_times.argtypes = [P(C.c_float), P(glong)]
+    L.gli_b200_measure_fp64_peak.argtypes = [P(C.c_double)]
+    return L

@@ -1,0 +1,37 @@
+// Device-built lookup tables shared by the integral kernels.
+#pragma once
+#include "gli_internal.cuh"
+
+namespace gli {
+
+// Lattice description of a sparse ERI/ERIDA evaluation.  Every class value is
+//   sum_{u,v,t >= 0} W[kx][u] W[ky][v] W[kz][t] T[u^2 + v^2 + t^2]
+// where W[k] is the folded (|position|-indexed) product weight of per-axis key k
+// and T the Coulomb table on the integer lattice.
+struct LatticeTables {
+    int kind = 0;            // 0 = ERIDA, 1 = ERI
+    i64 L = 0;               // largest axis length of the grid (table sizing as in the reference)
+    i64 nkeys = 0;           // size of the dense per-axis key space
+    i64 U = 0;               // folded lattice extent: positions 0 .. U-1
+    i64 Up = 0;              // U rounded up to a multiple of 4 (row pitch of W)
+    i64 tlen = 0;            // T entries: 3 (U-1)^2 + 1
+    DevBuf<double> W;        // nkeys x Up
+    DevBuf<double> T;        // tlen
+};
+
+// Builds P (ERIDA) or the shift-pair products (ERI) from the coefficients, masks
+// entries with |P| <= tol exactly as the reference's trimming and skipping do,
+// folds them into W and evaluates T.  Synchronises once to learn U.
+void build_lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol,
+                          LatticeTables& t, cudaStream_t s);
+
+// dense ERI key of one axis: shift pair (|s01|, |s23|) unordered and |c|/3
+__host__ __device__ inline i64 eri_axis_key(i64 s01, i64 s23, i64 cc, i64 L) {
+    i64 a = s01 < 0 ? -s01 : s01;
+    i64 b = s23 < 0 ? -s23 : s23;
+    if (a > b) { i64 t = a; a = b; b = t; }
+    const i64 c = cc < 0 ? -cc : cc;
+    return (b * (b + 1) / 2 + a) * (2 * L - 1) + c;
+}
+
+}  // namespace gli

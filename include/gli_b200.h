@@ -1,0 +1,300 @@
+/*
+ * gli_b200.h -- C ABI of libgli_b200, a B200 (sm_100a) implementation of the
+ * gausslectronitegrate integral hot path.
+ *
+ * Part 1 declares the reference's own C interface with identical prototypes
+ * and struct layouts, so that code written against the reference headers
+ * (include/{eri,erida,nuclear,kinetic}_integrals.h, grid.h, range.h,
+ * gausslet.h, symmetry.h, aligned_memory.h of the reference) links against
+ * this library unchanged; the compatibility headers next to this file carry
+ * the reference's header names and include this one.  Every bulk computation
+ * runs in CUDA kernels on the GPU; there is no CPU fallback.  Results handed
+ * back inside the reference structs are host memory from aligned_malloc(),
+ * released by the matching delete_* call, exactly as in the reference.
+ *
+ * Part 2 declares extensions: error status, device-resident entry points
+ * (class lists and values kept in HBM) and the precision form switch.
+ *
+ * Errors: the reference API returns void.  On failure (no CUDA device, a
+ * CUDA error, an argument the reference would silently mis-handle such as a
+ * non-symmetric grid for the symmetry-reduced paths) the call prints one line
+ * to stderr, leaves the result empty (NULL arrays, zero counts) and records a
+ * status readable with gli_b200_last_error() / gli_b200_last_error_message().
+ */
+#ifndef GLI_B200_H
+#define GLI_B200_H
+
+#include <assert.h>
+#include <math.h>
+#include <stdbool.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Part 1: types of the reference interface (same layout, own code)
+ * ---------------------------------------------------------------------- */
+
+/* universal integer, reference include/util.h:10 */
+typedef int64_t glong;
+#ifndef GLONG_MAX
+#define GLONG_MAX INT64_MAX
+#endif
+
+/* reference include/range.h:10-14 */
+struct range {
+	glong istart;  /* first integer */
+	glong num;     /* number of integers */
+};
+
+/* reference include/grid.h:10-17 */
+union cartesian_grid_point_3d {
+	struct {
+		glong x, y, z;
+	};
+	glong c[3];
+};
+
+/* reference include/grid.h:23-26 */
+struct cartesian_grid_3d {
+	struct range coord_range[3];  /* x, y, z axes: first coordinate and count */
+};
+
+/* reference include/gausslet.h:10-14 */
+struct gausslet_data {
+	double* coefficients;  /* coefficients b_j of the elementary Gaussians */
+	struct range indices;  /* j range, istart = -(num-1)/2 for the odd sets used */
+};
+
+/* reference include/nuclear_integrals.h:11-15 */
+struct atomic_nucleus {
+	double pos[3];  /* position in grid units */
+	int charge;
+};
+
+/* reference include/kinetic_integrals.h:14-18 */
+struct kinetic_gausslet_integrals {
+	double* integral_values;  /* dense N x N, row-major */
+	struct cartesian_grid_3d grid;
+};
+
+/* reference include/nuclear_integrals.h:31-37 */
+struct nuclear_gausslet_integrals {
+	double* integral_values;  /* dense N x N, row-major */
+	struct cartesian_grid_3d grid;
+	struct atomic_nucleus* nuclei;
+	int num_nuclei;
+};
+
+/* reference include/eri_integrals.h:23-28 */
+struct sparse_eri_indices {
+	glong* four_indices;  /* ((i N + j) N + k) N + l, sorted ascending */
+	glong num;
+	struct cartesian_grid_3d grid;
+};
+
+/* reference include/eri_integrals.h:41-47 */
+struct sparse_eri_gausslet_integrals {
+	double* integral_values;
+	glong* four_indices;
+	glong num_entries;
+	struct cartesian_grid_3d grid;
+};
+
+/* reference include/erida_integrals.h:21-26 */
+struct sparse_erida_indices {
+	glong* two_indices;  /* i N + j, sorted ascending */
+	glong num;
+	struct cartesian_grid_3d grid;
+};
+
+/* reference include/erida_integrals.h:39-45 */
+struct sparse_erida_gausslet_integrals {
+	double* integral_values;
+	glong* two_indices;
+	glong num_entries;
+	struct cartesian_grid_3d grid;
+};
+
+/* ------------------------------------------------------------------------
+ * Inline helpers the reference exposes from its headers (same behaviour).
+ * ---------------------------------------------------------------------- */
+
+/* reference include/util.h:43-62 */
+static inline glong lmin(const glong a, const glong b) { return a <= b ? a : b; }
+static inline glong lmax(const glong a, const glong b) { return a >= b ? a : b; }
+static inline double square(const double x) { return x * x; }
+static inline glong lsquare(const glong x) { return x * x; }
+
+/* 64-byte aligned host allocations, reference include/aligned_memory.h:14-50 */
+#define MEM_DATA_ALIGN 64
+static inline void* aligned_malloc(size_t size)
+{
+	return aligned_alloc(MEM_DATA_ALIGN, (size + MEM_DATA_ALIGN - 1) & ~((size_t)MEM_DATA_ALIGN - 1));
+}
+static inline void* aligned_calloc(size_t size)
+{
+	void* p = aligned_malloc(size);
+	if (p != NULL) memset(p, 0, size);
+	return p;
+}
+static inline void aligned_free(void* p) { free(p); }
+
+/* x-major linear indexing, reference include/grid.h:33-82 */
+static inline glong cartesian_grid_3d_num_points(const struct cartesian_grid_3d* grid)
+{
+	return grid->coord_range[0].num * grid->coord_range[1].num * grid->coord_range[2].num;
+}
+static inline glong cartesian_grid_3d_cartesian_to_linear_index(const struct cartesian_grid_3d* grid,
+	const glong ix, const glong iy, const glong iz)
+{
+	assert(0 <= ix && ix < grid->coord_range[0].num);
+	assert(0 <= iy && iy < grid->coord_range[1].num);
+	assert(0 <= iz && iz < grid->coord_range[2].num);
+	return (ix * grid->coord_range[1].num + iy) * grid->coord_range[2].num + iz;
+}
+static inline glong cartesian_grid_point_3d_to_linear_index(const struct cartesian_grid_3d* grid,
+	const union cartesian_grid_point_3d* pt)
+{
+	return cartesian_grid_3d_cartesian_to_linear_index(grid,
+		pt->x - grid->coord_range[0].istart,
+		pt->y - grid->coord_range[1].istart,
+		pt->z - grid->coord_range[2].istart);
+}
+static inline void linear_index_to_cartesian_grid_point_3d(const struct cartesian_grid_3d* grid,
+	const glong idx, union cartesian_grid_point_3d* pt)
+{
+	const glong nz = grid->coord_range[2].num, ny = grid->coord_range[1].num;
+	pt->z = grid->coord_range[2].istart + idx % nz;
+	pt->y = grid->coord_range[1].istart + (idx / nz) % ny;
+	pt->x = grid->coord_range[0].istart + idx / (nz * ny);
+}
+
+/* ------------------------------------------------------------------------
+ * Part 1: functions of the reference interface
+ * ---------------------------------------------------------------------- */
+
+/* kinetic: reference include/kinetic_integrals.h:7, :21, :24 */
+double compute_kinetic_gausslet_integral(const struct gausslet_data* gdata, const union cartesian_grid_point_3d points[2]);
+void compute_kinetic_gausslet_integrals(const struct gausslet_data* gdata, const struct cartesian_grid_3d* grid, struct kinetic_gausslet_integrals* kgi);
+void delete_kinetic_gausslet_integrals(struct kinetic_gausslet_integrals* kgi);
+
+/* nuclear: reference include/nuclear_integrals.h:22-24, :40-43, :46 */
+double compute_nuclear_gausslet_integral(
+	const struct gausslet_data* gdata, const union cartesian_grid_point_3d points[2],
+	const struct atomic_nucleus* nuclei, const int num_nuclei, const double tol);
+void compute_nuclear_gausslet_integrals(
+	const struct gausslet_data* gdata, const struct cartesian_grid_3d* grid,
+	const struct atomic_nucleus* nuclei, const int num_nuclei,
+	const double tol, struct nuclear_gausslet_integrals* ngi);
+void delete_nuclear_gausslet_integrals(struct nuclear_gausslet_integrals* ngi);
+
+/* ERI: reference include/eri_integrals.h:7, :14-16, :31, :34, :50-52, :55, :57, :59, :61, :64 */
+double compute_eri_gausslet_integral(const struct gausslet_data* gdata, const union cartesian_grid_point_3d points[4], const double tol);
+glong minimum_octahedral_orbit_eri_tensor_index(
+	const glong num_points, const glong* octahedral_perm[48],
+	const glong i, const glong j, const glong k, const glong l);
+void enumerate_symmetry_reduced_eri_indices(const struct cartesian_grid_3d* grid, struct sparse_eri_indices* ret);
+void delete_sparse_eri_indices(struct sparse_eri_indices* indices);
+void compute_sparse_eri_gausslet_integrals(const struct gausslet_data* gdata,
+	const struct cartesian_grid_3d* grid, const glong* four_indices, const glong num_indices,
+	const double tol, struct sparse_eri_gausslet_integrals* eri);
+double sparse_eri_gausslet_integrals_get_value(const struct sparse_eri_gausslet_integrals* eri, const glong index);
+void project_sparse_eri_gausslet_integrals(const struct sparse_eri_gausslet_integrals* eri, const double* basis, const glong num_states, double* eri_proj);
+void fill_dense_eri_tensor(const struct sparse_eri_gausslet_integrals* eri_sparse, const struct cartesian_grid_3d* grid_dense, double* eri_tensor);
+void apply_sparse_eri_tensor(const struct sparse_eri_gausslet_integrals* eri, const double* states, const glong num_states, double* ret);
+void delete_sparse_eri_gausslet_integrals(struct sparse_eri_gausslet_integrals* eri);
+
+/* ERIDA: reference include/erida_integrals.h:7, :14, :29, :32, :48-50, :53, :55, :57, :60 */
+double compute_erida_gausslet_integral(const struct gausslet_data* gdata, const union cartesian_grid_point_3d points[2], const double tol);
+glong minimum_octahedral_orbit_erida_tensor_index(const glong num_points, const glong* octahedral_perm[48], const glong i, const glong j);
+void enumerate_symmetry_reduced_erida_indices(const struct cartesian_grid_3d* grid, struct sparse_erida_indices* ret);
+void delete_sparse_erida_indices(struct sparse_erida_indices* indices);
+void compute_sparse_erida_gausslet_integrals(const struct gausslet_data* gdata,
+	const struct cartesian_grid_3d* grid, const glong* two_indices, const glong num_indices,
+	const double tol, struct sparse_erida_gausslet_integrals* erida);
+double sparse_erida_gausslet_integrals_get_value(const struct sparse_erida_gausslet_integrals* erida, const glong index);
+void project_sparse_erida_gausslet_integrals(const struct sparse_erida_gausslet_integrals* erida, const double* basis, const glong num_states, double* eri_proj);
+void fill_dense_erida_matrix(const struct sparse_erida_gausslet_integrals* erida_sparse, const struct cartesian_grid_3d* grid_dense, double* erida_matrix);
+void delete_sparse_erida_gausslet_integrals(struct sparse_erida_gausslet_integrals* erida);
+
+/* O_h grid permutations: reference include/symmetry.h:24.  perm[g] receives a
+ * 48-way table of aligned_malloc'ed arrays (caller frees each with aligned_free);
+ * the grid must be rotationally symmetric. */
+void evaluate_octahedral_grid_permutations(const struct cartesian_grid_3d* grid, glong* perm[48]);
+
+/* ------------------------------------------------------------------------
+ * Part 2: extensions (no reference counterpart unless noted)
+ * ---------------------------------------------------------------------- */
+
+enum gli_b200_status {
+	GLI_OK = 0,
+	GLI_ERR_CUDA = 1,        /* a CUDA runtime call failed */
+	GLI_ERR_ARGUMENT = 2,    /* invalid argument (sizes, grid shape, form) */
+	GLI_ERR_NO_DEVICE = 3,   /* no CUDA device visible */
+	GLI_ERR_ALLOC = 4,       /* host allocation failed */
+	GLI_ERR_LIMIT = 5,       /* a size exceeds a documented limit */
+	GLI_ERR_INTERNAL = 6     /* an internal consistency check failed */
+};
+
+/* status and message of the last call made by this thread */
+int gli_b200_last_error(void);
+const char* gli_b200_last_error_message(void);
+
+/* number of visible CUDA devices (0 without a GPU; never fails) */
+int gli_b200_device_count(void);
+/* CUDA device used by the calling thread's subsequent calls (default 0) */
+int gli_b200_set_device(int ordinal);
+/* library version string */
+const char* gli_b200_version(void);
+
+/* precision forms of the sparse ERI/ERIDA evaluation */
+#define GLI_FORM_FP64 0   /* plain FP64 throughout: the drop-in form */
+#define GLI_FORM_MIXED 1  /* FP32 bulk lattice sums, compensated, FP64 final accumulation */
+
+/* kinds of sparse class lists */
+#define GLI_KIND_ERIDA 0
+#define GLI_KIND_ERI 1
+
+/* Sparse ERI (kind 1) / ERIDA (kind 0) values for a class list already in
+ * device memory; d_values receives num doubles in device memory.  Same
+ * semantics as compute_sparse_{eri,erida}_gausslet_integrals (reference
+ * src/eri_integrals.c:544-678, src/erida_integrals.c:429-542).  stream is a
+ * cudaStream_t (NULL = the library's per-thread stream); the call returns
+ * after the work is queued on it.  Returns a gli_b200_status. */
+int gli_b200_sparse_values_dev(int kind, const double* coeffs, glong num_coeffs,
+	const struct cartesian_grid_3d* grid, const glong* d_indices, glong num,
+	double tol, int form, double* d_values, void* stream);
+
+/* Same evaluation with host buffers (copies inside): the reference call with a
+ * form switch.  values receives num doubles. */
+int gli_b200_sparse_values(int kind, const struct gausslet_data* gdata,
+	const struct cartesian_grid_3d* grid, const glong* indices, glong num,
+	double tol, int form, double* values);
+
+/* Symmetry-reduced class list of kind 0/1 into device memory (reference
+ * src/eri_integrals.c:382-526, src/erida_integrals.c:300-410).  *d_indices is
+ * allocated with cudaMallocAsync on stream; release with gli_b200_free_dev. */
+int gli_b200_enumerate_dev(int kind, const struct cartesian_grid_3d* grid,
+	glong** d_indices, glong* num, void* stream);
+int gli_b200_free_dev(void* d_ptr, void* stream);
+
+/* Per-stage device times (ms) of the last staged evaluation on this thread:
+ * [tables, stage A, stage B, stage C]; sizes = [keys, key pairs, lattice extent U].
+ * Filled only when timing is enabled with gli_b200_set_timing(1). */
+int gli_b200_set_timing(int enable);
+
+/* Measured FP64 FMA throughput of the current device (TFLOP/s), from a
+ * compute-only probe kernel; the denominator of the FP64 roofline. */
+int gli_b200_measure_fp64_peak(double* tflops);
+int gli_b200_last_stage_times(float ms[4], glong sizes[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLI_B200_H */
