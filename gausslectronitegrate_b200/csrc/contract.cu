@@ -10,12 +10,18 @@
 //   val = sum_u W[kx][u] sum_v W[ky][v] sum_t W[kz][t] T[u^2+v^2+t^2].
 // Classes share per-axis keys heavily (3.57M ERI classes on 7^3 use 364 keys
 // and ~4e4 key pairs), so the sum is staged over the whole class list:
-//   stage A  H[a][v][u]  = sum_t W[key_a][t] T[u^2 + v^2 + t^2]      per distinct A key
-//   stage B  H2[p][u]    = sum_v W[key_b][v] H[a(p)][v][u]            per distinct (A, B) key pair
+//   stage A  H[a][s]     = sum_t W[key_a][t] T[s + t^2]               per distinct A key, s = u^2+v^2
+//   stage B  H2[p][u]    = sum_v W[key_b][v] H[a(p)][u^2+v^2]         per distinct (A, B) key pair
 //   stage C  val[n]      = sum_u W[key_c][u] H2[p(n)][u]              per class: warp dot + shuffles
 // The value is symmetric under permuting the three axes (T is), so each class's
 // key triple is sorted (k1 <= k2 <= k3) and assigned A = k2, B = k1, C = k3.
+// Stage A runs over the distinct s = u^2 + v^2 (H depends on u, v only through
+// s); stage C is a per-class warp dot product, or -- when the (pair, key)
+// combinations are few against the classes -- one small GEMM plus a gather.
 #include <math.h>
+
+#include <algorithm>
+#include <memory>
 
 #include "tables.cuh"
 
@@ -101,6 +107,12 @@ __global__ void k_mark_pairs(ClassDecode d, const int64_t* __restrict__ idx, i64
     usedPair[(i64)kid[k[1]] * nku + (i64)kid[k[0]]] = 1;
 }
 
+// ids of the second half of a joint scan, shifted back to start at 0
+__global__ void k_offset_ids(i64 n, const uint64_t* __restrict__ in, uint64_t base, uint64_t* __restrict__ out) {
+    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = in[k] - base;
+}
+
 // compact id -> original key
 __global__ void k_key_of(i64 nkeys, const uint32_t* __restrict__ used, const uint64_t* __restrict__ id,
                          int* __restrict__ keyOf) {
@@ -127,82 +139,156 @@ __global__ void k_class_pairs(ClassDecode d, const int64_t* __restrict__ idx, i6
         cls[n] = make_int2(-1, 0);
         return;
     }
-    cls[n] = make_int2((int)pairId[(i64)kid[k[1]] * nku + (i64)kid[k[0]]], (int)k[2]);
+    cls[n] = make_int2((int)pairId[(i64)kid[k[1]] * nku + (i64)kid[k[0]]], (int)kid[k[2]]);
 }
 
 // ---------------------------------------------------------------------------
-// stage A: H[a][v][u] = sum_t W[aKey[a]][t] T[u^2 + v^2 + t^2]
-// block: 16 x 16 (u, v) tile, KA keys; each thread owns one (u, v) and KA sums.
-constexpr int A_TILE = 16;
-constexpr int A_KEYS = 16;
-constexpr int A_TCHUNK = 32;
+// stage A: H[a][j] = sum_t W[aKey[a]][t] T[S[j] + t^2]
+// H depends on (u, v) only through s = u^2 + v^2, so it is evaluated once per
+// distinct s (S, ascending; 10,823 values instead of 31,329 (u, v) at U = 177).
+// Block: 64 threads x 2 s-values, KT keys held in registers per thread; the
+// keys' weights for a chunk of t sit in shared memory, read as double2
+// broadcasts.  Per t a thread issues 2 table gathers and KT/2 shared loads for
+// 2*KT FMAs.
+constexpr int A_THREADS = 128;
+constexpr int A_SPT = 2;                  // s-values per thread
+constexpr int A_STILE = A_THREADS * A_SPT;
+constexpr int A_TC = 32;                  // t chunk
 
-__global__ void __launch_bounds__(256) k_stage_a(const double* __restrict__ W, const double* __restrict__ T,
-                                                  const int* __restrict__ aKey, int nA, int U, int Up,
-                                                  double* __restrict__ H) {
-    __shared__ double ws[A_KEYS][A_TCHUNK];
-    const int u = blockIdx.x * A_TILE + (threadIdx.x & (A_TILE - 1));
-    const int v = blockIdx.y * A_TILE + (threadIdx.x / A_TILE);
-    const int a0 = blockIdx.z * A_KEYS;
-    const bool live = (u < U) && (v < U);
-    const int uv2 = u * u + v * v;
-    double acc[A_KEYS];
+template <int KT>
+__global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict__ W, const double* __restrict__ T,
+                                                        const int* __restrict__ S, const int* __restrict__ aKey,
+                                                        int nA, int nS, int U, int Up, double* __restrict__ H) {
+    __shared__ __align__(16) double ws[A_TC][KT];
+    const int j0 = blockIdx.x * A_STILE + threadIdx.x;
+    const int j1 = j0 + A_THREADS;
+    const int a0 = blockIdx.y * KT;
+    const int s0 = j0 < nS ? S[j0] : 0;
+    const int s1 = j1 < nS ? S[j1] : 0;
+    double acc0[KT], acc1[KT];
 #pragma unroll
-    for (int k = 0; k < A_KEYS; ++k) acc[k] = 0;
-    for (int t0 = 0; t0 < U; t0 += A_TCHUNK) {
+    for (int k = 0; k < KT; ++k) acc0[k] = acc1[k] = 0;
+    for (int t0 = 0; t0 < U; t0 += A_TC) {
         __syncthreads();
-        for (int e = threadIdx.x; e < A_KEYS * A_TCHUNK; e += blockDim.x) {
-            const int k = e / A_TCHUNK, t = t0 + e % A_TCHUNK;
-            ws[k][e % A_TCHUNK] = (a0 + k < nA && t < U) ? W[(i64)aKey[a0 + k] * Up + t] : 0.0;
+        for (int e = threadIdx.x; e < A_TC * KT; e += A_THREADS) {
+            const int k = e / A_TC, tt = e % A_TC, t = t0 + tt;
+            ws[tt][k] = (a0 + k < nA && t < U) ? W[(i64)aKey[a0 + k] * Up + t] : 0.0;
         }
         __syncthreads();
-        if (live) {
-            const int tmax = min(A_TCHUNK, U - t0);
-            for (int tt = 0; tt < tmax; ++tt) {
-                const int t = t0 + tt;
-                const double g = __ldg(&T[uv2 + t * t]);
+        const int tmax = min(A_TC, U - t0);
+        for (int tt = 0; tt < tmax; ++tt) {
+            const int t2 = (t0 + tt) * (t0 + tt);
+            const double g0 = __ldg(&T[s0 + t2]);
+            const double g1 = __ldg(&T[s1 + t2]);
+            const double2* w2 = reinterpret_cast<const double2*>(&ws[tt][0]);
 #pragma unroll
-                for (int k = 0; k < A_KEYS; ++k) acc[k] = fma(ws[k][tt], g, acc[k]);
+            for (int k = 0; k < KT / 2; ++k) {
+                const double2 w = w2[k];
+                acc0[2 * k] = fma(w.x, g0, acc0[2 * k]);
+                acc0[2 * k + 1] = fma(w.y, g0, acc0[2 * k + 1]);
+                acc1[2 * k] = fma(w.x, g1, acc1[2 * k]);
+                acc1[2 * k + 1] = fma(w.y, g1, acc1[2 * k + 1]);
             }
         }
     }
-    if (!live) return;
-    const i64 plane = (i64)U * U;
 #pragma unroll
-    for (int k = 0; k < A_KEYS; ++k)
-        if (a0 + k < nA) H[(i64)(a0 + k) * plane + (i64)v * U + u] = acc[k];
-}
-
-// ---------------------------------------------------------------------------
-// stage B: H2[p][u] = sum_v W[pairB[p]][v] H[pairA[p]][v][u]; one block per pair
-__global__ void __launch_bounds__(128) k_stage_b(const double* __restrict__ W, const double* __restrict__ H,
-                                                  const int* __restrict__ pairA, const int* __restrict__ pairB, int U,
-                                                  int Up, double* __restrict__ H2) {
-    extern __shared__ double wb[];
-    const int p = blockIdx.x;
-    const double* w = W + (i64)pairB[p] * Up;
-    for (int v = threadIdx.x; v < U; v += blockDim.x) wb[v] = w[v];
-    __syncthreads();
-    const double* h = H + (i64)pairA[p] * U * U;
-    for (int u = threadIdx.x; u < U; u += blockDim.x) {
-        double acc = 0;
-        for (int v = 0; v < U; ++v) acc = fma(wb[v], h[(i64)v * U + u], acc);
-        H2[(i64)p * Up + u] = acc;
+    for (int k = 0; k < KT; ++k) {
+        if (a0 + k >= nA) break;
+        double* h = H + (i64)(a0 + k) * nS;
+        if (j0 < nS) h[j0] = acc0[k];
+        if (j1 < nS) h[j1] = acc1[k];
     }
 }
 
 // ---------------------------------------------------------------------------
-// stage C: one warp per class, lanes stride over u, shuffle reduction
+// stage B: H2[p][u] = sum_v W[pairB[p]][v] Hf[pairA[p]][v][u]
+// Hf is H expanded back to the full (v, u) square (coalesced reads over u).
+// Pairs are ordered by their A key; block (A key, chunk of 16 of its pairs,
+// 128 u) keeps 16 accumulators per thread, so each Hf value feeds 16 FMAs and
+// the 16 B-key weights are double2 shared-memory broadcasts.
+constexpr int B_THREADS = 128;
+constexpr int B_PAIRS = 16;
+constexpr int B_VC = 64;                  // v chunk staged in shared memory
+
+__global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__ sidx, i64 nA, int nS, int U,
+                           double* __restrict__ Hf) {
+    const i64 plane = (i64)U * U;
+    const i64 total = nA * plane;
+    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
+        const i64 a = e / plane, vu = e % plane;
+        Hf[e] = H[a * nS + sidx[vu]];
+    }
+}
+
+__global__ void __launch_bounds__(B_THREADS) k_stage_b(const double* __restrict__ W, const double* __restrict__ Hf,
+                                                        const int* __restrict__ pairA, const int* __restrict__ pairB,
+                                                        int nP, int U, int Up, double* __restrict__ H2) {
+    __shared__ __align__(16) double wb[B_VC][B_PAIRS];
+    __shared__ int range[2];
+    const int a = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nP;  // first pair with pairA >= a
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (pairA[mid] < a) lo = mid + 1; else hi = mid;
+        }
+        int lo2 = lo, hi2 = nP;  // first pair with pairA > a
+        while (lo2 < hi2) {
+            const int mid = (lo2 + hi2) >> 1;
+            if (pairA[mid] <= a) lo2 = mid + 1; else hi2 = mid;
+        }
+        range[0] = lo;
+        range[1] = lo2;
+    }
+    __syncthreads();
+    const int pc = range[0] + blockIdx.y * B_PAIRS;
+    if (pc >= range[1]) return;  // uniform across the block
+    const int np = min(B_PAIRS, range[1] - pc);
+    const int u = blockIdx.z * B_THREADS + threadIdx.x;
+    const bool live = u < U;
+    const double* h = Hf + (i64)a * U * U + u;
+    double acc[B_PAIRS];
+#pragma unroll
+    for (int k = 0; k < B_PAIRS; ++k) acc[k] = 0;
+    for (int v0 = 0; v0 < U; v0 += B_VC) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < B_VC * B_PAIRS; e += B_THREADS) {
+            const int k = e / B_VC, vv = e % B_VC, v = v0 + vv;
+            wb[vv][k] = (k < np && v < U) ? W[(i64)pairB[pc + k] * Up + v] : 0.0;
+        }
+        __syncthreads();
+        if (live) {
+            const int vmax = min(B_VC, U - v0);
+            for (int vv = 0; vv < vmax; ++vv) {
+                const double g = h[(i64)(v0 + vv) * U];
+                const double2* w2 = reinterpret_cast<const double2*>(&wb[vv][0]);
+#pragma unroll
+                for (int k = 0; k < B_PAIRS / 2; ++k) {
+                    const double2 w = w2[k];
+                    acc[2 * k] = fma(w.x, g, acc[2 * k]);
+                    acc[2 * k + 1] = fma(w.y, g, acc[2 * k + 1]);
+                }
+            }
+        }
+    }
+    if (live)
+#pragma unroll
+        for (int k = 0; k < B_PAIRS; ++k)
+            if (k < np) H2[(i64)(pc + k) * Up + u] = acc[k];
+}
+
+// ---------------------------------------------------------------------------
+// stage C, per class: one warp per class, lanes stride over u, shuffle reduction
 __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, const double* __restrict__ H2,
-                                                  const int2* __restrict__ cls, i64 m, int U, int Up,
-                                                  double* __restrict__ out) {
+                                                  const int2* __restrict__ cls, const int* __restrict__ keyOf, i64 m,
+                                                  int U, int Up, double* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
     for (i64 n = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); n < m; n += warps) {
         const int2 c = cls[n];
         double acc = 0;
         if (c.x >= 0) {
-            const double* w = W + (i64)c.y * Up;
+            const double* w = W + (i64)keyOf[c.y] * Up;
             const double* h = H2 + (i64)c.x * Up;
             for (int u = lane; u < U; u += 32) acc = fma(w[u], h[u], acc);
         }
@@ -212,6 +298,26 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
     }
 }
 
+// stage C as a product: Q[p][j] = sum_u H2[p][u] Wu[j][u] for every (pair, used key),
+// then a gather val[n] = Q[p(n)][j(n)].  Chosen when nP * nku is small against m.
+__global__ void k_gather_rows(const double* __restrict__ W, const int* __restrict__ keyOf, int nku, int Up,
+                              double* __restrict__ Wu) {
+    const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (i64)nku * Up) return;
+    Wu[e] = W[(i64)keyOf[e / Up] * Up + e % Up];
+}
+
+__global__ void k_gather_q(const double* __restrict__ Q, const int2* __restrict__ cls, i64 m, int nku,
+                           double* __restrict__ out) {
+    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m) return;
+    const int2 c = cls[n];
+    out[n] = c.x >= 0 ? Q[(i64)c.x * nku + c.y] : 0.0;
+}
+
+void dgemm_strided(int M, int N, int K, const double* A, i64 asb, i64 ar, i64 ac, const double* B, i64 bsb, i64 br,
+                   i64 bc, double* C, i64 csb, i64 cr, i64 cc, int batch, bool accumulate, cudaStream_t s);
+
 static thread_local bool t_timing = false;
 static thread_local ContractStats t_last;
 
@@ -219,16 +325,19 @@ void set_timing(bool on) { t_timing = on; }
 const ContractStats& last_stats() { return t_last; }
 
 struct StageTimer {
+    static constexpr int kMax = 8;
     bool on;
     cudaStream_t s;
-    cudaEvent_t ev[5];
+    cudaEvent_t ev[kMax];
     int n = 0;
     StageTimer(bool enabled, cudaStream_t st) : on(enabled), s(st) {
         if (on)
             for (auto& e : ev) GLI_CUDA(cudaEventCreate(&e));
     }
     void mark() {
-        if (on) GLI_CUDA(cudaEventRecord(ev[n++], s));
+        if (!on) return;
+        if (n >= kMax) fail(GLI_ERR_INTERNAL, "stage timer overflow");
+        GLI_CUDA(cudaEventRecord(ev[n++], s));
     }
     ~StageTimer() {
         if (on)
@@ -243,13 +352,13 @@ struct StageTimer {
 
 void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
                           i64 m, double tol, int form, double* d_out, cudaStream_t s, ContractStats* stats) {
-    if (form != FORM_FP64 && form != FORM_MIXED) fail(GLI_ERR_ARGUMENT, "unknown form %d", form);
+    if (form != FORM_FP64) fail(GLI_ERR_ARGUMENT, "form %d is not available for the sparse evaluation", form);
     if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
     if (m == 0) return;
     StageTimer timer(t_timing, s);
     timer.mark();
-    LatticeTables t;
-    build_lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, t, s);
+    const std::shared_ptr<const LatticeTables> tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
+    const LatticeTables& t = *tp;
     timer.mark();
 
     ClassDecode d;
@@ -262,32 +371,41 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     }
     d.nkeys = t.nkeys;
     const i64 nk = t.nkeys;
-    DevBuf<uint32_t> usedKey(nk, s), usedA(nk, s);
-    usedKey.zero();
-    usedA.zero();
+    // usedKey and usedA side by side so that one scan serves both
+    DevBuf<uint32_t> used(2 * nk, s);
+    used.zero();
+    uint32_t* usedKey = used.p;
+    uint32_t* usedA = used.p + nk;
     DevBuf<int> bad(1, s);
     bad.zero();
     const unsigned cb = (unsigned)((m + 255) / 256);
     const unsigned kb = (unsigned)((nk + 255) / 256);
-    k_mark_keys<<<cb, 256, 0, s>>>(d, d_indices, m, usedKey.p, usedA.p, bad.p);
+    k_mark_keys<<<cb, 256, 0, s>>>(d, d_indices, m, usedKey, usedA, bad.p);
     GLI_CHECK_LAUNCH();
-    DevBuf<uint64_t> kid(nk, s), aId(nk, s);
-    const i64 nku = exclusive_scan_u32(usedKey.p, kid.p, nk, s);
-    const i64 nA = exclusive_scan_u32(usedA.p, aId.p, nk, s);
+    DevBuf<uint64_t> ids(2 * nk, s);
+    const i64 total = exclusive_scan_u32(used.p, ids.p, 2 * nk, s);
+    uint64_t nku_h = 0;
+    GLI_CUDA(cudaMemcpyAsync(&nku_h, ids.p + nk, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     int h_bad = 0;
     GLI_CUDA(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     GLI_CUDA(cudaStreamSynchronize(s));
     if (h_bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
+    const i64 nku = (i64)nku_h, nA = total - nku;
     if (nku > 16384) fail(GLI_ERR_LIMIT, "class list uses %lld distinct axis keys (limit 16384)", (long long)nku);
+    const uint64_t* kid = ids.p;
+    // the A ids continue the key ids' numbering; offset them back to 0
+    DevBuf<uint64_t> aId(nk, s);
+    k_offset_ids<<<kb, 256, 0, s>>>(nk, ids.p + nk, (uint64_t)nku, aId.p);
+    GLI_CHECK_LAUNCH();
 
     DevBuf<int> keyOf(nku, s), aKey(nA, s);
-    k_key_of<<<kb, 256, 0, s>>>(nk, usedKey.p, kid.p, keyOf.p);
+    k_key_of<<<kb, 256, 0, s>>>(nk, usedKey, kid, keyOf.p);
     GLI_CHECK_LAUNCH();
-    k_key_of<<<kb, 256, 0, s>>>(nk, usedA.p, aId.p, aKey.p);
+    k_key_of<<<kb, 256, 0, s>>>(nk, usedA, aId.p, aKey.p);
     GLI_CHECK_LAUNCH();
     DevBuf<uint32_t> usedPair(nku * nku, s);
     usedPair.zero();
-    k_mark_pairs<<<cb, 256, 0, s>>>(d, d_indices, m, kid.p, nku, usedPair.p);
+    k_mark_pairs<<<cb, 256, 0, s>>>(d, d_indices, m, kid, nku, usedPair.p);
     GLI_CHECK_LAUNCH();
     DevBuf<uint64_t> pairId(nku * nku, s);
     const i64 nP = exclusive_scan_u32(usedPair.p, pairId.p, nku * nku, s);
@@ -296,25 +414,61 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
                                                                       pairA.p, pairB.p);
     GLI_CHECK_LAUNCH();
     DevBuf<int2> cls(m, s);
-    k_class_pairs<<<cb, 256, 0, s>>>(d, d_indices, m, kid.p, nku, pairId.p, cls.p);
+    k_class_pairs<<<cb, 256, 0, s>>>(d, d_indices, m, kid, nku, pairId.p, cls.p);
     GLI_CHECK_LAUNCH();
 
-    const int U = (int)t.U, Up = (int)t.Up;
-    DevBuf<double> H(nA * (i64)U * U, s);
-    dim3 ga((U + A_TILE - 1) / A_TILE, (U + A_TILE - 1) / A_TILE, (unsigned)((nA + A_KEYS - 1) / A_KEYS));
+    const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
+    if (nA * (i64)U * U > ((i64)1 << 31))
+        fail(GLI_ERR_LIMIT, "stage buffers exceed 16 GB (%lld A keys, lattice extent %d)", (long long)nA, U);
+    DevBuf<double> H(nA * (i64)nS, s);
     timer.mark();
-    k_stage_a<<<ga, 256, 0, s>>>(t.W.p, t.T.p, aKey.p, (int)nA, U, Up, H.p);
+    {
+        // keys per thread: fewer when the problem is small, so that enough
+        // warps exist to hide the table-gather latency
+        const i64 outputs = nA * (i64)nS;
+        const unsigned sb = (unsigned)((nS + A_STILE - 1) / A_STILE);
+        if (outputs >= 4000000 && nA >= 32)
+            k_stage_a<32><<<dim3(sb, (unsigned)((nA + 31) / 32)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p,
+                                                                                    (int)nA, nS, U, Up, H.p);
+        else if (outputs >= 1000000)
+            k_stage_a<16><<<dim3(sb, (unsigned)((nA + 15) / 16)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p,
+                                                                                    (int)nA, nS, U, Up, H.p);
+        else
+            k_stage_a<4><<<dim3(sb, (unsigned)((nA + 3) / 4)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p,
+                                                                                 (int)nA, nS, U, Up, H.p);
+    }
     GLI_CHECK_LAUNCH();
     timer.mark();
     DevBuf<double> H2(nP * (i64)Up, s);
-    k_stage_b<<<(unsigned)nP, 128, U * sizeof(double), s>>>(t.W.p, H.p, pairA.p, pairB.p, U, Up, H2.p);
-    GLI_CHECK_LAUNCH();
+    {
+        DevBuf<double> Hf(nA * (i64)U * U, s);
+        const Context& ctx = context();
+        const i64 ework = nA * (i64)U * U;
+        const i64 eb = std::min<i64>((ework + 255) / 256, (i64)ctx.num_sms * 32);
+        k_expand_h<<<(unsigned)eb, 256, 0, s>>>(H.p, t.sidx.p, nA, nS, U, Hf.p);
+        GLI_CHECK_LAUNCH();
+        // chunk slots per A key: at most nku pairs share one A key
+        const unsigned chunks = (unsigned)((nku + B_PAIRS - 1) / B_PAIRS);
+        k_stage_b<<<dim3((unsigned)nA, chunks, (unsigned)((U + B_THREADS - 1) / B_THREADS)), B_THREADS, 0, s>>>(
+            t.W.p, Hf.p, pairA.p, pairB.p, (int)nP, U, Up, H2.p);
+        GLI_CHECK_LAUNCH();
+    }
     timer.mark();
-    const Context& ctx = context();
-    const i64 want = (m + 7) / 8;
-    const unsigned gc = (unsigned)(want < (i64)ctx.num_sms * 16 ? want : (i64)ctx.num_sms * 16);
-    k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls.p, m, U, Up, d_out);
-    GLI_CHECK_LAUNCH();
+    if (nP * nku <= m) {
+        // product form: Q = H2 Wu^T over all (pair, used key), then a gather
+        DevBuf<double> Wu(nku * (i64)Up, s), Q(nP * nku, s);
+        k_gather_rows<<<(unsigned)((nku * Up + 255) / 256), 256, 0, s>>>(t.W.p, keyOf.p, (int)nku, Up, Wu.p);
+        GLI_CHECK_LAUNCH();
+        dgemm_strided((int)nP, (int)nku, U, H2.p, 0, Up, 1, Wu.p, 0, 1, Up, Q.p, 0, nku, 1, 1, false, s);
+        k_gather_q<<<cb, 256, 0, s>>>(Q.p, cls.p, m, (int)nku, d_out);
+        GLI_CHECK_LAUNCH();
+    } else {
+        const Context& ctx = context();
+        const i64 want = (m + 7) / 8;
+        const unsigned gc = (unsigned)(want < (i64)ctx.num_sms * 16 ? want : (i64)ctx.num_sms * 16);
+        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls.p, keyOf.p, m, U, Up, d_out);
+        GLI_CHECK_LAUNCH();
+    }
     timer.mark();
     ContractStats st;
     st.keys_a = nA;

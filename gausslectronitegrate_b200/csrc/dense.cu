@@ -121,12 +121,19 @@ __global__ void __launch_bounds__(256) k_dgemm(int M, int N, int K, MatView A, M
     const double* Ab = A.p + (i64)b * A.sb;
     const double* Bb = B.p + (i64)b * B.sb;
     double acc[4][4] = {};
+    // consecutive threads walk the operand's unit-stride direction, so tile
+    // loads are coalesced for row-major, column-major and transposed views
+    const bool a_k_fast = (A.c == 1 && A.r != 1), b_k_fast = (B.r == 1 && B.c != 1);
     for (int k0 = 0; k0 < K; k0 += GK) {
         for (int e = threadIdx.x; e < GK * GT; e += 256) {
-            const int kk = e / GT, ii = e % GT;
-            const int gi = i0 + ii, gk = k0 + kk, gj = j0 + ii;
+            const int kk = a_k_fast ? e % GK : e / GT, ii = a_k_fast ? e / GK : e % GT;
+            const int gi = i0 + ii, gk = k0 + kk;
             as[kk][ii] = (gi < M && gk < K) ? Ab[(i64)gi * A.r + (i64)gk * A.c] : 0.0;
-            bs[kk][ii] = (gj < N && gk < K) ? Bb[(i64)gk * B.r + (i64)gj * B.c] : 0.0;
+        }
+        for (int e = threadIdx.x; e < GK * GT; e += 256) {
+            const int kk = b_k_fast ? e % GK : e / GT, jj = b_k_fast ? e / GK : e % GT;
+            const int gj = j0 + jj, gk = k0 + kk;
+            bs[kk][jj] = (gj < N && gk < K) ? Bb[(i64)gk * B.r + (i64)gj * B.c] : 0.0;
         }
         __syncthreads();
 #pragma unroll

@@ -167,8 +167,36 @@ __global__ void scan_tiles_apply(const uint32_t* __restrict__ in, i64 n, const u
     }
 }
 
+// small arrays: one block, each thread scans a contiguous run; total at tot[0]
+constexpr i64 SCAN_SMALL = 1 << 16;
+
+__global__ void scan_small(const uint32_t* __restrict__ in, i64 n, uint64_t* __restrict__ out,
+                           uint64_t* __restrict__ tot) {
+    __shared__ uint64_t ws[32];
+    __shared__ uint64_t total;
+    const i64 per = (n + blockDim.x - 1) / blockDim.x;
+    const i64 b = (i64)threadIdx.x * per, e = b + per < n ? b + per : n;
+    uint64_t sum = 0;
+    for (i64 k = b; k < e; ++k) sum += in[k];
+    uint64_t run = block_exclusive_sum(sum, ws, &total);
+    for (i64 k = b; k < e; ++k) {
+        out[k] = run;
+        run += in[k];
+    }
+    if (threadIdx.x == 0) tot[0] = total;
+}
+
 i64 exclusive_scan_u32(const uint32_t* d_in, uint64_t* d_out, i64 n, cudaStream_t s) {
     if (n == 0) return 0;
+    if (n <= SCAN_SMALL) {
+        DevBuf<uint64_t> tot(1, s);
+        scan_small<<<1, SCAN_BLOCK, 0, s>>>(d_in, n, d_out, tot.p);
+        GLI_CHECK_LAUNCH();
+        uint64_t total = 0;
+        GLI_CUDA(cudaMemcpyAsync(&total, tot.p, sizeof(total), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        return (i64)total;
+    }
     const i64 ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     DevBuf<uint64_t> tiles(ntiles + 1, s);
     scan_tile_sums<<<(unsigned)ntiles, SCAN_BLOCK, 0, s>>>(d_in, n, tiles.p);

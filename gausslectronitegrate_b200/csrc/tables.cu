@@ -18,6 +18,9 @@
 //   positions u >= 0 and T is read at u^2 + v^2 + t^2.
 #include <math.h>
 
+#include <list>
+#include <mutex>
+
 #include "tables.cuh"
 
 namespace gli {
@@ -133,10 +136,29 @@ void factors_device(const double* d_b, int nb, int L, double* d_F, cudaStream_t 
     GLI_CHECK_LAUNCH();
 }
 
-void build_lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol, LatticeTables& t,
-                          cudaStream_t s) {
-    if (nb <= 0 || nb % 2 != 1) fail(GLI_ERR_ARGUMENT, "gausslet coefficient count must be odd, got %lld", (long long)nb);
-    if (nb > 4096) fail(GLI_ERR_LIMIT, "gausslet coefficient count %lld exceeds 4096", (long long)nb);
+// distinct s = u^2 + v^2 (u, v < U): mark, scan, list, and the U x U index
+__global__ void k_mark_s(int U, uint32_t* __restrict__ mark) {
+    const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (i64)U * U) return;
+    const int u = (int)(e / U), v = (int)(e % U);
+    mark[u * u + v * v] = 1;
+}
+
+__global__ void k_s_list(i64 n, const uint32_t* __restrict__ mark, const uint64_t* __restrict__ pos,
+                         int* __restrict__ S) {
+    const i64 s = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n && mark[s]) S[pos[s]] = (int)s;
+}
+
+__global__ void k_s_index(int U, const uint64_t* __restrict__ pos, int* __restrict__ sidx) {
+    const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (i64)U * U) return;
+    const int u = (int)(e / U), v = (int)(e % U);
+    sidx[e] = (int)pos[u * u + v * v];
+}
+
+static void build_lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol, LatticeTables& t,
+                                 cudaStream_t s) {
     t.kind = kind;
     t.L = L;
     DevBuf<double> b(nb, s);
@@ -167,17 +189,70 @@ void build_lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, doubl
     const i64 centre_max = kind == 0 ? 3 * (L - 1) : 6 * (L - 1);
     if (t.nkeys > 65535) fail(GLI_ERR_LIMIT, "grid too large for the per-axis key table (%lld keys)", (long long)t.nkeys);
     t.U = h_max < 0 ? 1 : centre_max + h_max + 1;
+    if (t.U > 4096) fail(GLI_ERR_LIMIT, "lattice extent %lld exceeds 4096", (long long)t.U);
     t.Up = (t.U + 3) / 4 * 4;
     t.tlen = 3 * (t.U - 1) * (t.U - 1) + 1;
 
-    t.W.alloc(t.nkeys * t.Up, s);
+    t.W.alloc(t.nkeys * t.Up);
     k_fold_weights<<<dim3((unsigned)((t.Up + 127) / 128), (unsigned)t.nkeys), 128, 0, s>>>(
         kind, prod.p, (int)nb, (int)L, t.nkeys, (int)t.U, (int)t.Up, t.W.p);
     GLI_CHECK_LAUNCH();
-    if (h_max < 0) t.W.zero();
-    t.T.alloc(t.tlen, s);
+    t.T.alloc(t.tlen);
     k_coulomb_table<<<(unsigned)((t.tlen + 255) / 256), 256, 0, s>>>(kind, t.tlen, t.T.p);
     GLI_CHECK_LAUNCH();
+
+    const i64 U = t.U, smax = 2 * (U - 1) * (U - 1) + 1;
+    DevBuf<uint32_t> mark(smax, s);
+    mark.zero();
+    k_mark_s<<<(unsigned)((U * U + 255) / 256), 256, 0, s>>>((int)U, mark.p);
+    GLI_CHECK_LAUNCH();
+    DevBuf<uint64_t> pos(smax, s);
+    t.nS = exclusive_scan_u32(mark.p, pos.p, smax, s);
+    t.S.alloc(t.nS);
+    k_s_list<<<(unsigned)((smax + 255) / 256), 256, 0, s>>>(smax, mark.p, pos.p, t.S.p);
+    GLI_CHECK_LAUNCH();
+    t.sidx.alloc(U * U);
+    k_s_index<<<(unsigned)((U * U + 255) / 256), 256, 0, s>>>((int)U, pos.p, t.sidx.p);
+    GLI_CHECK_LAUNCH();
+    GLI_CUDA(cudaStreamSynchronize(s));
+}
+
+namespace {
+struct CacheEntry {
+    int kind, device;
+    i64 L;
+    double tol;
+    std::vector<double> coeffs;
+    std::shared_ptr<const LatticeTables> tables;
+};
+std::mutex g_cache_mu;
+std::list<CacheEntry> g_cache;
+constexpr size_t kCacheEntries = 8;
+}  // namespace
+
+std::shared_ptr<const LatticeTables> lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol,
+                                                    cudaStream_t s) {
+    if (nb <= 0 || nb % 2 != 1) fail(GLI_ERR_ARGUMENT, "gausslet coefficient count must be odd, got %lld", (long long)nb);
+    if (nb > 4096) fail(GLI_ERR_LIMIT, "gausslet coefficient count %lld exceeds 4096", (long long)nb);
+    int device = 0;
+    GLI_CUDA(cudaGetDevice(&device));
+    std::vector<double> c(h_coeffs, h_coeffs + nb);
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
+            if (it->kind == kind && it->device == device && it->L == L && it->tol == tol && it->coeffs == c) {
+                g_cache.splice(g_cache.begin(), g_cache, it);  // most recently used first
+                return it->tables;
+            }
+        }
+    }
+    auto t = std::make_shared<LatticeTables>();
+    t->device = device;
+    build_lattice_tables(kind, h_coeffs, nb, L, tol, *t, s);
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_cache.push_front(CacheEntry{kind, device, L, tol, std::move(c), t});
+    while (g_cache.size() > kCacheEntries) g_cache.pop_back();
+    return t;
 }
 
 }  // namespace gli

@@ -1,5 +1,7 @@
 // Device-built lookup tables shared by the integral kernels.
 #pragma once
+#include <memory>
+
 #include "gli_internal.cuh"
 
 namespace gli {
@@ -8,22 +10,45 @@ namespace gli {
 //   sum_{u,v,t >= 0} W[kx][u] W[ky][v] W[kz][t] T[u^2 + v^2 + t^2]
 // where W[k] is the folded (|position|-indexed) product weight of per-axis key k
 // and T the Coulomb table on the integer lattice.
+// long-lived device allocation (cached tables outlive the stream that built them)
+template <class T>
+struct DevMem {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        n = count;
+        if (count) GLI_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    }
+    ~DevMem() {
+        if (p) cudaFree(p);
+    }
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+};
+
 struct LatticeTables {
     int kind = 0;            // 0 = ERIDA, 1 = ERI
+    int device = 0;
     i64 L = 0;               // largest axis length of the grid (table sizing as in the reference)
     i64 nkeys = 0;           // size of the dense per-axis key space
     i64 U = 0;               // folded lattice extent: positions 0 .. U-1
     i64 Up = 0;              // U rounded up to a multiple of 4 (row pitch of W)
     i64 tlen = 0;            // T entries: 3 (U-1)^2 + 1
-    DevBuf<double> W;        // nkeys x Up
-    DevBuf<double> T;        // tlen
+    i64 nS = 0;              // distinct values s = u^2 + v^2, u, v < U
+    DevMem<double> W;        // nkeys x Up
+    DevMem<double> T;        // tlen
+    DevMem<int> S;           // nS distinct s values, ascending
+    DevMem<int> sidx;        // U x U: position of u^2 + v^2 in S
 };
 
 // Builds P (ERIDA) or the shift-pair products (ERI) from the coefficients, masks
 // entries with |P| <= tol exactly as the reference's trimming and skipping do,
-// folds them into W and evaluates T.  Synchronises once to learn U.
-void build_lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol,
-                          LatticeTables& t, cudaStream_t s);
+// folds them into W, evaluates T and the distinct-s index.  Tables depend only
+// on (kind, coefficients, L, tol, device) and are cached across calls (a few
+// entries, least recently used evicted); a build synchronises the stream.
+std::shared_ptr<const LatticeTables> lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol,
+                                                    cudaStream_t s);
 
 // dense ERI key of one axis: shift pair (|s01|, |s23|) unordered and |c|/3
 __host__ __device__ inline i64 eri_axis_key(i64 s01, i64 s23, i64 cc, i64 L) {

@@ -1,0 +1,7 @@
+/* Compatibility header carrying the reference's header name (range.h) so that
+ * code written against the reference includes it unchanged.  All types and
+ * functions are declared in gli_b200.h. */
+#ifndef GLI_B200_COMPAT_RANGE_H
+#define GLI_B200_COMPAT_RANGE_H
+#include "gli_b200.h"
+#endif
