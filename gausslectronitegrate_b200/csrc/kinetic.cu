@@ -6,6 +6,9 @@
 // i, threads stride over j with coalesced stores; the table sits in shared
 // memory.
 #include <math.h>
+#include <stdlib.h>
+
+#include <mutex>
 
 #include "gli_internal.cuh"
 
@@ -75,4 +78,79 @@ void kinetic_matrix_device(const double* h_coeffs, i64 nb, const GridDesc& g, do
     GLI_CHECK_LAUNCH();
 }
 
+// ---------------------------------------------------------------------------
+// Kinetic matrix without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they need the
+// matrix: code that has reserved its whole device-memory budget up front (a
+// solver that pre-sizes its arena before the first iteration), code running
+// while another framework captures a CUDA graph or owns the allocator, and
+// hosts that forbid allocation inside a latency-critical loop.  For them the
+// per-axis kinetic table -- the only scratch this computation needs -- lives in
+// the file-scope device array below instead of a cudaMalloc'ed buffer; the
+// caller supplies the coefficients and the output matrix in device memory.
+//
+// The array holds one table entry per grid shift, so the largest axis of the
+// grid may have at most kNoAllocMaxAxis points.  Every GPU that loads the
+// library keeps these 8 KB until the process exits.  The array is shared by all
+// calls on a device: each call rewrites the entries it reads before reading
+// them (nothing needs clearing), so consecutive calls are independent, but two
+// calls whose kernels overlap on the GPU (different streams or threads without
+// ordering between them) race on it.
+constexpr int kNoAllocMaxAxis = 1024;
+static __device__ __align__(256) double g_noalloc_kinetic_table[kNoAllocMaxAxis];
+
+// Host code may not use g_noalloc_kinetic_table directly: on the host that name
+// is a host-side stand-in, not a device address.  The device address is looked
+// up once per device (with that device current) and remembered.
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_table_ptr[64] = {};
+
+static double* noalloc_table_address() {
+    int device = 0;
+    GLI_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= 64) fail(GLI_ERR_LIMIT, "device ordinal %d out of range for the no-alloc table", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_table_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_kinetic_table);
+        if (e != cudaSuccess || p == nullptr)
+            fail(GLI_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc kinetic table failed: %s", cudaGetErrorString(e));
+        g_noalloc_table_ptr[device] = static_cast<double*>(p);
+    }
+    return g_noalloc_table_ptr[device];
+}
+
+static void kinetic_matrix_noalloc(const double* d_coeffs, i64 nb, const GridDesc& g, double* d_out, cudaStream_t s) {
+    if (!d_coeffs || !d_out) fail(GLI_ERR_ARGUMENT, "coefficient and matrix pointers must be device memory, not NULL");
+    if (nb <= 0 || nb % 2 != 1) fail(GLI_ERR_ARGUMENT, "gausslet coefficient count must be odd, got %lld", (long long)nb);
+    const i64 L = g.max_range();
+    if (L > kNoAllocMaxAxis)
+        fail(GLI_ERR_LIMIT, "the allocation-free kinetic matrix supports axes up to %d points (got %lld)", kNoAllocMaxAxis,
+             (long long)L);
+    double* table = noalloc_table_address();
+    k_kinetic_1d<<<(unsigned)L, 256, 0, s>>>(d_coeffs, (int)nb, table);
+    GLI_CHECK_LAUNCH();
+    const i64 N = g.points();
+    const i64 yrows = N < 65535 ? N : 65535;
+    const i64 zrows = (N + yrows - 1) / yrows;
+    const i64 xblocks = (N + 255) / 256 < 8 ? (N + 255) / 256 : 8;
+    k_kinetic_matrix<<<dim3((unsigned)xblocks, (unsigned)yrows, (unsigned)zrows), 256, 0, s>>>(
+        table, (int)L, (int)g.num[0], (int)g.num[1], (int)g.num[2], d_out);
+    GLI_CHECK_LAUNCH();
+}
+
 }  // namespace gli
+
+extern "C" int gli_b200_kinetic_matrix_noalloc(const double* d_coeffs, glong num_coeffs,
+                                               const struct cartesian_grid_3d* grid, double* d_matrix, void* stream) {
+    gli::clear_error();
+    try {
+        if (!grid) gli::fail(GLI_ERR_ARGUMENT, "grid missing");
+        const gli::GridDesc g = gli::grid_desc(grid);
+        gli::kinetic_matrix_noalloc(d_coeffs, num_coeffs, g, d_matrix, static_cast<cudaStream_t>(stream));
+    } catch (const gli::Failure&) {
+        if (!getenv("GLI_B200_QUIET")) fprintf(stderr, "gausslectronitegrate_b200: %s\n", gli::last_message());
+    }
+    return gli::last_error();
+}

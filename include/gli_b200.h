@@ -291,6 +291,24 @@ int gli_b200_set_timing(int enable);
 /* Measured FP64 FMA throughput of the current device (TFLOP/s), from a
  * compute-only probe kernel; the denominator of the FP64 roofline. */
 int gli_b200_measure_fp64_peak(double* tflops);
+
+/* Kinetic matrix (same values as compute_kinetic_gausslet_integrals) for
+ * callers that must not allocate device memory -- code that reserved its whole
+ * device-memory budget up front, code running while another framework captures
+ * a CUDA graph or owns the allocator, or a latency-critical loop where
+ * allocation is forbidden.  This entry point has no counterpart in the
+ * reference and allocates nothing: d_coeffs (num_coeffs doubles) and d_matrix
+ * (N x N doubles, N = grid points, row-major) are device memory supplied by the
+ * caller; the only scratch, a per-axis table of at most 1024 doubles, lives in a
+ * static device array inside the library, so the grid's largest axis may have
+ * at most 1024 points (larger grids fail with GLI_ERR_LIMIT).  The array is
+ * shared by every call on a device, so calls whose kernels overlap on the GPU
+ * race; calls ordered on one stream do not.  The first call on each device
+ * looks the array's device address up (make it before any stream capture).
+ * stream is a cudaStream_t (NULL = the legacy default stream); the call returns
+ * once the work is queued.  Returns a gli_b200_status. */
+int gli_b200_kinetic_matrix_noalloc(const double* d_coeffs, glong num_coeffs,
+	const struct cartesian_grid_3d* grid, double* d_matrix, void* stream);
 int gli_b200_last_stage_times(float ms[4], glong sizes[3]);
 
 #ifdef __cplusplus
