@@ -242,6 +242,7 @@ def run_ours(args):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
+    launches0 = L.gli_b200_launch_count()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     t_wall = time.perf_counter()
@@ -256,6 +257,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t_wall
     clk = clocks.stop()
+    launches = L.gli_b200_launch_count() - launches0
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     my_ms = sum(step_ms)
     t = torch.tensor([my_ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -334,7 +336,7 @@ def run_ours(args):
                      "algorithmic_flops_per_launch": flops_a, "traffic": None},
         "e2e": {"value": m / e2e_s, "unit": "classes/s", "h2d_bytes_per_step": 8 * m + 8 * b.size,
                 "d2h_bytes_per_step": 8 * m},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "clocks": clk,
         "cpu_baseline": cpu,
     }

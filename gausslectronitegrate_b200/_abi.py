@@ -76,7 +76,7 @@ EXPORTS = [
     "gli_b200_last_error", "gli_b200_last_error_message", "gli_b200_device_count", "gli_b200_set_device",
     "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
     "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_measure_fp64_peak",
-    "gli_b200_kinetic_matrix_noalloc",
+    "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
 ]
 
 
@@ -128,4 +128,8 @@ def load(path=LIB_PATH):
     L.gli_b200_measure_fp64_peak.argtypes = [P(C.c_double)]
     L.gli_b200_kinetic_matrix_noalloc.argtypes = [C.c_void_p, glong, P(Grid), C.c_void_p, C.c_void_p]
     L.gli_b200_kinetic_matrix_noalloc.restype = C.c_int
+    L.gli_b200_launch_count.restype = C.c_longlong
+    L.gli_b200_dgemm_sliced_dev.argtypes = [C.c_void_p, glong, C.c_void_p, glong, C.c_void_p, glong, glong, glong, glong,
+                                            C.c_void_p]
+    L.gli_b200_dgemm_sliced_dev.restype = C.c_int
     return L

@@ -216,6 +216,8 @@ int gli_b200_set_device(int ordinal) {
     return gli::set_device(ordinal);
 }
 
+long long gli_b200_launch_count(void) { return gli::launch_count(); }
+
 int gli_b200_measure_fp64_peak(double* tflops) {
     *tflops = 0;
     guarded([&] { *tflops = gli::fp64_probe_tflops(); });

@@ -46,7 +46,14 @@ struct Failure {
                         cudaGetErrorString(_e));                                         \
     } while (0)
 
-#define GLI_CHECK_LAUNCH() GLI_CUDA(cudaGetLastError())
+// every kernel launch site is followed by GLI_CHECK_LAUNCH(), which also counts
+// the launch (per thread) for gli_b200_launch_count()
+void count_launch();
+#define GLI_CHECK_LAUNCH()            \
+    do {                              \
+        ::gli::count_launch();        \
+        GLI_CUDA(cudaGetLastError()); \
+    } while (0)
 
 // ---------------------------------------------------------------------------
 // device context: the calling thread's device and its non-blocking stream
@@ -158,6 +165,7 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
 
 // runtime.cu / contract.cu
 double fp64_probe_tflops();
+long long launch_count();
 const char* last_message();
 int set_device(int ordinal);
 void set_timing(bool on);

@@ -38,6 +38,10 @@ void fail(int code, const char* fmt, ...) {
 
 const char* last_message() { return t_message; }
 
+static thread_local long long t_launches = 0;
+void count_launch() { ++t_launches; }
+long long launch_count() { return t_launches; }
+
 int set_device(int ordinal) {
     t_device = ordinal;
     return GLI_OK;
