@@ -315,6 +315,129 @@ __global__ void k_gather_q(const double* __restrict__ Q, const int2* __restrict_
     out[n] = c.x >= 0 ? Q[(i64)c.x * nku + c.y] : 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// mixed form: stages A and B as int8-sliced products on the tensor cores
+//   stage A:  H^T[j][a] = sum_t G[j][t] W[aKey[a]][t],   G[j][t] = T[S[j] + t^2]
+//   stage B:  H2[p][u]  = sum_v Hf[a][u][v] W[pairB[p]][v]  for the pairs p of A key a
+// (Hf[a] is symmetric, so its rows serve as the K-major operand), and stage C
+// in its product form Q = H2 Wu^T with the FP64-level slicing.
+struct LatticeGRows {
+    const double* T;
+    const int* S;
+    __device__ double operator()(i64 r, int k) const { return T[S[r] + k * k]; }
+    __device__ i64 dest(i64 r) const { return r; }
+};
+
+struct ExpandedHRows {  // row r = a * U + u of the stacked Hf[a], batch a padded to whole tiles
+    const double* H;
+    const int* sidx;
+    i64 nS;
+    int U, blocks;
+    __device__ double operator()(i64 r, int k) const {
+        const i64 a = r / U, u = r % U;
+        return H[a * nS + sidx[u * U + k]];
+    }
+    __device__ i64 dest(i64 r) const { return (r / U) * blocks * TC_BM + r % U; }
+};
+
+struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
+    const double* W;
+    const int* pairA;
+    const int* pairB;
+    const int* first;  // first pair of each A key
+    const int* tile0;  // first tile of each A key
+    i64 Up;
+    __device__ double operator()(i64 p, int k) const { return W[(i64)pairB[p] * Up + k]; }
+    __device__ i64 dest(i64 p) const {
+        const int a = pairA[p];
+        return (i64)tile0[a] * TC_BN + (p - first[a]);
+    }
+};
+
+// One block: first pair, pair count and first tile of every A key (pairs are
+// ordered by A key), and the tile list of stage B (tiles of 64 pairs, each in
+// one A key); tiles past the last one get no columns.
+__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, int nP, int nA, int max_tiles,
+                                                      int* __restrict__ first, int* __restrict__ tile0,
+                                                      int* __restrict__ tile_batch, int* __restrict__ tile_col0,
+                                                      int* __restrict__ tile_ncols) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;
+    __syncthreads();
+    for (int base = 0; base < nA; base += blockDim.x) {
+        const int a = base + threadIdx.x;
+        int lo = 0, cnt = 0;
+        if (a < nA) {
+            int hi = nP;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (pairA[mid] < a) lo = mid + 1; else hi = mid;
+            }
+            int lo2 = lo, hi2 = nP;
+            while (lo2 < hi2) {
+                const int mid = (lo2 + hi2) >> 1;
+                if (pairA[mid] <= a) lo2 = mid + 1; else hi2 = mid;
+            }
+            cnt = lo2 - lo;
+        }
+        const int nt = (cnt + TC_BN - 1) / TC_BN;
+        // block exclusive scan of nt
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        int incl = nt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int ws = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            int wi = ws;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += v;
+            }
+            warp_sums[lane] = wi - ws;
+        }
+        __syncthreads();
+        const int t0 = carry + warp_sums[warp] + incl - nt;
+        if (a < nA) {
+            first[a] = lo;
+            tile0[a] = t0;
+            for (int k = 0; k < nt; ++k) {
+                tile_batch[t0 + k] = a;
+                tile_col0[t0 + k] = lo + k * TC_BN;
+                tile_ncols[t0 + k] = min(TC_BN, cnt - k * TC_BN);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = t0 + nt;
+        __syncthreads();
+    }
+}
+
+// G sliced once per table set (cached with the tables); the build synchronises
+// the stream so that the slices are ready for any stream that uses them later
+static TiledOperand lattice_g_slices(const LatticeTables& t, cudaStream_t s) {
+    std::lock_guard<std::mutex> lk(t.g_mu);
+    if (!t.g_sliced) {
+        auto g = std::make_unique<TiledTable>();
+        const int nkc = (int)((t.U + TC_BK - 1) / TC_BK);
+        const i64 rows = (t.nS + TC_BM - 1) / TC_BM * TC_BM;
+        g->data.alloc((size_t)MIXED_SLICES * rows * nkc * TC_BK);
+        g->e.alloc((size_t)rows);
+        g->view = TiledOperand{g->data.p, g->e.p, nkc, MIXED_SLICES};
+        k_slice_tiled<LatticeGRows><<<(unsigned)((t.nS * 32 + 255) / 256), 256, 0, s>>>(
+            LatticeGRows{t.T.p, t.S.p}, t.nS, (int)t.U, nkc, MIXED_SLICES, TC_BM, g->data.p, g->e.p);
+        GLI_CHECK_LAUNCH();
+        GLI_CUDA(cudaStreamSynchronize(s));
+        t.g_sliced = std::move(g);
+    }
+    return t.g_sliced->view;
+}
+
 void dgemm_strided(int M, int N, int K, const double* A, i64 asb, i64 ar, i64 ac, const double* B, i64 bsb, i64 br,
                    i64 bc, double* C, i64 csb, i64 cr, i64 cc, int batch, bool accumulate, cudaStream_t s);
 
@@ -352,13 +475,16 @@ struct StageTimer {
 
 void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
                           i64 m, double tol, int form, double* d_out, cudaStream_t s, ContractStats* stats) {
-    if (form != FORM_FP64) fail(GLI_ERR_ARGUMENT, "form %d is not available for the sparse evaluation", form);
+    if (form != FORM_FP64 && form != FORM_MIXED)
+        fail(GLI_ERR_ARGUMENT, "form %d is not a sparse evaluation form (0 = FP64, 1 = mixed)", form);
+    const bool mixed = form == FORM_MIXED;
     if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
     if (m == 0) return;
     StageTimer timer(t_timing, s);
     timer.mark();
     const std::shared_ptr<const LatticeTables> tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
     const LatticeTables& t = *tp;
+    const TiledOperand G = mixed ? lattice_g_slices(t, s) : TiledOperand{};
     timer.mark();
 
     ClassDecode d;
@@ -421,8 +547,26 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     if (nA * (i64)U * U > ((i64)1 << 31))
         fail(GLI_ERR_LIMIT, "stage buffers exceed 16 GB (%lld A keys, lattice extent %d)", (long long)nA, U);
     DevBuf<double> H(nA * (i64)nS, s);
+    DevBuf<int> tc_err;
+    if (mixed) {
+        tc_err.alloc(1, s);
+        tc_err.zero();
+    }
     timer.mark();
-    {
+    if (mixed) {
+        TiledSlices Wa;
+        const int nbt = (int)((nA + TC_BN - 1) / TC_BN);
+        Wa.alloc(nbt, TC_BN, U, MIXED_SLICES, s);
+        slice_tiled(GatheredRows{t.W.p, aKey.p, Up}, nA, U, Wa, s);
+        TileWork w;
+        w.a_rows = nS;
+        w.a_blocks = (int)((nS + TC_BM - 1) / TC_BM);
+        w.n_total = (int)nA;
+        w.C = H.p;
+        w.rs = 1;
+        w.cs = nS;
+        tc_gemm_tiled(G, Wa.view(), w, nbt, tc_err.p, s);
+    } else {
         // keys per thread: fewer when the problem is small, so that enough
         // warps exist to hide the table-gather latency
         const i64 outputs = nA * (i64)nS;
@@ -440,7 +584,35 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     GLI_CHECK_LAUNCH();
     timer.mark();
     DevBuf<double> H2(nP * (i64)Up, s);
-    {
+    if (mixed) {
+        const int mb = (U + TC_BM - 1) / TC_BM;
+        TiledSlices Hs, Wb;
+        Hs.alloc(nA * mb, TC_BM, U, MIXED_SLICES, s);
+        slice_tiled(ExpandedHRows{H.p, t.sidx.p, nS, U, mb}, nA * U, U, Hs, s);
+        const i64 max_tiles = nP / TC_BN + nA + 1;
+        DevBuf<int> grp(2 * nA + 3 * max_tiles, s);
+        int* first = grp.p;
+        int* tile0 = grp.p + nA;
+        int* tile_batch = grp.p + 2 * nA;
+        int* tile_col0 = tile_batch + max_tiles;
+        int* tile_ncols = tile_col0 + max_tiles;
+        k_pair_tiles<<<1, 1024, 0, s>>>(pairA.p, (int)nP, (int)nA, (int)max_tiles, first, tile0, tile_batch, tile_col0,
+                                        tile_ncols);
+        GLI_CHECK_LAUNCH();
+        Wb.alloc(max_tiles, TC_BN, U, MIXED_SLICES, s);
+        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, Up}, nP, U, Wb, s);
+        TileWork w;
+        w.a_rows = U;
+        w.a_blocks = mb;
+        w.a_batched = 1;
+        w.tile_batch = tile_batch;
+        w.tile_col0 = tile_col0;
+        w.tile_ncols = tile_ncols;
+        w.C = H2.p;
+        w.rs = 1;
+        w.cs = Up;
+        tc_gemm_tiled(Hs.view(), Wb.view(), w, (int)max_tiles, tc_err.p, s);
+    } else {
         DevBuf<double> Hf(nA * (i64)U * U, s);
         const Context& ctx = context();
         const i64 ework = nA * (i64)U * U;
@@ -454,7 +626,26 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
         GLI_CHECK_LAUNCH();
     }
     timer.mark();
-    if (nP * nku <= m) {
+    if (mixed && nP * nku <= m) {
+        // product form on the tensor cores (FP64-level slicing), then a gather
+        TiledSlices Hs2, Wus;
+        const i64 pb = (nP + TC_BM - 1) / TC_BM, kb2 = (nku + TC_BN - 1) / TC_BN;
+        Hs2.alloc(pb, TC_BM, U, FP64_SLICES, s);
+        slice_tiled(DenseRows{H2.p, Up}, nP, U, Hs2, s);
+        Wus.alloc(kb2, TC_BN, U, FP64_SLICES, s);
+        slice_tiled(GatheredRows{t.W.p, keyOf.p, Up}, nku, U, Wus, s);
+        DevBuf<double> Q(nP * nku, s);
+        TileWork w;
+        w.a_rows = (int)nP;
+        w.a_blocks = (int)pb;
+        w.n_total = (int)nku;
+        w.C = Q.p;
+        w.rs = nku;
+        w.cs = 1;
+        tc_gemm_tiled(Hs2.view(), Wus.view(), w, (int)kb2, tc_err.p, s);
+        k_gather_q<<<cb, 256, 0, s>>>(Q.p, cls.p, m, (int)nku, d_out);
+        GLI_CHECK_LAUNCH();
+    } else if (nP * nku <= m) {
         // product form: Q = H2 Wu^T over all (pair, used key), then a gather
         DevBuf<double> Wu(nku * (i64)Up, s), Q(nP * nku, s);
         k_gather_rows<<<(unsigned)((nku * Up + 255) / 256), 256, 0, s>>>(t.W.p, keyOf.p, (int)nku, Up, Wu.p);
@@ -470,6 +661,12 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
         GLI_CHECK_LAUNCH();
     }
     timer.mark();
+    if (mixed) {
+        int h_err = 0;
+        GLI_CUDA(cudaMemcpyAsync(&h_err, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        if (h_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired");
+    }
     ContractStats st;
     st.keys_a = nA;
     st.pairs = nP;

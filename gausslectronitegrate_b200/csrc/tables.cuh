@@ -1,8 +1,10 @@
 // Device-built lookup tables shared by the integral kernels.
 #pragma once
 #include <memory>
+#include <mutex>
 
 #include "gli_internal.cuh"
+#include "tc_gemm.cuh"
 
 namespace gli {
 
@@ -27,6 +29,13 @@ struct DevMem {
     DevMem& operator=(const DevMem&) = delete;
 };
 
+// a tiled sliced operand that lives as long as the tables it was made from
+struct TiledTable {
+    DevMem<int8_t> data;
+    DevMem<int> e;
+    TiledOperand view;
+};
+
 struct LatticeTables {
     int kind = 0;            // 0 = ERIDA, 1 = ERI
     int device = 0;
@@ -40,6 +49,9 @@ struct LatticeTables {
     DevMem<double> T;        // tlen
     DevMem<int> S;           // nS distinct s values, ascending
     DevMem<int> sidx;        // U x U: position of u^2 + v^2 in S
+    // the mixed form's stage-A operand G[j][t] = T[S[j] + t^2], sliced on first use
+    mutable std::mutex g_mu;
+    mutable std::unique_ptr<TiledTable> g_sliced;
 };
 
 // Builds P (ERIDA) or the shift-pair products (ERI) from the coefficients, masks

@@ -1,29 +1,149 @@
 // Sliced int8 tensor-core GEMM (tc_gemm.cu): FP64-accurate products on the
-// tcgen05 tensor cores, used by the mixed form of the integral stages.
+// tcgen05 tensor cores, used by the mixed form of the integral stages and by
+// the FP64-level GEMM entry point.
+//
+// An FP64 operand row x is split as  x = 2^e sum_{p<S} 2^(-7(p+1)) d_p  with
+// int8 slices d_p in [-64, 64] and one exponent e per row (|x| 2^-e < 1/2).
+// Operands are stored pre-tiled for the kernel: rows in blocks of RB (128 for
+// the A side, 64 for the B side), K in chunks of TC_BK = 64 bytes, and for each
+// (row block, K chunk) the S slices one after another, each an RB x 64 byte
+// tile in the tensor cores' K-major core-matrix order (8 rows x 16 bytes per
+// core matrix, core matrices along K first).  One (row block, K chunk) is thus
+// one contiguous run of S * RB * 64 bytes that a single bulk copy moves into
+// shared memory.
 #pragma once
 #include "gli_internal.cuh"
 
 namespace gli {
 
-// S int8 slices of `batches` row blocks of `rows` rows (one block's rows count),
-// K padded to Kp (multiple of 32), slice-major, one exponent per row
-struct SlicedMatrix {
-    DevBuf<int8_t> data;
-    DevBuf<int> e;
-    i64 rows = 0, Kp = 0, batches = 1;
-    int slices = 0;
-    i64 slice_stride() const { return rows * Kp * batches; }
+constexpr int MIXED_SLICES = 5;  // mixed form: products of slices p + q < 5 (~2^-36 per term)
+constexpr int FP64_SLICES = 7;   // FP64 level: products p + q < 8 (~2^-50 per term)
+constexpr int TC_BM = 128;       // A rows per tile (MMA M)
+constexpr int TC_BN = 64;        // B rows per tile (MMA N)
+constexpr int TC_BK = 64;        // K bytes per chunk (two MMAs of K = 32)
+
+__host__ __device__ inline i64 tiled_offset(i64 rb, int kc, int p, int r, int k, int nkc, int S, int RB) {
+    return ((rb * nkc + kc) * S + p) * (i64)RB * TC_BK + ((r >> 3) * (TC_BK / 16) + (k >> 4)) * 128 + (r & 7) * 16 +
+           (k & 15);
+}
+
+// device view of a tiled sliced operand; e[] is indexed by padded row
+// (row block * RB + row within the block)
+struct TiledOperand {
+    const int8_t* data = nullptr;
+    const int* e = nullptr;
+    int nkc = 0;  // K chunks (K padded to nkc * 64)
+    int S = 0;    // slices
 };
 
-// slice rows of an FP64 matrix (rows x K per batch, row stride ld, batch stride bs)
-// nslices = 5 (the mixed form: ~1e-9 Ha on the integral values) or 7 (FP64-level)
-void slice_rows(const double* src, i64 rows, int K, i64 ld, i64 bs, int batches, int nslices, SlicedMatrix& out,
-                cudaStream_t s);
+// stream-ordered owner
+struct TiledSlices {
+    DevBuf<int8_t> data;
+    DevBuf<int> e;
+    i64 blocks = 0;
+    int RB = 0, nkc = 0, S = 0;
+    void alloc(i64 row_blocks, int rb, int K, int nslices, cudaStream_t s) {
+        blocks = row_blocks;
+        RB = rb;
+        S = nslices;
+        nkc = (K + TC_BK - 1) / TC_BK;
+        data.alloc((size_t)(blocks * RB) * nkc * TC_BK * S, s);
+        e.alloc((size_t)(blocks * RB), s);
+    }
+    TiledOperand view() const { return TiledOperand{data.p, e.p, nkc, S}; }
+};
 
-// C[b] (+)= A[b] B[b]^T; ragged B batches via b_row0/b_rows and output column
-// offsets c_col0 (device arrays, or NULL for uniform batches)
-void tc_gemm_sliced(const SlicedMatrix& A, const SlicedMatrix& B, int n_max, double* C, i64 rs, i64 cs, i64 bs,
-                    int batches, const int* b_row0, const int* b_rows, const int* c_col0, bool accumulate,
-                    cudaStream_t s);
+// Writes the slices of source rows r = 0 .. rows-1 (src(r, k), k < K) to their
+// padded rows src.dest(r).  One warp per row, one 16-byte piece of K per lane
+// and pass.  Src: device functor with `double operator()(i64 r, int k) const`
+// and `i64 dest(i64 r) const`.
+template <class Src>
+__global__ void k_slice_tiled(Src src, i64 rows, int K, int nkc, int S, int RB, int8_t* __restrict__ dst,
+                              int* __restrict__ e) {
+    const i64 r = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    double mx = 0;
+    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(src(r, k)));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int ex = 0;
+    if (mx > 0) {
+        frexp(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
+        ex += 1;         // |x| 2^-ex < 1/2
+    }
+    const i64 pr = src.dest(r);
+    const i64 rb = pr / RB;
+    const int rr = (int)(pr % RB);
+    if (lane == 0) e[pr] = ex;
+    const int pieces = nkc * (TC_BK / 16);
+    for (int pc = lane; pc < pieces; pc += 32) {
+        double v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int k = pc * 16 + j;
+            v[j] = (k < K && mx > 0) ? ldexp(src(r, k), -ex) : 0.0;
+        }
+        const int kc = pc / (TC_BK / 16), k0 = (pc % (TC_BK / 16)) * 16;
+        for (int p = 0; p < S; ++p) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const double t = v[j] * 128.0;
+                const double d = rint(t);  // |t| <= 64
+                v[j] = t - d;              // exact in FP64, |v| <= 1/2
+                w[j >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (j & 3));
+            }
+            *reinterpret_cast<uint4*>(dst + tiled_offset(rb, kc, p, rr, k0, nkc, S, RB)) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+template <class Src>
+void slice_tiled(const Src& src, i64 rows, int K, TiledSlices& out, cudaStream_t s) {
+    if (rows <= 0) return;
+    k_slice_tiled<Src><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(src, rows, K, out.nkc, out.S, out.RB,
+                                                                          out.data.p, out.e.p);
+    GLI_CHECK_LAUNCH();
+}
+
+// source functors ----------------------------------------------------------------
+struct DenseRows {  // row r at src + r * ld
+    const double* src;
+    i64 ld;
+    __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
+    __device__ i64 dest(i64 r) const { return r; }
+};
+
+struct GatheredRows {  // row r at src + rowmap[r] * ld
+    const double* src;
+    const int* rowmap;
+    i64 ld;
+    __device__ double operator()(i64 r, int k) const { return src[(i64)rowmap[r] * ld + k]; }
+    __device__ i64 dest(i64 r) const { return r; }
+};
+
+// Work of one launch.  The A side has a_rows valid rows per batch in a_blocks
+// row blocks; batched A takes row block batch * a_blocks + m-tile, shared A
+// takes the m-tile.  The B side is a list of 64-row tiles (tiled row block t):
+// tile t belongs to batch tile_batch[t], its columns are tile_col0[t] ..
+// tile_col0[t] + tile_ncols[t] - 1 of the output (device arrays), or, with
+// tile_batch NULL, one batch whose tile t covers columns 64 t .. of n_total.
+// Output element (row i of the batch, column j) is C[i * rs + j * cs].
+struct TileWork {
+    int a_rows = 0, a_blocks = 0, a_batched = 0;
+    const int* tile_batch = nullptr;
+    const int* tile_col0 = nullptr;
+    const int* tile_ncols = nullptr;
+    int n_total = 0;
+    double* C = nullptr;
+    i64 rs = 0, cs = 0;
+};
+
+// launches the tensor-core GEMM over ntiles B tiles x a_blocks m-tiles; a CTA
+// that gives up waiting sets *d_err (with d_err NULL the call checks its own
+// flag and synchronises the stream)
+void tc_gemm_tiled(const TiledOperand& A, const TiledOperand& B, const TileWork& w, int ntiles, int* d_err,
+                   cudaStream_t s);
 
 }  // namespace gli
