@@ -10,8 +10,13 @@ the coefficients and the grid.
 One step = one evaluation of every class value from the class list already
 resident in HBM (tables, staged contraction, write-back), i.e. one
 gli_b200_sparse_values_dev call.  The class enumeration is measured apart.
+The metric compares the two forms: `value` is the chosen form (--form, default
+mixed: the bulk lattice stages as int8-sliced products on the tensor cores);
+the other form is timed the same way beside it, and the mixed form's max abs
+error against the FP64 form (and both against the reference C core) is
+reported in Hartree.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|mixed] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64] [--impl ours|reference]
 
 Timing: W >= 3 untimed warm-up steps; each timed step is bracketed by CUDA
 events on the stream the library launches on; L2 (126 MB) is flushed by
@@ -142,9 +147,10 @@ def cpu_baseline_main(gpu_values_path):
     idx = RefLib().enumerate("erida", spec)
     rate, sample, vals = cpu_reference_rate(b, spec, idx, TOL)
     gpu = np.load(gpu_values_path)
-    err = float(np.max(np.abs(vals - gpu)) / SPACING) if gpu.shape == vals.shape else None
+    errs = {f"max_abs_err_ha_gpu_{k}_vs_reference": float(np.max(np.abs(vals - gpu[k])) / SPACING)
+            for k in ("fp64", "mixed") if gpu[k].shape == vals.shape}
     print(json.dumps({"value": rate, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
-                      "sample": sample, "max_abs_err_ha_vs_gpu_fp64": err}))
+                      "sample": sample, **errs}))
     return 0
 
 
@@ -192,7 +198,9 @@ def run_ours(args):
     from gausslectronitegrate_b200 import _abi
     L = gli.lib()
     L.gli_b200_set_device(local)
-    form = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}[args.form]
+    FORMS = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}
+    chosen = args.form
+    other = "fp64" if chosen == "mixed" else "mixed"
     b = np.ascontiguousarray(g10())
     spec = grid_spec()
     gs = gli._grid_struct(spec)
@@ -224,81 +232,90 @@ def run_ours(args):
             raise RuntimeError(L.gli_b200_last_error_message().decode())
 
     log(f"{m} classes; accuracy check")
-    # accuracy of the chosen form against the FP64 form (max abs error in Ha)
-    step(_abi.GLI_FORM_FP64)
-    stream.synchronize()
-    ref64 = out.cpu().numpy().copy()
-    step(form)
-    stream.synchronize()
-    got = out.cpu().numpy().copy()
-    scale = 1.0 / SPACING
-    max_abs_err_ha = float(np.max(np.abs(got - ref64)) * scale)
+    vals = {}
+    for name, f in FORMS.items():
+        step(f)
+        stream.synchronize()
+        vals[name] = out.cpu().numpy().copy()
+    scale = 1.0 / SPACING  # grid units -> Hartree at this spacing
+    max_abs_err_ha = float(np.max(np.abs(vals["mixed"] - vals["fp64"])) * scale)
 
-    log("warm-up")
-    for _ in range(max(args.warmup, 3)):
-        step(form)
-    stream.synchronize()
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    launches0 = L.gli_b200_launch_count()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    t_wall = time.perf_counter()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            starts[k].record(stream)
-        step(form)
-        with torch.cuda.stream(stream):
-            ends[k].record(stream)
-    stream.synchronize()
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t_wall
-    clk = clocks.stop()
-    launches = L.gli_b200_launch_count() - launches0
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    my_ms = sum(step_ms)
-    t = torch.tensor([my_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if ws > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.barrier()
-    total_ms = float(t.item())
-    value = ws * m * args.steps / (total_ms * 1e-3)
+    def timed(name, steps, sample_clocks):
+        f = FORMS[name]
+        for _ in range(max(args.warmup, 3)):
+            step(f)
+        stream.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        clocks = Clocks(local) if sample_clocks else None
+        launches0 = L.gli_b200_launch_count()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        t_wall = time.perf_counter()
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # L2 flush between timed steps, outside the events
+                starts[k].record(stream)
+            step(f)
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_wall
+        clk = clocks.stop() if clocks else None
+        launches = L.gli_b200_launch_count() - launches0
+        my_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
+        t = torch.tensor([my_ms], dtype=torch.float64, device=f"cuda:{local}")
+        if ws > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            torch.distributed.barrier()
+        total_ms = float(t.item())
+        return {"value": ws * m * steps / (total_ms * 1e-3), "ms_per_step": total_ms / steps, "wall_s": wall,
+                "launches": launches, "clocks": clk}
+
+    log("timed steps")
+    main = timed(chosen, args.steps, True)
+    side = timed(other, args.steps, False)
 
     log("stage timing and FP64 peak probe")
-    # per-stage device times of one step (library events on the same stream)
-    L.gli_b200_set_timing(1)
-    step(form)
-    stream.synchronize()
-    ms4 = (C.c_float * 4)()
-    sz3 = (_abi.glong * 3)()
-    L.gli_b200_last_stage_times(ms4, sz3)
-    L.gli_b200_set_timing(0)
-    nA, nP, U = int(sz3[0]), int(sz3[1]), int(sz3[2])
-    flops_a = 2.0 * nA * U * U * U
+    # per-stage device times of one step (library events on the same stream;
+    # the first timed call warms the stream-ordered pool for the untimed path)
+    stage = {}
+    for name, f in FORMS.items():
+        L.gli_b200_set_timing(1)
+        for _ in range(2):
+            step(f)
+            stream.synchronize()
+        ms4 = (C.c_float * 4)()
+        sz3 = (_abi.glong * 3)()
+        L.gli_b200_last_stage_times(ms4, sz3)
+        L.gli_b200_set_timing(0)
+        stage[name] = {"tables": float(ms4[0]), "A": float(ms4[1]), "B": float(ms4[2]), "C": float(ms4[3]),
+                       "sizes": (int(sz3[0]), int(sz3[1]), int(sz3[2]))}
+    nA, nP, U = stage["fp64"]["sizes"]
     peak = C.c_double()
     L.gli_b200_measure_fp64_peak(C.byref(peak))
 
-    log("end-to-end through the C API")
-    # e2e: the reference-facing C call with host buffers (copies inside); the
-    # host class list comes from the reference-facing enumeration call
+    log("end-to-end through the C API (host buffers)")
+    # e2e: the C call with host buffers (host->device copy of the class list and
+    # device->host copy of the values inside the timed call); the host class
+    # list comes from the reference-facing enumeration call
     idx_s = _abi.SparseIndices()
     L.enumerate_symmetry_reduced_erida_indices(C.byref(gs), C.byref(idx_s))
     idx_np = np.ctypeslib.as_array(idx_s.indices, shape=(idx_s.num,)).copy()
     L.delete_sparse_erida_indices(C.byref(idx_s))
     gd, keep = gli._parse_coeffs(b, "")
+    host_vals = np.empty(m)
     e2e_times = []
-    for k in range(max(3, args.steps)):
-        res = _abi.SparseIntegrals()
+    for k in range(max(3, args.steps) + 1):
         t0 = time.perf_counter()
-        L.compute_sparse_erida_gausslet_integrals(C.byref(gd), C.byref(gs), idx_np.ctypes.data_as(_abi.lptr), m, TOL,
-                                                  C.byref(res))
-        vals = np.ctypeslib.as_array(res.integral_values, shape=(m,)).copy()
+        rc = L.gli_b200_sparse_values(_abi.GLI_KIND_ERIDA, C.byref(gd), C.byref(gs), idx_np.ctypes.data_as(_abi.lptr),
+                                      m, TOL, FORMS[chosen], host_vals.ctypes.data_as(_abi.dptr))
         e2e_times.append(time.perf_counter() - t0)
-        L.delete_sparse_erida_gausslet_integrals(C.byref(res))
-    e2e_s = statistics.median(e2e_times[1:]) if len(e2e_times) > 1 else e2e_times[0]
+        if rc:
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+    e2e_s = statistics.median(e2e_times[1:])
 
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -310,34 +327,38 @@ def run_ours(args):
     if not args.no_cpu_baseline:
         log("CPU baseline (reference core, separate process)")
         try:
-            tmp = tempfile.mktemp(suffix=".npy")
-            np.save(tmp, ref64)
+            tmp = tempfile.mktemp(suffix=".npz")
+            np.savez(tmp, fp64=vals["fp64"], mixed=vals["mixed"])
             cpu = cpu_baseline_subprocess(tmp)
             os.unlink(tmp)
         except Exception as ex:  # the reference core must be prebuilt (make -C oracle ref)
             cpu = {"value": None, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {ex}"}
-    ms_a = float(ms4[1])
-    achieved = flops_a / (ms_a * 1e-3) / 1e12 if ms_a > 0 else None
+    st = stage[chosen]
+    dom = max(("A", "B", "C"), key=lambda k: st[k])
+    roof = roofline(chosen, dom, st, nA, nP, U, m, peak.value)
     line = {
-        "metric": METRIC, "value": value, "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64",
+        "metric": METRIC, "value": main["value"], "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": main["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if chosen == "fp64" else "s8 tensor-core slices (int32 exact) + f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "classes": m, "form": args.form, "tol": TOL, "spacing_bohr": SPACING,
-                   "l2": "flushed between timed steps (256 MB write)", "max_abs_err_ha_vs_fp64": max_abs_err_ha,
-                   "enumeration_ms": enum_ms, "stage_ms": {"tables": float(ms4[0]), "A": ms_a, "B": float(ms4[2]),
-                                                          "C": float(ms4[3])},
+        "config": {"workload": WORKLOAD, "classes": m, "form": chosen, "tol": TOL, "spacing_bohr": SPACING,
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "max_abs_err_ha_mixed_vs_fp64": max_abs_err_ha,
+                   "forms": {chosen: {"classes_per_s": main["value"], "ms_per_step": main["ms_per_step"]},
+                             other: {"classes_per_s": side["value"], "ms_per_step": side["ms_per_step"]}},
+                   "mixed_over_fp64": (main["value"] / side["value"]) if chosen == "mixed" else
+                   (side["value"] / main["value"]),
+                   "enumeration_ms": enum_ms,
+                   "stage_ms": {k: {s_: v[s_] for s_ in ("tables", "A", "B", "C")} for k, v in stage.items()},
                    "stage_sizes": {"keys_A": nA, "key_pairs": nP, "lattice_U": U},
-                   "wall_s_timed_region": wall},
-        "roofline": {"bound": "fp64", "kernel": "k_stage_a", "achieved": achieved, "peak": peak.value,
-                     "unit": "TFLOP/s", "frac": (achieved / peak.value) if (achieved and peak.value) else None,
-                     "peak_source": "measured FP64 FMA probe on this device (gli_b200_measure_fp64_peak)",
-                     "algorithmic_flops_per_launch": flops_a, "traffic": None},
+                   "wall_s_timed_region": main["wall_s"]},
+        "roofline": roof,
         "e2e": {"value": m / e2e_s, "unit": "classes/s", "h2d_bytes_per_step": 8 * m + 8 * b.size,
                 "d2h_bytes_per_step": 8 * m},
-        "gpu_launches": launches,
-        "clocks": clk,
+        "gpu_launches": main["launches"],
+        "clocks": main["clocks"],
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -345,12 +366,61 @@ def run_ours(args):
     return 0
 
 
+def lattice_nS(U):
+    """number of distinct u^2 + v^2 with 0 <= u, v < U (rows of stage A)"""
+    u = np.arange(U, dtype=np.int64)
+    return int(np.unique((u[:, None] ** 2 + u[None, :] ** 2).ravel()).size)
+
+
+def roofline(form, dom, st, nA, nP, U, m, fp64_peak):
+    """Roofline entry of the dominant stage (from the library's stage events).
+    FP64 form: the stage's FP64 FLOPs against the measured FP64 FMA peak.  Mixed
+    form: the stage's sliced tensor-core work is bound by the bytes it must move
+    (FP64 sources, int8 slices written and read, FP64 results) against the
+    measured HBM bandwidth."""
+    ms = st[dom]
+    nS = lattice_nS(U)
+    kp = (U + 63) // 64 * 64
+    if form == "fp64":
+        flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U, "C": 2.0 * m * U}[dom]
+        achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
+        return {"bound": "fp64", "stage": dom,
+                "kernel": {"A": "k_stage_a", "B": "k_stage_b", "C": "k_stage_c"}[dom],
+                "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak if achieved and fp64_peak else None,
+                "peak_source": "measured FP64 FMA probe on this device (gli_b200_measure_fp64_peak)",
+                "algorithmic_flops_per_launch": flops, "traffic": None}
+    S, BN = 5, 96
+    nsp = (nS + 127) // 128 * 128
+    bytes_ = {"A": S * nsp * kp + S * ((nA + BN - 1) // BN * BN) * kp + 8 * nA * nS,
+              "B": 8.0 * nA * nS + 2 * S * nA * ((U + 127) // 128 * 128) * kp + 2 * S * nP * kp + 8 * nP * U,
+              "C": 8.0 * nP * U + 16 * m}[dom]
+    achieved = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
+    peak = measured_peaks()["hbm_gbs"]
+    return {"bound": "hbm", "stage": dom,
+            "kernel": {"A": "k_tc_gemm<5,5> (stage A)", "B": "k_slice_tiled + k_tc_gemm<5,5> (stage B)",
+                       "C": "k_stage_c"}[dom],
+            "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved and peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "algorithmic_bytes_per_launch": bytes_, "traffic": None}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--form", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-json", default=None, help=argparse.SUPPRESS)

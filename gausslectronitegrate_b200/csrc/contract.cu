@@ -20,7 +20,10 @@
 // combinations are few against the classes -- one small GEMM plus a gather.
 #include <math.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
+#include <list>
 #include <memory>
 
 #include "tables.cuh"
@@ -81,6 +84,14 @@ __device__ inline bool class_keys(const ClassDecode& d, i64 idx, i64 k[3]) {
     return true;
 }
 
+// counts of one evaluation, kept in device memory so that kernels can size their
+// work without a host round trip
+struct PlanCounts {
+    uint64_t key_total;  // used keys + used A keys (joint scan total)
+    uint64_t nP;         // distinct (A, B) key pairs
+    int64_t nku, nA;     // used keys, used A keys
+};
+
 // mark every key the class list uses (any role) and the A keys (k2)
 __global__ void k_mark_keys(ClassDecode d, const int64_t* __restrict__ idx, i64 m, uint32_t* __restrict__ usedKey,
                             uint32_t* __restrict__ usedA, int* __restrict__ bad) {
@@ -97,41 +108,48 @@ __global__ void k_mark_keys(ClassDecode d, const int64_t* __restrict__ idx, i64 
     usedA[k[1]] = 1;
 }
 
-// (A, B) pairs over the compacted key ids: slot = kid(k2) * nku + kid(k1)
+// After the joint scan of (usedKey | usedA): compact key id kid[k] = ids[k],
+// A id = ids[nk + k] - nku.  Records both inverse maps and the counts.
+__global__ void k_plan_keys(i64 nk, const uint32_t* __restrict__ used, const uint64_t* __restrict__ ids,
+                            int* __restrict__ keyOf, int* __restrict__ aId, int* __restrict__ aKey,
+                            PlanCounts* __restrict__ cnt) {
+    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nku = ids[nk];  // exclusive scan at nk = number of used keys
+    if (k == 0) {
+        cnt->nku = (int64_t)nku;
+        cnt->nA = (int64_t)(cnt->key_total - nku);
+    }
+    if (k >= nk) return;
+    if (used[k]) keyOf[ids[k]] = (int)k;
+    if (used[nk + k]) {
+        const int a = (int)(ids[nk + k] - nku);
+        aId[k] = a;
+        aKey[a] = (int)k;
+    }
+}
+
+// (A, B) pairs over the compacted key ids: slot = kid(k2) * stride + kid(k1)
 __global__ void k_mark_pairs(ClassDecode d, const int64_t* __restrict__ idx, i64 m, const uint64_t* __restrict__ kid,
-                             i64 nku, uint32_t* __restrict__ usedPair) {
+                             i64 stride, uint32_t* __restrict__ usedPair) {
     const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m) return;
     i64 k[3];
     if (!class_keys(d, idx[n], k)) return;
-    usedPair[(i64)kid[k[1]] * nku + (i64)kid[k[0]]] = 1;
+    usedPair[(i64)kid[k[1]] * stride + (i64)kid[k[0]]] = 1;
 }
 
-// ids of the second half of a joint scan, shifted back to start at 0
-__global__ void k_offset_ids(i64 n, const uint64_t* __restrict__ in, uint64_t base, uint64_t* __restrict__ out) {
-    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) out[k] = in[k] - base;
-}
-
-// compact id -> original key
-__global__ void k_key_of(i64 nkeys, const uint32_t* __restrict__ used, const uint64_t* __restrict__ id,
-                         int* __restrict__ keyOf) {
-    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < nkeys && used[k]) keyOf[id[k]] = (int)k;
-}
-
-__global__ void k_pair_lists(i64 nku, const uint32_t* __restrict__ usedPair, const uint64_t* __restrict__ pairId,
-                             const int* __restrict__ keyOf, const uint64_t* __restrict__ aId, int* __restrict__ pairA,
-                             int* __restrict__ pairB) {
+__global__ void k_pair_lists(i64 slots, i64 stride, const uint32_t* __restrict__ usedPair,
+                             const uint64_t* __restrict__ pairId, const int* __restrict__ keyOf,
+                             const int* __restrict__ aId, int* __restrict__ pairA, int* __restrict__ pairB) {
     const i64 slot = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= nku * nku || !usedPair[slot]) return;
-    const i64 ka = keyOf[slot / nku], kb = keyOf[slot % nku];
-    pairA[pairId[slot]] = (int)aId[ka];
+    if (slot >= slots || !usedPair[slot]) return;
+    const i64 ka = keyOf[slot / stride], kb = keyOf[slot % stride];
+    pairA[pairId[slot]] = aId[ka];
     pairB[pairId[slot]] = (int)kb;
 }
 
 __global__ void k_class_pairs(ClassDecode d, const int64_t* __restrict__ idx, i64 m, const uint64_t* __restrict__ kid,
-                              i64 nku, const uint64_t* __restrict__ pairId, int2* __restrict__ cls) {
+                              i64 stride, const uint64_t* __restrict__ pairId, int2* __restrict__ cls) {
     const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m) return;
     i64 k[3];
@@ -139,7 +157,7 @@ __global__ void k_class_pairs(ClassDecode d, const int64_t* __restrict__ idx, i6
         cls[n] = make_int2(-1, 0);
         return;
     }
-    cls[n] = make_int2((int)pairId[(i64)kid[k[1]] * nku + (i64)kid[k[0]]], (int)kid[k[2]]);
+    cls[n] = make_int2((int)pairId[(i64)kid[k[1]] * stride + (i64)kid[k[0]]], (int)kid[k[2]]);
 }
 
 // ---------------------------------------------------------------------------
@@ -158,11 +176,14 @@ constexpr int A_TC = 32;                  // t chunk
 template <int KT>
 __global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict__ W, const double* __restrict__ T,
                                                         const int* __restrict__ S, const int* __restrict__ aKey,
-                                                        int nA, int nS, int U, int Up, double* __restrict__ H) {
+                                                        const PlanCounts* __restrict__ cnt, int nS, int U, int Up,
+                                                        double* __restrict__ H) {
     __shared__ __align__(16) double ws[A_TC][KT];
     const int j0 = blockIdx.x * A_STILE + threadIdx.x;
     const int j1 = j0 + A_THREADS;
     const int a0 = blockIdx.y * KT;
+    const int nA = (int)cnt->nA;
+    if (a0 >= nA) return;  // grids are sized by a bound on nA
     const int s0 = j0 < nS ? S[j0] : 0;
     const int s1 = j1 < nS ? S[j1] : 0;
     double acc0[KT], acc1[KT];
@@ -210,10 +231,10 @@ constexpr int B_THREADS = 128;
 constexpr int B_PAIRS = 16;
 constexpr int B_VC = 64;                  // v chunk staged in shared memory
 
-__global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__ sidx, i64 nA, int nS, int U,
-                           double* __restrict__ Hf) {
+__global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__ sidx,
+                           const PlanCounts* __restrict__ cnt, int nS, int U, double* __restrict__ Hf) {
     const i64 plane = (i64)U * U;
-    const i64 total = nA * plane;
+    const i64 total = cnt->nA * plane;
     for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
         const i64 a = e / plane, vu = e % plane;
         Hf[e] = H[a * nS + sidx[vu]];
@@ -222,10 +243,13 @@ __global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__
 
 __global__ void __launch_bounds__(B_THREADS) k_stage_b(const double* __restrict__ W, const double* __restrict__ Hf,
                                                         const int* __restrict__ pairA, const int* __restrict__ pairB,
-                                                        int nP, int U, int Up, double* __restrict__ H2) {
+                                                        const PlanCounts* __restrict__ cnt, int U, int Up,
+                                                        double* __restrict__ H2) {
     __shared__ __align__(16) double wb[B_VC][B_PAIRS];
     __shared__ int range[2];
     const int a = blockIdx.x;
+    if (a >= cnt->nA) return;  // grids are sized by a bound on nA
+    const int nP = (int)cnt->nP;
     if (threadIdx.x == 0) {
         int lo = 0, hi = nP;  // first pair with pairA >= a
         while (lo < hi) {
@@ -300,10 +324,10 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
 
 // stage C as a product: Q[p][j] = sum_u H2[p][u] Wu[j][u] for every (pair, used key),
 // then a gather val[n] = Q[p(n)][j(n)].  Chosen when nP * nku is small against m.
-__global__ void k_gather_rows(const double* __restrict__ W, const int* __restrict__ keyOf, int nku, int Up,
-                              double* __restrict__ Wu) {
+__global__ void k_gather_rows(const double* __restrict__ W, const int* __restrict__ keyOf,
+                              const PlanCounts* __restrict__ cnt, int Up, double* __restrict__ Wu) {
     const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (i64)nku * Up) return;
+    if (e >= cnt->nku * Up) return;
     Wu[e] = W[(i64)keyOf[e / Up] * Up + e % Up];
 }
 
@@ -326,11 +350,23 @@ struct LatticeGRows {
     const int* S;
     __device__ double operator()(i64 r, int k) const { return T[S[r] + k * k]; }
     __device__ i64 dest(i64 r) const { return r; }
+    __device__ bool valid(i64) const { return true; }
+};
+
+struct AKeyRows {  // A key a: row W[aKey[a]]
+    const double* W;
+    const int* aKey;
+    const PlanCounts* cnt;
+    i64 Up;
+    __device__ double operator()(i64 a, int k) const { return W[(i64)aKey[a] * Up + k]; }
+    __device__ i64 dest(i64 a) const { return a; }
+    __device__ bool valid(i64 a) const { return a < cnt->nA; }
 };
 
 struct ExpandedHRows {  // row r = a * U + u of the stacked Hf[a], batch a padded to whole tiles
     const double* H;
     const int* sidx;
+    const PlanCounts* cnt;
     i64 nS;
     int U, blocks;
     __device__ double operator()(i64 r, int k) const {
@@ -338,6 +374,7 @@ struct ExpandedHRows {  // row r = a * U + u of the stacked Hf[a], batch a padde
         return H[a * nS + sidx[u * U + k]];
     }
     __device__ i64 dest(i64 r) const { return (r / U) * blocks * TC_BM + r % U; }
+    __device__ bool valid(i64 r) const { return r < cnt->nA * U; }
 };
 
 struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
@@ -346,29 +383,54 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
     const int* pairB;
     const int* first;  // first pair of each A key
     const int* tile0;  // first tile of each A key
+    const PlanCounts* cnt;
     i64 Up;
+    int bn;  // rows per tile
     __device__ double operator()(i64 p, int k) const { return W[(i64)pairB[p] * Up + k]; }
     __device__ i64 dest(i64 p) const {
         const int a = pairA[p];
-        return (i64)tile0[a] * TC_BN + (p - first[a]);
+        return (i64)tile0[a] * bn + (p - first[a]);
     }
+    __device__ bool valid(i64 p) const { return p < (i64)cnt->nP; }
+};
+
+// used key j: row W[keyOf[j]], for j below the used-key count in device memory
+struct UsedKeyRows {
+    const double* W;
+    const int* keyOf;
+    const PlanCounts* cnt;
+    i64 Up;
+    __device__ double operator()(i64 j, int k) const { return W[(i64)keyOf[j] * Up + k]; }
+    __device__ i64 dest(i64 j) const { return j; }
+    __device__ bool valid(i64 j) const { return j < cnt->nku; }
+};
+
+// dense rows whose count lives in device memory (PlanCounts::nP)
+struct PairCountedRows {
+    const double* src;
+    const PlanCounts* cnt;
+    i64 ld;
+    __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
+    __device__ i64 dest(i64 r) const { return r; }
+    __device__ bool valid(i64 r) const { return r < (i64)cnt->nP; }
 };
 
 // One block: first pair, pair count and first tile of every A key (pairs are
-// ordered by A key), and the tile list of stage B (tiles of 64 pairs, each in
+// ordered by A key), and the tile list of stage B (tiles of bn pairs, each in
 // one A key); tiles past the last one get no columns.
-__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, int nP, int nA, int max_tiles,
-                                                      int* __restrict__ first, int* __restrict__ tile0,
-                                                      int* __restrict__ tile_batch, int* __restrict__ tile_col0,
-                                                      int* __restrict__ tile_ncols) {
+__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, const PlanCounts* __restrict__ cnt,
+                                                      int bn, int max_tiles, int* __restrict__ first,
+                                                      int* __restrict__ tile0, int* __restrict__ tile_batch,
+                                                      int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
     __shared__ int warp_sums[32];
     __shared__ int carry;
+    const int nP = (int)cnt->nP, nA = (int)cnt->nA;
     if (threadIdx.x == 0) carry = 0;
     for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;
     __syncthreads();
     for (int base = 0; base < nA; base += blockDim.x) {
         const int a = base + threadIdx.x;
-        int lo = 0, cnt = 0;
+        int lo = 0, npairs = 0;
         if (a < nA) {
             int hi = nP;
             while (lo < hi) {
@@ -380,9 +442,9 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
                 const int mid = (lo2 + hi2) >> 1;
                 if (pairA[mid] <= a) lo2 = mid + 1; else hi2 = mid;
             }
-            cnt = lo2 - lo;
+            npairs = lo2 - lo;
         }
-        const int nt = (cnt + TC_BN - 1) / TC_BN;
+        const int nt = (npairs + bn - 1) / bn;
         // block exclusive scan of nt
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         int incl = nt;
@@ -408,8 +470,8 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
             tile0[a] = t0;
             for (int k = 0; k < nt; ++k) {
                 tile_batch[t0 + k] = a;
-                tile_col0[t0 + k] = lo + k * TC_BN;
-                tile_ncols[t0 + k] = min(TC_BN, cnt - k * TC_BN);
+                tile_col0[t0 + k] = lo + k * bn;
+                tile_ncols[t0 + k] = min(bn, npairs - k * bn);
             }
         }
         __syncthreads();
@@ -473,134 +535,158 @@ struct StageTimer {
     }
 };
 
-void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
-                          i64 m, double tol, int form, double* d_out, cudaStream_t s, ContractStats* stats) {
-    if (form != FORM_FP64 && form != FORM_MIXED)
-        fail(GLI_ERR_ARGUMENT, "form %d is not a sparse evaluation form (0 = FP64, 1 = mixed)", form);
-    const bool mixed = form == FORM_MIXED;
-    if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
-    if (m == 0) return;
-    StageTimer timer(t_timing, s);
-    timer.mark();
-    const std::shared_ptr<const LatticeTables> tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
-    const LatticeTables& t = *tp;
-    const TiledOperand G = mixed ? lattice_g_slices(t, s) : TiledOperand{};
-    timer.mark();
+// status of one evaluation, read back by the host after the last kernel
+struct EvalStatus {
+    PlanCounts cnt;
+    int bad;     // a class index outside the tensor
+    int tc_err;  // a tensor-core CTA gave up waiting
+};
 
+struct EvalArgs {
+    bool mixed = false;
+    const LatticeTables* t = nullptr;
+    TiledOperand G;
     ClassDecode d;
-    d.kind = kind;
-    d.N = g.points();
-    d.L = t.L;
-    for (int a = 0; a < 3; ++a) {
-        d.istart[a] = g.istart[a];
-        d.num[a] = g.num[a];
-    }
-    d.nkeys = t.nkeys;
-    const i64 nk = t.nkeys;
+    const int64_t* idx = nullptr;
+    i64 m = 0;
+    double* out = nullptr;
+    int num_sms = 148;
+};
+
+// Sizes that the host must know to allocate and launch: either bounds derived
+// from the key space (no host synchronisation: the whole evaluation can be
+// queued, and captured in a CUDA graph) or the exact counts (two host round
+// trips; used when the key space is too large for bounds to be cheap).
+struct EvalSizes {
+    i64 nku = 0, nA = 0, nP = 0;
+};
+
+// A key space of at most this many dense keys is planned with bounds: every
+// ERIDA grid up to 256 points per axis and ERI grids up to 5 points per axis
+// (135 keys).  Larger ERI key spaces (364 keys at 7 points) keep exact sizes:
+// their pair count is far below the bound, and the exact count selects the
+// product form of stage C.
+constexpr i64 BOUNDED_KEYS = 256;
+
+static void read_status(EvalStatus* d_st, EvalStatus& h, cudaStream_t s) {
+    GLI_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
+    GLI_CUDA(cudaStreamSynchronize(s));
+}
+
+// Queues one evaluation on stream s.  Kernels read the counts from st->cnt;
+// the host sizes buffers and grids by `sz`.
+static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
+                         cudaStream_t s) {
+    const LatticeTables& t = *a.t;
+    const i64 nk = t.nkeys, m = a.m;
+    const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
+    GLI_CUDA(cudaMemsetAsync(st, 0, sizeof(EvalStatus), s));
+    PlanCounts* cnt = &st->cnt;
     // usedKey and usedA side by side so that one scan serves both
     DevBuf<uint32_t> used(2 * nk, s);
     used.zero();
-    uint32_t* usedKey = used.p;
-    uint32_t* usedA = used.p + nk;
-    DevBuf<int> bad(1, s);
-    bad.zero();
     const unsigned cb = (unsigned)((m + 255) / 256);
     const unsigned kb = (unsigned)((nk + 255) / 256);
-    k_mark_keys<<<cb, 256, 0, s>>>(d, d_indices, m, usedKey, usedA, bad.p);
+    k_mark_keys<<<cb, 256, 0, s>>>(a.d, a.idx, m, used.p, used.p + nk, &st->bad);
     GLI_CHECK_LAUNCH();
     DevBuf<uint64_t> ids(2 * nk, s);
-    const i64 total = exclusive_scan_u32(used.p, ids.p, 2 * nk, s);
-    uint64_t nku_h = 0;
-    GLI_CUDA(cudaMemcpyAsync(&nku_h, ids.p + nk, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    int h_bad = 0;
-    GLI_CUDA(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    GLI_CUDA(cudaStreamSynchronize(s));
-    if (h_bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
-    const i64 nku = (i64)nku_h, nA = total - nku;
-    if (nku > 16384) fail(GLI_ERR_LIMIT, "class list uses %lld distinct axis keys (limit 16384)", (long long)nku);
-    const uint64_t* kid = ids.p;
-    // the A ids continue the key ids' numbering; offset them back to 0
-    DevBuf<uint64_t> aId(nk, s);
-    k_offset_ids<<<kb, 256, 0, s>>>(nk, ids.p + nk, (uint64_t)nku, aId.p);
+    exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
+    DevBuf<int> keyOf(nk, s), aId(nk, s), aKey(nk, s);
+    k_plan_keys<<<kb, 256, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
     GLI_CHECK_LAUNCH();
-
-    DevBuf<int> keyOf(nku, s), aKey(nA, s);
-    k_key_of<<<kb, 256, 0, s>>>(nk, usedKey, kid, keyOf.p);
-    GLI_CHECK_LAUNCH();
-    k_key_of<<<kb, 256, 0, s>>>(nk, usedA, aId.p, aKey.p);
-    GLI_CHECK_LAUNCH();
-    DevBuf<uint32_t> usedPair(nku * nku, s);
+    if (bounded) {
+        sz.nku = nk;
+        sz.nA = nk;
+    } else {
+        EvalStatus h;
+        read_status(st, h, s);
+        if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", t.kind ? "ERI" : "ERIDA");
+        sz.nku = h.cnt.nku;
+        sz.nA = h.cnt.nA;
+        if (sz.nku > 16384)
+            fail(GLI_ERR_LIMIT, "class list uses %lld distinct axis keys (limit 16384)", (long long)sz.nku);
+    }
+    const i64 stride = sz.nku, slots = sz.nku * sz.nku;
+    DevBuf<uint32_t> usedPair(slots, s);
     usedPair.zero();
-    k_mark_pairs<<<cb, 256, 0, s>>>(d, d_indices, m, kid, nku, usedPair.p);
+    k_mark_pairs<<<cb, 256, 0, s>>>(a.d, a.idx, m, ids.p, stride, usedPair.p);
     GLI_CHECK_LAUNCH();
-    DevBuf<uint64_t> pairId(nku * nku, s);
-    const i64 nP = exclusive_scan_u32(usedPair.p, pairId.p, nku * nku, s);
-    DevBuf<int> pairA(nP, s), pairB(nP, s);
-    k_pair_lists<<<(unsigned)((nku * nku + 255) / 256), 256, 0, s>>>(nku, usedPair.p, pairId.p, keyOf.p, aId.p,
-                                                                      pairA.p, pairB.p);
+    DevBuf<uint64_t> pairId(slots, s);
+    exclusive_scan_u32_dev(usedPair.p, pairId.p, slots, &cnt->nP, s);
+    if (bounded) {
+        // pairs (A, B) have kid(A) >= kid(B); every class has one pair
+        sz.nP = std::min(sz.nku * (sz.nku + 1) / 2, m);
+    } else {
+        EvalStatus h;
+        read_status(st, h, s);
+        sz.nP = (i64)h.cnt.nP;
+    }
+    DevBuf<int> pairA(sz.nP, s), pairB(sz.nP, s);
+    k_pair_lists<<<(unsigned)((slots + 255) / 256), 256, 0, s>>>(slots, stride, usedPair.p, pairId.p, keyOf.p, aId.p,
+                                                                  pairA.p, pairB.p);
     GLI_CHECK_LAUNCH();
     DevBuf<int2> cls(m, s);
-    k_class_pairs<<<cb, 256, 0, s>>>(d, d_indices, m, kid, nku, pairId.p, cls.p);
+    k_class_pairs<<<cb, 256, 0, s>>>(a.d, a.idx, m, ids.p, stride, pairId.p, cls.p);
     GLI_CHECK_LAUNCH();
 
-    const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
+    const i64 nA = sz.nA, nP = sz.nP, nku = sz.nku;
     if (nA * (i64)U * U > ((i64)1 << 31))
         fail(GLI_ERR_LIMIT, "stage buffers exceed 16 GB (%lld A keys, lattice extent %d)", (long long)nA, U);
     DevBuf<double> H(nA * (i64)nS, s);
-    DevBuf<int> tc_err;
-    if (mixed) {
-        tc_err.alloc(1, s);
-        tc_err.zero();
-    }
     timer.mark();
-    if (mixed) {
+    // ---- stage A
+    if (a.mixed) {
+        constexpr int BN = tile_n(MIXED_SLICES);
         TiledSlices Wa;
-        const int nbt = (int)((nA + TC_BN - 1) / TC_BN);
-        Wa.alloc(nbt, TC_BN, U, MIXED_SLICES, s);
-        slice_tiled(GatheredRows{t.W.p, aKey.p, Up}, nA, U, Wa, s);
+        const int nbt = (int)((nA + BN - 1) / BN);
+        Wa.alloc(nbt, BN, U, MIXED_SLICES, s);
+        slice_tiled(AKeyRows{t.W.p, aKey.p, cnt, Up}, nA, U, Wa, s);
         TileWork w;
         w.a_rows = nS;
-        w.a_blocks = (int)((nS + TC_BM - 1) / TC_BM);
+        w.a_blocks = (nS + TC_BM - 1) / TC_BM;
         w.n_total = (int)nA;
+        w.n_dev = &cnt->nA;
         w.C = H.p;
         w.rs = 1;
         w.cs = nS;
-        tc_gemm_tiled(G, Wa.view(), w, nbt, tc_err.p, s);
+        tc_gemm_tiled(a.G, Wa.view(), w, nbt, &st->tc_err, s);
     } else {
         // keys per thread: fewer when the problem is small, so that enough
         // warps exist to hide the table-gather latency
         const i64 outputs = nA * (i64)nS;
         const unsigned sb = (unsigned)((nS + A_STILE - 1) / A_STILE);
         if (outputs >= 4000000 && nA >= 32)
-            k_stage_a<32><<<dim3(sb, (unsigned)((nA + 31) / 32)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p,
-                                                                                    (int)nA, nS, U, Up, H.p);
+            k_stage_a<32><<<dim3(sb, (unsigned)((nA + 31) / 32)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt,
+                                                                                    nS, U, Up, H.p);
         else if (outputs >= 1000000)
-            k_stage_a<16><<<dim3(sb, (unsigned)((nA + 15) / 16)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p,
-                                                                                    (int)nA, nS, U, Up, H.p);
+            k_stage_a<16><<<dim3(sb, (unsigned)((nA + 15) / 16)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt,
+                                                                                    nS, U, Up, H.p);
         else
-            k_stage_a<4><<<dim3(sb, (unsigned)((nA + 3) / 4)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p,
-                                                                                 (int)nA, nS, U, Up, H.p);
+            k_stage_a<4><<<dim3(sb, (unsigned)((nA + 3) / 4)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt,
+                                                                                 nS, U, Up, H.p);
+        GLI_CHECK_LAUNCH();
     }
-    GLI_CHECK_LAUNCH();
     timer.mark();
+    // ---- stage B
     DevBuf<double> H2(nP * (i64)Up, s);
-    if (mixed) {
+    if (a.mixed) {
+        constexpr int BN = tile_n(MIXED_SLICES);
         const int mb = (U + TC_BM - 1) / TC_BM;
         TiledSlices Hs, Wb;
         Hs.alloc(nA * mb, TC_BM, U, MIXED_SLICES, s);
-        slice_tiled(ExpandedHRows{H.p, t.sidx.p, nS, U, mb}, nA * U, U, Hs, s);
-        const i64 max_tiles = nP / TC_BN + nA + 1;
+        slice_tiled(ExpandedHRows{H.p, t.sidx.p, cnt, nS, U, mb}, nA * U, U, Hs, s);
+        const i64 max_tiles = nP / BN + nA + 1;
         DevBuf<int> grp(2 * nA + 3 * max_tiles, s);
         int* first = grp.p;
         int* tile0 = grp.p + nA;
         int* tile_batch = grp.p + 2 * nA;
         int* tile_col0 = tile_batch + max_tiles;
         int* tile_ncols = tile_col0 + max_tiles;
-        k_pair_tiles<<<1, 1024, 0, s>>>(pairA.p, (int)nP, (int)nA, (int)max_tiles, first, tile0, tile_batch, tile_col0,
+        k_pair_tiles<<<1, 1024, 0, s>>>(pairA.p, cnt, BN, (int)max_tiles, first, tile0, tile_batch, tile_col0,
                                         tile_ncols);
         GLI_CHECK_LAUNCH();
-        Wb.alloc(max_tiles, TC_BN, U, MIXED_SLICES, s);
-        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, Up}, nP, U, Wb, s);
+        Wb.alloc(max_tiles, BN, U, MIXED_SLICES, s);
+        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, cnt, Up, BN}, nP, U, Wb, s);
         TileWork w;
         w.a_rows = U;
         w.a_blocks = mb;
@@ -611,68 +697,193 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
         w.C = H2.p;
         w.rs = 1;
         w.cs = Up;
-        tc_gemm_tiled(Hs.view(), Wb.view(), w, (int)max_tiles, tc_err.p, s);
+        tc_gemm_tiled(Hs.view(), Wb.view(), w, (int)max_tiles, &st->tc_err, s);
     } else {
         DevBuf<double> Hf(nA * (i64)U * U, s);
-        const Context& ctx = context();
         const i64 ework = nA * (i64)U * U;
-        const i64 eb = std::min<i64>((ework + 255) / 256, (i64)ctx.num_sms * 32);
-        k_expand_h<<<(unsigned)eb, 256, 0, s>>>(H.p, t.sidx.p, nA, nS, U, Hf.p);
+        const i64 eb = std::min<i64>((ework + 255) / 256, (i64)a.num_sms * 32);
+        k_expand_h<<<(unsigned)eb, 256, 0, s>>>(H.p, t.sidx.p, cnt, nS, U, Hf.p);
         GLI_CHECK_LAUNCH();
         // chunk slots per A key: at most nku pairs share one A key
         const unsigned chunks = (unsigned)((nku + B_PAIRS - 1) / B_PAIRS);
         k_stage_b<<<dim3((unsigned)nA, chunks, (unsigned)((U + B_THREADS - 1) / B_THREADS)), B_THREADS, 0, s>>>(
-            t.W.p, Hf.p, pairA.p, pairB.p, (int)nP, U, Up, H2.p);
+            t.W.p, Hf.p, pairA.p, pairB.p, cnt, U, Up, H2.p);
         GLI_CHECK_LAUNCH();
     }
     timer.mark();
-    if (mixed && nP * nku <= m) {
-        // product form on the tensor cores (FP64-level slicing), then a gather
-        TiledSlices Hs2, Wus;
-        const i64 pb = (nP + TC_BM - 1) / TC_BM, kb2 = (nku + TC_BN - 1) / TC_BN;
-        Hs2.alloc(pb, TC_BM, U, FP64_SLICES, s);
-        slice_tiled(DenseRows{H2.p, Up}, nP, U, Hs2, s);
-        Wus.alloc(kb2, TC_BN, U, FP64_SLICES, s);
-        slice_tiled(GatheredRows{t.W.p, keyOf.p, Up}, nku, U, Wus, s);
+    // ---- stage C: the product form computes every (pair, key) dot product --
+    // up to 16x more than the classes need on the tensor cores, as many as the
+    // classes in FP64 -- but as a GEMM it reuses each H2 row across keys instead
+    // of re-reading it per class; small class lists keep the per-class kernel
+    const bool product = a.mixed ? (m >= 65536 && nP * nku <= 16 * m) : (nP * nku <= m);
+    if (product) {
         DevBuf<double> Q(nP * nku, s);
-        TileWork w;
-        w.a_rows = (int)nP;
-        w.a_blocks = (int)pb;
-        w.n_total = (int)nku;
-        w.C = Q.p;
-        w.rs = nku;
-        w.cs = 1;
-        tc_gemm_tiled(Hs2.view(), Wus.view(), w, (int)kb2, tc_err.p, s);
-        k_gather_q<<<cb, 256, 0, s>>>(Q.p, cls.p, m, (int)nku, d_out);
-        GLI_CHECK_LAUNCH();
-    } else if (nP * nku <= m) {
-        // product form: Q = H2 Wu^T over all (pair, used key), then a gather
-        DevBuf<double> Wu(nku * (i64)Up, s), Q(nP * nku, s);
-        k_gather_rows<<<(unsigned)((nku * Up + 255) / 256), 256, 0, s>>>(t.W.p, keyOf.p, (int)nku, Up, Wu.p);
-        GLI_CHECK_LAUNCH();
-        dgemm_strided((int)nP, (int)nku, U, H2.p, 0, Up, 1, Wu.p, 0, 1, Up, Q.p, 0, nku, 1, 1, false, s);
-        k_gather_q<<<cb, 256, 0, s>>>(Q.p, cls.p, m, (int)nku, d_out);
+        if (a.mixed) {
+            constexpr int BN = tile_n(FP64_SLICES);
+            TiledSlices Hs2, Wus;
+            const i64 pb = (nP + TC_BM - 1) / TC_BM, kb2 = (nku + BN - 1) / BN;
+            Hs2.alloc(pb, TC_BM, U, FP64_SLICES, s);
+            slice_tiled(PairCountedRows{H2.p, cnt, Up}, nP, U, Hs2, s);
+            Wus.alloc(kb2, BN, U, FP64_SLICES, s);
+            slice_tiled(UsedKeyRows{t.W.p, keyOf.p, cnt, Up}, nku, U, Wus, s);
+            TileWork w;
+            w.a_rows = (int)nP;
+            w.a_blocks = (int)pb;
+            w.n_total = (int)nku;
+            w.C = Q.p;
+            w.rs = nku;
+            w.cs = 1;
+            tc_gemm_tiled(Hs2.view(), Wus.view(), w, (int)kb2, &st->tc_err, s);
+        } else {
+            DevBuf<double> Wu(nku * (i64)Up, s);
+            k_gather_rows<<<(unsigned)((nku * Up + 255) / 256), 256, 0, s>>>(t.W.p, keyOf.p, cnt, Up, Wu.p);
+            GLI_CHECK_LAUNCH();
+            dgemm_strided((int)nP, (int)nku, U, H2.p, 0, Up, 1, Wu.p, 0, 1, Up, Q.p, 0, nku, 1, 1, false, s);
+        }
+        k_gather_q<<<cb, 256, 0, s>>>(Q.p, cls.p, m, (int)nku, a.out);
         GLI_CHECK_LAUNCH();
     } else {
-        const Context& ctx = context();
         const i64 want = (m + 7) / 8;
-        const unsigned gc = (unsigned)(want < (i64)ctx.num_sms * 16 ? want : (i64)ctx.num_sms * 16);
-        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls.p, keyOf.p, m, U, Up, d_out);
+        const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
+        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls.p, keyOf.p, m, U, Up, a.out);
         GLI_CHECK_LAUNCH();
     }
     timer.mark();
-    if (mixed) {
-        int h_err = 0;
-        GLI_CUDA(cudaMemcpyAsync(&h_err, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-        GLI_CUDA(cudaStreamSynchronize(s));
-        if (h_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired");
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graphs of bounded evaluations.  A bounded evaluation issues no host
+// synchronisation, so the whole launch sequence (allocations, memsets and about
+// 15 kernels) is captured once and replayed: every replay recomputes everything
+// from the class list in device memory; only the launch overhead is saved.
+// A graph is keyed by what fixes its launch sequence and its pointers: the
+// table set (kept alive by the entry), the grid, the class-list pointer and
+// length, the output pointer and the form.
+struct GraphEntry {
+    const LatticeTables* tables = nullptr;
+    std::shared_ptr<const LatticeTables> keep;
+    int device = 0, mixed = 0;
+    const int64_t* idx = nullptr;
+    double* out = nullptr;
+    i64 m = 0;
+    i64 istart[3] = {}, num[3] = {};
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;  // kernels in the graph
+    DevMem<EvalStatus> status;
+    ~GraphEntry() {
+        if (exec) cudaGraphExecDestroy(exec);
     }
+};
+
+static thread_local std::list<std::unique_ptr<GraphEntry>> t_graphs;
+static constexpr size_t kGraphEntries = 8;
+static const bool g_graphs_enabled = getenv("GLI_B200_NO_GRAPHS") == nullptr;
+
+static GraphEntry* find_graph(const EvalArgs& a, int device) {
+    for (auto it = t_graphs.begin(); it != t_graphs.end(); ++it) {
+        GraphEntry& e = **it;
+        if (e.tables == a.t && e.device == device && e.mixed == (int)a.mixed && e.idx == a.idx && e.out == a.out &&
+            e.m == a.m && e.istart[0] == a.d.istart[0] && e.istart[1] == a.d.istart[1] &&
+            e.istart[2] == a.d.istart[2] && e.num[0] == a.d.num[0] && e.num[1] == a.d.num[1] &&
+            e.num[2] == a.d.num[2]) {
+            t_graphs.splice(t_graphs.begin(), t_graphs, it);  // most recently used first
+            return t_graphs.front().get();
+        }
+    }
+    return nullptr;
+}
+
+static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const LatticeTables>& tp, int device,
+                                 cudaStream_t s) {
+    auto e = std::make_unique<GraphEntry>();
+    e->tables = a.t;
+    e->keep = tp;
+    e->device = device;
+    e->mixed = a.mixed;
+    e->idx = a.idx;
+    e->out = a.out;
+    e->m = a.m;
+    for (int k = 0; k < 3; ++k) {
+        e->istart[k] = a.d.istart[k];
+        e->num[k] = a.d.num[k];
+    }
+    e->status.alloc(1);
+    tc_gemm_prepare();  // function attributes are set outside the capture
+    const long long l0 = launch_count();
+    GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+        StageTimer timer(false, s);
+        EvalSizes sz;
+        enqueue_eval(a, true, e->status.p, timer, sz, s);
+    } catch (...) {
+        cudaStreamEndCapture(s, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    GLI_CUDA(cudaStreamEndCapture(s, &graph));
+    e->launches = launch_count() - l0;
+    const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    GLI_CUDA(ie);
+    t_graphs.push_front(std::move(e));
+    while (t_graphs.size() > kGraphEntries) t_graphs.pop_back();
+    return t_graphs.front().get();
+}
+
+void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
+                          i64 m, double tol, int form, double* d_out, cudaStream_t s, ContractStats* stats) {
+    if (form != FORM_FP64 && form != FORM_MIXED)
+        fail(GLI_ERR_ARGUMENT, "form %d is not a sparse evaluation form (0 = FP64, 1 = mixed)", form);
+    if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
+    if (m == 0) return;
+    const Context& ctx = context();
+    StageTimer timer(t_timing, s);
+    timer.mark();
+    const std::shared_ptr<const LatticeTables> tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
+    const LatticeTables& t = *tp;
+    EvalArgs a;
+    a.mixed = form == FORM_MIXED;
+    a.t = &t;
+    if (a.mixed) a.G = lattice_g_slices(t, s);
+    timer.mark();
+    a.d.kind = kind;
+    a.d.N = g.points();
+    a.d.L = t.L;
+    for (int k = 0; k < 3; ++k) {
+        a.d.istart[k] = g.istart[k];
+        a.d.num[k] = g.num[k];
+    }
+    a.d.nkeys = t.nkeys;
+    a.idx = d_indices;
+    a.m = m;
+    a.out = d_out;
+    a.num_sms = ctx.num_sms;
+
+    const bool bounded = t.nkeys <= BOUNDED_KEYS;
+    EvalStatus h;
+    if (bounded && !t_timing && g_graphs_enabled) {
+        GraphEntry* e = find_graph(a, ctx.device);
+        if (!e) e = capture_graph(a, tp, ctx.device, s);
+        GLI_CUDA(cudaGraphLaunch(e->exec, s));
+        add_launches(e->launches);
+        read_status(e->status.p, h, s);
+    } else {
+        DevBuf<EvalStatus> st(1, s);
+        EvalSizes sz;
+        enqueue_eval(a, bounded, st.p, timer, sz, s);
+        read_status(st.p, h, s);
+    }
+    if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
+    if (h.tc_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired (code %d)", h.tc_err);
+    if (h.cnt.nku > 16384)
+        fail(GLI_ERR_LIMIT, "class list uses %lld distinct axis keys (limit 16384)", (long long)h.cnt.nku);
     ContractStats st;
-    st.keys_a = nA;
-    st.pairs = nP;
-    st.U = U;
+    st.keys_a = h.cnt.nA;
+    st.pairs = (i64)h.cnt.nP;
+    st.U = t.U;
     if (t_timing) {
-        GLI_CUDA(cudaStreamSynchronize(s));
         st.ms_tables = timer.between(0, 1);
         st.ms_a = timer.between(2, 3);
         st.ms_b = timer.between(3, 4);

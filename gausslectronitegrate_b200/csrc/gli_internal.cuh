@@ -92,7 +92,10 @@ struct DevBuf {
 };
 
 // exclusive prefix sum of 32-bit counts into 64-bit offsets; returns the total
+// (synchronises the stream)
 i64 exclusive_scan_u32(const uint32_t* d_in, uint64_t* d_out, i64 n, cudaStream_t s);
+// the same, total left in device memory at d_total (no synchronisation)
+void exclusive_scan_u32_dev(const uint32_t* d_in, uint64_t* d_out, i64 n, uint64_t* d_total, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // grids
@@ -166,6 +169,8 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
 // runtime.cu / contract.cu
 double fp64_probe_tflops();
 long long launch_count();
+// adds n kernels launched as part of a CUDA graph replay
+void add_launches(long long n);
 const char* last_message();
 int set_device(int ordinal);
 void set_timing(bool on);

@@ -41,6 +41,7 @@ const char* last_message() { return t_message; }
 static thread_local long long t_launches = 0;
 void count_launch() { ++t_launches; }
 long long launch_count() { return t_launches; }
+void add_launches(long long n) { t_launches += n; }
 
 int set_device(int ordinal) {
     t_device = ordinal;
@@ -213,6 +214,31 @@ i64 exclusive_scan_u32(const uint32_t* d_in, uint64_t* d_out, i64 n, cudaStream_
     GLI_CUDA(cudaMemcpyAsync(&total, tiles.p + ntiles, sizeof(total), cudaMemcpyDeviceToHost, s));
     GLI_CUDA(cudaStreamSynchronize(s));
     return (i64)total;
+}
+
+// the same scan with its total left in device memory (*d_total), no host sync
+__global__ void k_copy_total(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst) { *dst = *src; }
+
+void exclusive_scan_u32_dev(const uint32_t* d_in, uint64_t* d_out, i64 n, uint64_t* d_total, cudaStream_t s) {
+    if (n == 0) {
+        GLI_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), s));
+        return;
+    }
+    if (n <= SCAN_SMALL) {
+        scan_small<<<1, SCAN_BLOCK, 0, s>>>(d_in, n, d_out, d_total);
+        GLI_CHECK_LAUNCH();
+        return;
+    }
+    const i64 ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    DevBuf<uint64_t> tiles(ntiles + 1, s);
+    scan_tile_sums<<<(unsigned)ntiles, SCAN_BLOCK, 0, s>>>(d_in, n, tiles.p);
+    GLI_CHECK_LAUNCH();
+    scan_tile_offsets<<<1, SCAN_BLOCK, 0, s>>>(tiles.p, ntiles);
+    GLI_CHECK_LAUNCH();
+    scan_tiles_apply<<<(unsigned)ntiles, SCAN_BLOCK, 0, s>>>(d_in, n, tiles.p, d_out);
+    GLI_CHECK_LAUNCH();
+    k_copy_total<<<1, 1, 0, s>>>(tiles.p + ntiles, d_total);
+    GLI_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------

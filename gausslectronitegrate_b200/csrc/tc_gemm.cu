@@ -13,8 +13,9 @@
 // S = 5, R = 5 (about 2^-36 of max|a| max|b| per product term: the mixed form of
 // the integral stages) and S = 7, R = 8 (about 2^-50: FP64 level).
 //
-// One CTA computes a 128 x 64 tile of C with 128 threads:
-//   * warp 0 allocates 512 tensor-memory columns (R regions of 64 used);
+// One CTA computes a 128 x N tile of C (N = tile_n(S): 96 for S = 5, 64 for
+// S = 7) with 128 threads:
+//   * warp 0 allocates 512 tensor-memory columns (R regions of N used);
 //   * lane 0 of warp 0 is the producer: for every K chunk of 64 bytes it
 //     issues two bulk copies (all S slices of the A tile, all S slices of the B
 //     tile: one contiguous run each in the pre-tiled layout) into a ring of
@@ -30,6 +31,8 @@
 // tensor memory and returns.  The kernel uses no cluster and no multicast.
 #include <stdint.h>
 #include <stdlib.h>
+
+#include <atomic>
 
 #include "tc_gemm.cuh"
 
@@ -125,14 +128,16 @@ template <int S>
 __host__ __device__ constexpr int stages_for() { return S <= 5 ? 3 : 2; }
 
 template <int S>
-__host__ __device__ constexpr int smem_bytes() { return stages_for<S>() * S * (TC_BM + TC_BN) * TC_BK; }
+__host__ __device__ constexpr int smem_bytes() { return stages_for<S>() * S * (TC_BM + tile_n(S)) * TC_BK; }
 
 // first slice p of the pairs (p, q) with p + q = r, p, q < S
 __host__ __device__ constexpr int first_p(int r, int S) { return r < S ? 0 : r - (S - 1); }
 
 template <int S, int R>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand B, TileWork w, int* __restrict__ err) {
+    constexpr int TC_BN = tile_n(S);
     static_assert(R * TC_BN <= TC_TMEM_COLS, "tensor-memory regions exceed 512 columns");
+    static_assert(TC_BN % 16 == 0 && TC_BN >= 16 && TC_BN <= 256, "MMA N out of range for M = 128");
     static_assert(R <= 2 * S - 1, "more regions than slice pairs");
     constexpr int NST = stages_for<S>();
     constexpr uint32_t A_BYTES = S * TC_BM * TC_BK, B_BYTES = S * TC_BN * TC_BK;
@@ -146,7 +151,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand
     const int t = blockIdx.x, mt = blockIdx.y;
     const int batch = w.tile_batch ? w.tile_batch[t] : 0;
     const int col0 = w.tile_batch ? w.tile_col0[t] : t * TC_BN;
-    const int ncols = w.tile_batch ? w.tile_ncols[t] : min(TC_BN, w.n_total - t * TC_BN);
+    const int n_total = w.n_dev ? (int)*w.n_dev : w.n_total;
+    const int ncols = w.tile_batch ? w.tile_ncols[t] : min(TC_BN, n_total - t * TC_BN);
     const int rows_valid = min(TC_BM, w.a_rows - mt * TC_BM);
     if (ncols <= 0 || rows_valid <= 0) return;  // uniform across the CTA
     const i64 a_rb = w.a_batched ? (i64)batch * w.a_blocks + mt : mt;
@@ -263,11 +269,23 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand
 }
 
 // host ---------------------------------------------------------------------------
+static std::atomic<unsigned> g_prepared_devices{0};  // bit d: attributes set on device d
+
+void tc_gemm_prepare() {
+    int dev = 0;
+    GLI_CUDA(cudaGetDevice(&dev));
+    if (dev < 32 && (g_prepared_devices.load() >> dev) & 1u) return;
+    GLI_CUDA(cudaFuncSetAttribute(k_tc_gemm<MIXED_SLICES, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem_bytes<MIXED_SLICES>()));
+    GLI_CUDA(cudaFuncSetAttribute(k_tc_gemm<FP64_SLICES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem_bytes<FP64_SLICES>()));
+    if (dev < 32) g_prepared_devices.fetch_or(1u << dev);
+}
+
 template <int S, int R>
 static void launch_variant(const TiledOperand& A, const TiledOperand& B, const TileWork& w, int ntiles, int* err,
                            cudaStream_t s) {
     constexpr int smem = smem_bytes<S>();
-    GLI_CUDA(cudaFuncSetAttribute(k_tc_gemm<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     dim3 grid((unsigned)ntiles, (unsigned)w.a_blocks);
     k_tc_gemm<S, R><<<grid, 128, smem, s>>>(A, B, w, err);
     GLI_CHECK_LAUNCH();
@@ -280,6 +298,7 @@ void tc_gemm_tiled(const TiledOperand& A, const TiledOperand& B, const TileWork&
     if (A.S != B.S) fail(GLI_ERR_INTERNAL, "sliced GEMM operands disagree on the slice count");
     if (A.nkc <= 0 || A.nkc * TC_BK > 8192) fail(GLI_ERR_LIMIT, "sliced tensor-core GEMM supports 1 <= K <= 8192");
     if (w.a_blocks > 65535) fail(GLI_ERR_LIMIT, "sliced tensor-core GEMM: more than 65535 row tiles");
+    tc_gemm_prepare();
     DevBuf<int> own;
     int* err = d_err;
     if (!err) {
@@ -318,10 +337,11 @@ extern "C" int gli_b200_dgemm_sliced_dev(const double* d_A, glong lda, const dou
         if (K > 8192) gli::fail(GLI_ERR_LIMIT, "K above 8192");
         if (M > (glong)65535 * gli::TC_BM || N > ((glong)1 << 30)) gli::fail(GLI_ERR_LIMIT, "matrix too large");
         cudaStream_t s = stream ? (cudaStream_t)stream : gli::context().stream;
-        const gli::i64 mb = (M + gli::TC_BM - 1) / gli::TC_BM, nb = (N + gli::TC_BN - 1) / gli::TC_BN;
+        constexpr int BN = gli::tile_n(gli::FP64_SLICES);
+        const gli::i64 mb = (M + gli::TC_BM - 1) / gli::TC_BM, nb = (N + BN - 1) / BN;
         gli::TiledSlices As, Bs;
         As.alloc(mb, gli::TC_BM, (int)K, gli::FP64_SLICES, s);
-        Bs.alloc(nb, gli::TC_BN, (int)K, gli::FP64_SLICES, s);
+        Bs.alloc(nb, BN, (int)K, gli::FP64_SLICES, s);
         gli::slice_tiled(gli::DenseRows{d_A, lda}, M, (int)K, As, s);
         gli::slice_tiled(gli::DenseRows{d_B, ldb}, N, (int)K, Bs, s);
         gli::TileWork w;

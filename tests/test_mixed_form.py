@@ -56,6 +56,14 @@ def test_mixed_eri_against_reference(gli, L, tol):
     _check(s.values, c[f"eri_val_{L}_{tol:g}"], f"mixed ERI {L}^3 tol {tol:g}")
 
 
+def test_mixed_eri_5_tight_against_fp64_form(gli):
+    # tol 1e-16 on 5^3: 138,187 classes, enough for the product form of the
+    # last stage on the tensor cores, with key-count bounds above the counts
+    fp = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(5), 1e-16)
+    mx = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(5), 1e-16, form="mixed")
+    _check(mx.values, fp.values, "mixed ERI 5^3 tol 1e-16")
+
+
 def test_mixed_eri_7_against_fp64_form(gli):
     fp = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(7), 1e-10)
     mx = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(7), 1e-10, form="mixed")
