@@ -67,6 +67,26 @@ def grid_spec():
     return [(-(L_GRID // 2), L_GRID)] * 3
 
 
+def h_chain_batch(rng, count, edge_lo, edge_hi, spacing):
+    """Synthetic batch of linear H_n chains (the batched-nuclear workload):
+    n uniform in 2..8, bond lengths uniform in 1.0-3.0 bohr, every nucleus
+    jittered by N(0, 0.1) bohr, chain along x centred on the origin; grid edge
+    uniform in edge_lo..edge_hi points, centred, at `spacing` bohr.  Positions
+    are returned in grid units (bohr / spacing)."""
+    grids, positions, charges = [], [], []
+    for _ in range(count):
+        n = int(rng.integers(2, 9))
+        bonds = rng.uniform(1.0, 3.0, size=n - 1)
+        x = np.concatenate([[0.0], np.cumsum(bonds)])
+        x -= x.mean()
+        pos = np.stack([x, np.zeros(n), np.zeros(n)], axis=1) + rng.normal(0.0, 0.1, size=(n, 3))
+        edge = int(rng.integers(edge_lo, edge_hi + 1))
+        grids.append([(-(edge // 2), edge)] * 3)
+        positions.append(pos / spacing)
+        charges.append([1] * n)
+    return grids, positions, charges
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -282,6 +282,41 @@ def compute_nuclear_gausslet_integrals(gausslet_coeffs, grid, nuclear_positions,
     return res
 
 
+def compute_nuclear_gausslet_integrals_batch(gausslet_coeffs, grids, nuclear_positions, nuclear_charges, tol,
+                                             form="fp64"):
+    """Nuclear matrices of many instances in one call (extension: no
+    counterpart in the reference module).  grids[k], nuclear_positions[k] and
+    nuclear_charges[k] describe instance k exactly as for
+    compute_nuclear_gausslet_integrals; all instances share the coefficients and
+    tol.  form "fp64" (the reference's arithmetic) or "mixed" (tensor-core
+    contractions, about 1e-9 relative).  Returns a list of N_k x N_k arrays."""
+    syntax = ("compute_nuclear_gausslet_integrals_batch(gausslet_coeffs, grids, nuclear_positions, "
+              "nuclear_charges, tol, form='fp64')")
+    g, keep = _parse_coeffs(gausslet_coeffs, syntax)
+    if form not in _FORMS:
+        raise ValueError(f"'form' must be one of {sorted(_FORMS)}; syntax: {syntax}")
+    if not (len(grids) == len(nuclear_positions) == len(nuclear_charges)):
+        raise ValueError(f"grids, positions and charges must have one entry per instance; syntax: {syntax}")
+    n = len(grids)
+    if n == 0:
+        return []
+    specs = [_parse_grid(gr, syntax) for gr in grids]
+    gstructs = (_abi.Grid * n)(*[_grid_struct(sp) for sp in specs])
+    nucs, offsets = [], [0]
+    for pos, q in zip(nuclear_positions, nuclear_charges):
+        arr, cnt = _parse_nuclei(pos, q, syntax)
+        nucs.extend(arr[k] for k in range(cnt))
+        offsets.append(offsets[-1] + cnt)
+    nuc_arr = (_abi.Nucleus * len(nucs))(*nucs)
+    off = np.asarray(offsets, dtype=np.int64)
+    outs = [np.empty((sp[0][1] * sp[1][1] * sp[2][1],) * 2) for sp in specs]
+    ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+    lib().gli_b200_nuclear_batch(C.byref(g), n, gstructs, off.ctypes.data_as(_abi.lptr), nuc_arr,
+                                 _parse_tol(tol, syntax), _FORMS[form], ptrs)
+    _raise_if_failed(syntax)
+    return outs
+
+
 # ---------------------------------------------------------------------------
 # sparse ERI / ERIDA objects (python/pymodule.c:606-1108, 1334-1826)
 

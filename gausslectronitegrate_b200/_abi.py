@@ -77,6 +77,8 @@ EXPORTS = [
     "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
     "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_measure_fp64_peak",
     "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
+    "gli_b200_nuclear_batch_dev", "gli_b200_nuclear_batch", "gli_b200_last_nuclear_batch", "gli_b200_autotune_report",
+    "gli_b200_autotune_selftest",
 ]
 
 
@@ -132,4 +134,15 @@ def load(path=LIB_PATH):
     L.gli_b200_dgemm_sliced_dev.argtypes = [C.c_void_p, glong, C.c_void_p, glong, C.c_void_p, glong, glong, glong, glong,
                                             C.c_void_p]
     L.gli_b200_dgemm_sliced_dev.restype = C.c_int
+    L.gli_b200_nuclear_batch_dev.argtypes = [P(GaussletData), glong, P(Grid), lptr, P(Nucleus), C.c_double, C.c_int,
+                                             P(C.c_void_p), C.c_void_p]
+    L.gli_b200_nuclear_batch_dev.restype = C.c_int
+    L.gli_b200_nuclear_batch.argtypes = [P(GaussletData), glong, P(Grid), lptr, P(Nucleus), C.c_double, C.c_int,
+                                         P(C.c_void_p)]
+    L.gli_b200_nuclear_batch.restype = C.c_int
+    L.gli_b200_last_nuclear_batch.argtypes = [P(glong)]
+    L.gli_b200_last_nuclear_batch.restype = None
+    L.gli_b200_autotune_report.argtypes = [C.c_char_p, glong]
+    L.gli_b200_autotune_report.restype = glong
+    L.gli_b200_autotune_selftest.restype = C.c_int
     return L

@@ -620,6 +620,73 @@ int gli_b200_sparse_values_dev(int kind, const double* coeffs, glong num_coeffs,
     return gli::last_error();
 }
 
+// Batched nuclear-attraction matrices: every instance its own grid and nuclei
+// (same coefficients and tol), outputs in device memory.  Batches the matrix
+// entry point compute_nuclear_gausslet_integrals (reference
+// src/nuclear_integrals.c:133-266).
+int gli_b200_nuclear_batch_dev(const struct gausslet_data* gdata, glong num_instances,
+                               const struct cartesian_grid_3d* grids, const glong* nuclei_offsets,
+                               const struct atomic_nucleus* nuclei, double tol, int form, double* const* d_out,
+                               void* stream) {
+    guarded([&] {
+        check_gdata(gdata);
+        if (num_instances < 0) gli::fail(GLI_ERR_ARGUMENT, "num_instances must be non-negative");
+        if (num_instances == 0) return;
+        if (!grids || !nuclei_offsets || !nuclei || !d_out) gli::fail(GLI_ERR_ARGUMENT, "batch arrays missing");
+        std::vector<gli::NuclearJob> jobs((size_t)num_instances);
+        for (glong k = 0; k < num_instances; ++k) {
+            const gli::GridDesc g = gli::grid_desc(&grids[k]);
+            for (int a = 0; a < 3; ++a)
+                for (i64 c = 0; c < g.num[a]; ++c) jobs[k].axes[a].push_back((int)(g.istart[a] + c));
+            const glong n0 = nuclei_offsets[k], n1 = nuclei_offsets[k + 1];
+            if (n1 <= n0) gli::fail(GLI_ERR_ARGUMENT, "instance %lld has no nuclei", (long long)k);
+            jobs[k].nuclei = nuclei + n0;
+            jobs[k].nn = (int)(n1 - n0);
+            jobs[k].d_out = d_out[k];
+        }
+        gli::Context& ctx = gli::context();
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx.stream;
+        gli::nuclear_batch_device(gdata->coefficients, gdata->indices.num, jobs, tol, form, s);
+    });
+    return gli::last_error();
+}
+
+// The same batch with host outputs: h_out[k] receives instance k's N_k x N_k
+// matrix (the device copies are made and released inside the call).
+int gli_b200_nuclear_batch(const struct gausslet_data* gdata, glong num_instances,
+                           const struct cartesian_grid_3d* grids, const glong* nuclei_offsets,
+                           const struct atomic_nucleus* nuclei, double tol, int form, double* const* h_out) {
+    guarded([&] {
+        if (num_instances <= 0) return;
+        if (!grids || !h_out) gli::fail(GLI_ERR_ARGUMENT, "batch arrays missing");
+        gli::Context& ctx = gli::context();
+        cudaStream_t s = ctx.stream;
+        std::vector<DevBuf<double>> dev((size_t)num_instances);
+        std::vector<double*> dptr((size_t)num_instances);
+        std::vector<i64> n2((size_t)num_instances);
+        for (glong k = 0; k < num_instances; ++k) {
+            const gli::GridDesc g = gli::grid_desc(&grids[k]);
+            n2[k] = g.points() * g.points();
+            dev[k].alloc(n2[k], s);
+            dptr[k] = dev[k].p;
+        }
+        if (gli_b200_nuclear_batch_dev(gdata, num_instances, grids, nuclei_offsets, nuclei, tol, form, dptr.data(),
+                                       s) != GLI_OK)
+            throw gli::Failure{gli::last_error()};
+        for (glong k = 0; k < num_instances; ++k) to_host(h_out[k], dev[k].p, n2[k], s);
+        GLI_CUDA(cudaStreamSynchronize(s));
+    });
+    return gli::last_error();
+}
+
+// instances, graph chunks and contraction streams of the last nuclear batch
+void gli_b200_last_nuclear_batch(glong out[3]) {
+    const gli::NuclearBatchStats& st = gli::last_nuclear_stats();
+    out[0] = st.instances;
+    out[1] = st.chunks;
+    out[2] = st.streams;
+}
+
 int gli_b200_sparse_values(int kind, const struct gausslet_data* gdata, const struct cartesian_grid_3d* grid,
                            const glong* indices, glong num, double tol, int form, double* values) {
     guarded([&] {

@@ -7,7 +7,9 @@
 //   enumerate.cu  symmetry-reduced ERI / ERIDA class enumeration (bit-exact)
 //   contract.cu   the staged lattice contraction that evaluates every class
 //   kinetic.cu    dense kinetic matrix
-//   nuclear.cu    nuclear-attraction matrix (field + staged contraction)
+//   nuclear.cu    nuclear-attraction matrices (field + staged contraction), batches
+//   tc_gemm.cu    int8-sliced tcgen05 GEMM (mixed form, FP64-level products)
+//   autotune.cu   launch-configuration autotuner (host)
 //   dense.cu      sparse -> dense expansion, ERI apply, projections
 //   capi.cu       the extern "C" entry points (reference API + extensions)
 #pragma once
@@ -156,6 +158,23 @@ void factors_device(const double* d_b, int nb, int L, double* d_F, cudaStream_t 
 // nuclear.cu: dense nuclear matrix over the product of three axis coordinate lists
 void nuclear_matrix_device(const double* h_coeffs, i64 nb, const std::vector<int> axes[3],
                            const struct atomic_nucleus* nuclei, int nn, double tol, double* d_out, cudaStream_t s);
+
+// one instance of a nuclear batch: ascending coordinate lists per axis, its
+// nuclei (host memory) and its N x N output (device memory)
+struct NuclearJob {
+    std::vector<int> axes[3];
+    const struct atomic_nucleus* nuclei = nullptr;
+    int nn = 0;
+    double* d_out = nullptr;
+};
+struct NuclearBatchStats {
+    i64 instances = 0, chunks = 0;
+    int streams = 0;
+};
+// every instance's matrix, one graph per chunk of instances; form FP64 or mixed
+void nuclear_batch_device(const double* h_coeffs, i64 nb, const std::vector<NuclearJob>& jobs, double tol, int form,
+                          cudaStream_t s);
+const NuclearBatchStats& last_nuclear_stats();
 
 // dense.cu
 void fill_dense_device(int kind, const GridDesc& sparse, const int64_t* d_idx, const double* d_val, i64 m,

@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand
     const i64 a_rb = w.a_batched ? (i64)batch * w.a_blocks + mt : mt;
     const int nkc = A.nkc;
     const int8_t* gA = A.data + a_rb * nkc * (i64)A_BYTES;
-    const int8_t* gB = B.data + (i64)t * nkc * (i64)B_BYTES;
+    const i64 b_rb = w.tile_bblock ? w.tile_bblock[t] : t;
+    const int8_t* gB = B.data + b_rb * nkc * (i64)B_BYTES;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand
         const bool live = row < rows_valid;
         const int ea = live ? A.e[a_rb * TC_BM + row] : 0;
         double* crow = w.C + (i64)(mt * TC_BM + row) * w.rs;
-        const int* eb = B.e + (i64)t * TC_BN;
+        const int* eb = B.e + b_rb * TC_BN;
         for (int c0 = 0; c0 < TC_BN; c0 += 16) {
             double acc[16];
 #pragma unroll

@@ -157,6 +157,7 @@ struct TileWork {
     const int* tile_batch = nullptr;
     const int* tile_col0 = nullptr;
     const int* tile_ncols = nullptr;
+    const int* tile_bblock = nullptr;  // B row block of tile t (default t: every tile its own rows)
     int n_total = 0;
     const int64_t* n_dev = nullptr;
     double* C = nullptr;

@@ -279,6 +279,39 @@ int gli_b200_sparse_values(int kind, const struct gausslet_data* gdata,
 	const struct cartesian_grid_3d* grid, const glong* indices, glong num,
 	double tol, int form, double* values);
 
+/* Batched nuclear-attraction matrices on one device.  Instance k has grid
+ * grids[k] (any box), nuclei nuclei[nuclei_offsets[k] .. nuclei_offsets[k+1])
+ * and writes its N_k x N_k row-major matrix to the device buffer d_out[k];
+ * all instances share the coefficients and tol.  form GLI_FORM_FP64 is the
+ * reference's arithmetic; GLI_FORM_MIXED runs the three lattice contractions
+ * as int8-sliced tensor-core products (about 1e-9 relative).  Each chunk of
+ * instances is one CUDA graph launch; the number of concurrent instance
+ * pipelines is chosen by the autotuner.  Batches the reference's
+ * compute_nuclear_gausslet_integrals (include/nuclear_integrals.h:40-43,
+ * src/nuclear_integrals.c:133-266). */
+int gli_b200_nuclear_batch_dev(const struct gausslet_data* gdata, glong num_instances,
+	const struct cartesian_grid_3d* grids, const glong* nuclei_offsets,
+	const struct atomic_nucleus* nuclei, double tol, int form, double* const* d_out,
+	void* stream);
+
+/* The same batch with host outputs: h_out[k] (N_k x N_k doubles, caller
+ * memory) receives instance k's matrix. */
+int gli_b200_nuclear_batch(const struct gausslet_data* gdata, glong num_instances,
+	const struct cartesian_grid_3d* grids, const glong* nuclei_offsets,
+	const struct atomic_nucleus* nuclei, double tol, int form, double* const* h_out);
+
+/* instances, graph chunks and concurrent instance pipelines of the calling
+ * thread's last nuclear batch (no reference counterpart) */
+void gli_b200_last_nuclear_batch(glong out[3]);
+
+/* The autotuner's decisions as JSON (truncated to len bytes including the
+ * terminating zero); returns the full length.  No reference counterpart. */
+glong gli_b200_autotune_report(char* buf, glong len);
+
+/* Checks the autotuner's selection logic on a synthetic cost model, without a
+ * device; 0 on success.  No reference counterpart. */
+int gli_b200_autotune_selftest(void);
+
 /* Symmetry-reduced class list of kind 0/1 into device memory (reference
  * src/eri_integrals.c:382-526, src/erida_integrals.c:300-410).  *d_indices is
  * allocated with cudaMallocAsync on stream; release with gli_b200_free_dev. */
@@ -294,6 +327,20 @@ int gli_b200_set_timing(int enable);
 /* Measured FP64 FMA throughput of the current device (TFLOP/s), from a
  * compute-only probe kernel; the denominator of the FP64 roofline. */
 int gli_b200_measure_fp64_peak(double* tflops);
+
+/* Number of kernels this library launched on the calling thread so far
+ * (kernels inside a replayed CUDA graph count at every replay).  No reference
+ * counterpart. */
+long long gli_b200_launch_count(void);
+
+/* C = A B^T for device matrices in FP64 (row-major; A: M x K with leading
+ * dimension lda, B: N x K with ldb, C: M x N with ldc), evaluated on the
+ * tcgen05 tensor cores by splitting every row into 7 int8 slices of 7 bits
+ * under a per-row exponent and summing the exact int32 slice products of
+ * order < 8: about 2^-50 of max|a_i| max|b_j| per product term.  K <= 8192.
+ * No reference counterpart; the projections' contractions use it. */
+int gli_b200_dgemm_sliced_dev(const double* d_A, glong lda, const double* d_B, glong ldb, double* d_C,
+	glong ldc, glong M, glong N, glong K, void* stream);
 
 /* Kinetic matrix (same values as compute_kinetic_gausslet_integrals) for
  * callers that must not allocate device memory -- code that reserved its whole
