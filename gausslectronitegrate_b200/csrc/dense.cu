@@ -17,9 +17,24 @@
 // reference tests use as their check, test/test_eri_integrals.c:188-212)
 // instead of the O(N^4 M^4) atomic loop, slab by slab over the first index so
 // that the dense tensor is never held whole.
+//
+// Complete class lists.  When an ERI list holds every canonical class of its
+// grid (the count matches the enumeration, the indices increase strictly and
+// each is its orbit's minimum), an entry needs no canonicalisation: each class
+// value is a function of the sorted triple of per-axis keys of its four points
+// (the staged contraction computes it from exactly that), and every entry has
+// the key triple of its class.  The values are then scattered once into a
+// table indexed by the sorted key triple, and dense entries are generated by
+// key arithmetic and one table read.  The projection then generates each slab
+// of the first contraction directly as int8 slices and runs that contraction,
+// the O(N^4 M) one, on the tensor cores (FP64-level slicing).
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "symmetry.cuh"
+#include "tables.cuh"
+#include "tc_gemm.cuh"
 
 namespace gli {
 
@@ -86,6 +101,101 @@ __global__ void k_fill_eri_rows(SymGrid G, DenseGrid D, const int64_t* __restric
         out[e] = eri_entry(G, D, r / D.N, r % D.N, kl / D.N, kl % D.N, idx, val, m);
     }
 }
+
+// ---------------------------------------------------------------------------
+// complete class lists: values by sorted per-axis key triple
+__host__ __device__ inline i64 tetra_index(i64 k1, i64 k2, i64 k3) {  // k1 <= k2 <= k3
+    return k3 * (k3 + 1) * (k3 + 2) / 6 + k2 * (k2 + 1) / 2 + k1;
+}
+
+__device__ inline i64 eri_key_slot(const int p[4][3], i64 L) {
+    i64 k[3];
+    for (int a = 0; a < 3; ++a)
+        k[a] = eri_axis_key(p[0][a] - p[1][a], p[2][a] - p[3][a], (p[0][a] + p[1][a]) - (p[2][a] + p[3][a]), L);
+    if (k[0] > k[1]) { i64 t = k[0]; k[0] = k[1]; k[1] = t; }
+    if (k[1] > k[2]) { i64 t = k[1]; k[1] = k[2]; k[2] = t; }
+    if (k[0] > k[1]) { i64 t = k[0]; k[0] = k[1]; k[1] = t; }
+    return tetra_index(k[0], k[1], k[2]);
+}
+
+__device__ inline void eri_points(const SymGrid& G, i64 idx, int p[4][3]) {
+    const i64 l = idx % G.N;
+    idx /= G.N;
+    const i64 k = idx % G.N;
+    idx /= G.N;
+    const i64 j = idx % G.N;
+    point_of(G, idx / G.N, p[0]);
+    point_of(G, j, p[1]);
+    point_of(G, k, p[2]);
+    point_of(G, l, p[3]);
+}
+
+// bad = 1 unless every index is canonical and the list increases strictly
+__global__ void k_check_complete(SymGrid G, const int64_t* __restrict__ idx, i64 m, int* __restrict__ bad) {
+    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m) return;
+    const i64 v = idx[n];
+    if (v < 0 || v / (G.N * G.N) >= G.N * G.N || (n + 1 < m && v >= idx[n + 1])) {
+        atomicOr(bad, 1);
+        return;
+    }
+    int p[4][3], bias[3];
+    eri_points(G, v, p);
+    centre_points<4>(p, bias);
+    if (orbit_min_quad(G, p, bias) != v) atomicOr(bad, 1);
+}
+
+__global__ void k_key_table(SymGrid G, const int64_t* __restrict__ idx, const double* __restrict__ val, i64 m,
+                            double* __restrict__ table) {
+    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m) return;
+    int p[4][3];
+    eri_points(G, idx[n], p);
+    table[eri_key_slot(p, G.L)] = val[n];
+}
+
+// rows [row0, row0 + nrows) of the (ij) x (kl) flattening of the dense grid D,
+// from the key table of the sparse grid (range L)
+__global__ void k_fill_eri_rows_keyed(DenseGrid D, const double* __restrict__ table, i64 L, i64 row0, i64 nrows,
+                                      double* __restrict__ out) {
+    const i64 N2 = D.N * D.N;
+    const i64 total = nrows * N2;
+    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
+        const i64 r = row0 + e / N2, kl = e % N2;
+        int p[4][3];
+        dense_point(D, r / D.N, p[0]);
+        dense_point(D, r % D.N, p[1]);
+        dense_point(D, kl / D.N, p[2]);
+        dense_point(D, kl % D.N, p[3]);
+        out[e] = table[eri_key_slot(p, L)];
+    }
+}
+
+// row r = (j k) of slab i of the sparse grid's tensor, column l (keyed lookup)
+struct KeyedSlabRows {
+    SymGrid G;
+    const double* table;
+    i64 i;
+    __device__ double operator()(i64 r, int l) const {
+        int p[4][3];
+        point_of(G, i, p[0]);
+        point_of(G, r / G.N, p[1]);
+        point_of(G, r % G.N, p[2]);
+        point_of(G, l, p[3]);
+        return table[eri_key_slot(p, G.L)];
+    }
+    __device__ i64 dest(i64 r) const { return r; }
+    __device__ bool valid(i64) const { return true; }
+};
+
+// row s of the transpose of a row-major matrix with leading dimension ld
+struct TransposedRows {
+    const double* src;
+    i64 ld;
+    __device__ double operator()(i64 r, int k) const { return src[(i64)k * ld + r]; }
+    __device__ i64 dest(i64 r) const { return r; }
+    __device__ bool valid(i64) const { return true; }
+};
 
 // 48 x N permutation tables: perm[g][i] = linear index of O_h element g applied to point i
 __global__ void k_grid_perms(SymGrid G, int64_t* __restrict__ perm) {
@@ -219,6 +329,53 @@ static unsigned grid_for(i64 work, int per_block = 256) {
     return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
+// number of canonical ERI classes of a symmetric grid (enumerated once per extent)
+static i64 canonical_eri_count(const GridDesc& g, i64 e, cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<i64, i64> cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(e);
+        if (it != cache.end()) return it->second;
+    }
+    int64_t* d = nullptr;
+    const i64 n = enumerate_device(1, g, &d, s);
+    if (d) GLI_CUDA(cudaFreeAsync(d, s));
+    std::lock_guard<std::mutex> lk(mu);
+    cache[e] = n;
+    return n;
+}
+
+// Key table of a complete ERI class list, or an empty buffer when the list is
+// not the complete canonical list of its grid (then entries are looked up).
+struct KeyTable {
+    DevBuf<double> t;
+    bool ok = false;
+};
+
+static void build_key_table(const SymGrid& G, const GridDesc& g, const int64_t* d_idx, const double* d_val, i64 m,
+                            KeyTable& kt, cudaStream_t s) {
+    kt.ok = false;
+    if (m <= 0) return;
+    const i64 L = G.L;
+    const i64 nk = L * (L + 1) / 2 * (2 * L - 1);
+    const i64 slots = nk * (nk + 1) * (nk + 2) / 6;
+    if (slots > ((i64)1 << 29)) return;  // above 4 GB: keep the lookups
+    if (canonical_eri_count(g, G.e, s) != m) return;
+    DevBuf<int> bad(1, s);
+    bad.zero();
+    k_check_complete<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(G, d_idx, m, bad.p);
+    GLI_CHECK_LAUNCH();
+    int h = 0;
+    GLI_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GLI_CUDA(cudaStreamSynchronize(s));
+    if (h) return;
+    kt.t.alloc(slots, s);
+    k_key_table<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(G, d_idx, d_val, m, kt.t.p);
+    GLI_CHECK_LAUNCH();
+    kt.ok = true;
+}
+
 void fill_dense_device(int kind, const GridDesc& sparse, const int64_t* d_idx, const double* d_val, i64 m,
                        const GridDesc& dense, double* d_out, cudaStream_t s) {
     const SymGrid G = sym_of(sparse);
@@ -228,7 +385,15 @@ void fill_dense_device(int kind, const GridDesc& sparse, const int64_t* d_idx, c
         k_fill_erida<<<grid_for(D.N * D.N), 256, 0, s>>>(G, D, d_idx, d_val, m, d_out);
     } else {
         const i64 rows = D.N * D.N;
-        k_fill_eri_rows<<<grid_for(rows * rows), 256, 0, s>>>(G, D, d_idx, d_val, m, 0, rows, d_out);
+        KeyTable kt;
+        build_key_table(G, sparse, d_idx, d_val, m, kt, s);
+        if (kt.ok)
+            k_fill_eri_rows_keyed<<<grid_for(rows * rows), 256, 0, s>>>(D, kt.t.p, G.L, 0, rows, d_out);
+        else
+            k_fill_eri_rows<<<grid_for(rows * rows), 256, 0, s>>>(G, D, d_idx, d_val, m, 0, rows, d_out);
+        GLI_CHECK_LAUNCH();
+        // the key table is released on the stream after the fill
+        return;
     }
     GLI_CHECK_LAUNCH();
 }
@@ -251,10 +416,15 @@ void apply_eri_device(const GridDesc& g, const int64_t* d_idx, const double* d_v
     if (ci < 1) ci = 1;
     if (ci > N) ci = N;
     DevBuf<double> V(ci * per_i, s);
+    KeyTable kt;
+    build_key_table(G, g, d_idx, d_val, m, kt, s);
     for (i64 i0 = 0; i0 < N; i0 += ci) {
         const i64 ni = std::min(ci, N - i0);
         // V rows (i, j) for i in [i0, i0 + ni): layout [i][j][k][l]
-        k_fill_eri_rows<<<grid_for(ni * per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i0 * N, ni * N, V.p);
+        if (kt.ok)
+            k_fill_eri_rows_keyed<<<grid_for(ni * per_i), 256, 0, s>>>(D, kt.t.p, G.L, i0 * N, ni * N, V.p);
+        else
+            k_fill_eri_rows<<<grid_for(ni * per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i0 * N, ni * N, V.p);
         GLI_CHECK_LAUNCH();
         // for each (i, k): ret[i*N + k][s] = sum_j sum_l V[i][j][k][l] states[j*N + l][s]
         // batch over i (ni) and j-contributions accumulate: for fixed i, j:
@@ -292,12 +462,42 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     }
     // slab by slab over i: S[j][k][l] = V[i j k l]
     const i64 per_i = N2 * N;
-    DevBuf<double> S(per_i, s), A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s);
+    DevBuf<double> A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s);
+    KeyTable kt;
+    build_key_table(G, g, d_idx, d_val, m, kt, s);
+    const bool tensor = kt.ok && N <= 8192 && N2 <= (i64)65535 * TC_BM;
+    DevBuf<double> S;
+    TiledSlices Ss, Bs;
+    DevBuf<int> err;
+    constexpr int BN = tile_n(FP64_SLICES);
+    if (tensor) {
+        // the basis as the B side: row s = column s of B (K = l)
+        Ss.alloc((N2 + TC_BM - 1) / TC_BM, TC_BM, (int)N, FP64_SLICES, s);
+        Bs.alloc((M + BN - 1) / BN, BN, (int)N, FP64_SLICES, s);
+        slice_tiled(TransposedRows{d_basis, M}, M, (int)N, Bs, s);
+        err.alloc(1, s);
+        err.zero();
+    } else {
+        S.alloc(per_i, s);
+    }
     for (i64 i = 0; i < N; ++i) {
-        k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
-        GLI_CHECK_LAUNCH();
         // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-        dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false, s);
+        if (tensor) {
+            slice_tiled(KeyedSlabRows{G, kt.t.p, i}, N2, (int)N, Ss, s);
+            TileWork w;
+            w.a_rows = (int)N2;
+            w.a_blocks = (int)((N2 + TC_BM - 1) / TC_BM);
+            w.n_total = (int)M;
+            w.C = A1.p;
+            w.rs = M;
+            w.cs = 1;
+            tc_gemm_tiled(Ss.view(), Bs.view(), w, (int)((M + BN - 1) / BN), err.p, s);
+        } else {
+            k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
+            GLI_CHECK_LAUNCH();
+            dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false,
+                  s);
+        }
         // A2[j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j)
         dgemm((int)M, (int)M, (int)N, MatView{d_basis, 0, 1, M}, MatView{A1.p, N * M, M, 1}, A2.p, M * M, M, 1,
               (int)N, false, s);
@@ -308,6 +508,12 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     // E[p][(q r s)] = sum_i B[i][p] A3[i][(q r s)]
     dgemm((int)M, (int)(M * M * M), (int)N, MatView{d_basis, 0, 1, M}, MatView{A3.p, 0, M * M * M, 1}, d_out, 0,
           M * M * M, 1, 1, false, s);
+    if (tensor) {
+        int h = 0;
+        GLI_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        if (h) fail(GLI_ERR_INTERNAL, "tensor-core projection: an mbarrier wait expired (code %d)", h);
+    }
 }
 
 }  // namespace gli

@@ -111,21 +111,26 @@ __global__ void k_nuc_field(const NucInst* __restrict__ inst, const double* __re
 }
 
 // V[i][j] of every instance from its key-indexed block Vk[kx][kz * nky + ky];
-// grid (blocks, instance)
-__global__ void k_nuc_scatter(const NucInst* __restrict__ inst, const double* __restrict__ Vk) {
+// grid (row blocks, instance): a block writes whole rows i (coalesced), and
+// the coordinates of j come from two 32-bit divisions per element (every
+// instance has at most 256^3 points)
+__global__ void __launch_bounds__(256) k_nuc_scatter(const NucInst* __restrict__ inst, const double* __restrict__ Vk) {
     const NucInst& in = inst[blockIdx.y];
     const int ny = in.n[1], nz = in.n[2], nky = in.nk[1], nkz = in.nk[2];
-    const i64 N = in.N, total = N * N;
+    const int N = (int)in.N, nyz = ny * nz;
     const double* vk = Vk + in.vk_off;
-    double* V = in.out;
-    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
-        const i64 i = e / N, j = e % N;
-        const int iz = (int)(i % nz), iy = (int)((i / nz) % ny), ix = (int)(i / ((i64)nz * ny));
-        const int jz = (int)(j % nz), jy = (int)((j / nz) % ny), jx = (int)(j / ((i64)nz * ny));
-        const int ax = min(ix, jx), bx = max(ix, jx), ay = min(iy, jy), by = max(iy, jy);
-        const int az = min(iz, jz), bz = max(iz, jz);
-        const i64 kx = bx * (bx + 1) / 2 + ax, ky = by * (by + 1) / 2 + ay, kz = bz * (bz + 1) / 2 + az;
-        V[e] = vk[kx * ((i64)nkz * nky) + kz * nky + ky];
+    for (int i = blockIdx.x; i < N; i += gridDim.x) {
+        const int iz = i % nz, iy = (i / nz) % ny, ix = i / nyz;
+        double* row = in.out + (i64)i * N;
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const int jx = j / nyz, t = j - jx * nyz;
+            const int jy = t / nz, jz = t - jy * nz;
+            const int ax = min(ix, jx), bx = max(ix, jx), ay = min(iy, jy), by = max(iy, jy);
+            const int az = min(iz, jz), bz = max(iz, jz);
+            const i64 kx = bx * (bx + 1) / 2 + ax;
+            const int ky = by * (by + 1) / 2 + ay, kz = bz * (bz + 1) / 2 + az;
+            row[j] = vk[kx * ((i64)nkz * nky) + kz * nky + ky];
+        }
     }
 }
 
@@ -290,7 +295,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
     const int ni = (int)hosts.size();
     i64 w_total = 0, phi_total = 0, vk_total = 0;
     int max_nk = 1, max_u = 1;
-    i64 max_cells = 1, max_nn = 1;
+    i64 max_cells = 1, max_n = 1;
     for (const NucHost& h : hosts) {
         for (int a = 0; a < 3; ++a) {
             w_total = std::max(w_total, h.d.w_off[a] + (i64)h.d.nk[a] * h.d.U[a]);
@@ -301,7 +306,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
         phi_total = std::max(phi_total, h.d.phi_off + cells);
         vk_total = std::max(vk_total, h.d.vk_off + (i64)h.d.nk[0] * h.d.nk[1] * h.d.nk[2]);
         max_cells = std::max(max_cells, cells);
-        max_nn = std::max(max_nn, h.d.N * h.d.N);
+        max_n = std::max(max_n, h.d.N);
     }
     DevBuf<double> W(w_total, s), Phi(phi_total, s), Vk(vk_total, s);
     k_nuc_weights<<<dim3((unsigned)((max_u + 127) / 128), (unsigned)max_nk, (unsigned)(3 * ni)), 128, 0, s>>>(
@@ -328,7 +333,8 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
         GLI_CUDA(cudaEventRecord(t_ring.events[k], t_ring.streams[k]));
         GLI_CUDA(cudaStreamWaitEvent(s, t_ring.events[k], 0));
     }
-    const unsigned sb = (unsigned)std::min<i64>((max_nn + 255) / 256, std::max<i64>(1, (i64)num_sms * 16));
+    // rows per instance: enough blocks for every SM even when few instances are large
+    const unsigned sb = (unsigned)std::min<i64>(max_n, std::max<i64>(1, (i64)num_sms * 16));
     k_nuc_scatter<<<dim3(sb, (unsigned)ni), 256, 0, s>>>(d_inst, Vk.p);
     GLI_CHECK_LAUNCH();
 }

@@ -241,6 +241,30 @@ def test_project_eri(gli):
     assert np.max(np.abs(s.project(basis) - project_factored(dense, basis))) <= 1e-12
 
 
+def test_eri_keyed_fill_equals_oracle_fill(gli):
+    # a complete class list: dense entries come from the key-triple table; the
+    # oracle canonicalises every entry and looks it up -- same class values in,
+    # so the dense tensors must agree bit for bit
+    s = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(5), 1e-5)
+    dense_grid = [(-1, 3), (-2, 4), (0, 2)]
+    got = s.fill_tensor(dense_grid)
+    ref = ORACLE.fill_dense("eri", sym_grid(5), s.indices, s.values, dense_grid)
+    assert np.array_equal(got, ref)
+
+
+def test_eri_partial_list_fill_and_project(gli):
+    # a partial list (every third class missing) keeps the canonical lookups:
+    # missing classes read as zero, as in the reference
+    full = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(3), 1e-5)
+    keep = np.arange(full.indices.size) % 3 != 1
+    part = gli.SparseERI._make(g10(), sym_grid(3), full.indices[keep], full.values[keep], 1e-5)
+    got = part.fill_tensor(sym_grid(3))
+    ref = ORACLE.fill_dense("eri", sym_grid(3), full.indices[keep], full.values[keep], sym_grid(3))
+    assert np.array_equal(got, ref)
+    basis = np.random.default_rng(9).normal(size=(27, 3))
+    assert np.max(np.abs(part.project(basis) - project_factored(ref, basis))) <= 1e-12 * np.max(np.abs(ref)) * 27 ** 2
+
+
 def test_project_erida(gli):
     s = gli.compute_sparse_erida_gausslet_integrals(g10(), sym_grid(5), 1e-5)
     basis = np.random.default_rng(5).normal(size=(125, 5))
