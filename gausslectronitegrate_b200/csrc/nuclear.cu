@@ -87,26 +87,40 @@ __global__ void k_nuc_weights(const NucInst* __restrict__ inst, const double* __
     }
 }
 
+// the Gaussian-nucleus field at lattice point (u, v, t) of an instance
+__device__ inline double nuc_field_at(const NucInst& in, const double* __restrict__ npos,
+                                      const double* __restrict__ ncharge, int u, int v, int t) {
+    const double px = (u + in.u0[0]) / 6.0, py = (v + in.u0[1]) / 6.0, pz = (t + in.u0[2]) / 6.0;
+    double acc = 0;
+    for (int k = in.nuc0; k < in.nuc0 + in.nnuc; ++k) {
+        const double dx = px - npos[3 * k], dy = py - npos[3 * k + 1], dz = pz - npos[3 * k + 2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        // g(r) = erf(r / w) / r with w = 1/3; g(0) = 2 / (sqrt(pi) w).  For
+        // 3 r >= 6, erfc(3 r) <= 2.2e-17 is below a quarter ulp of 1: erf
+        // rounds to 1 and g = 1 / r
+        double g;
+        if (r2 >= 4.0) {
+            g = 1.0 / sqrt(r2);
+        } else {
+            const double r = sqrt(r2);
+            g = r > 0 ? erf(3.0 * r) / r : 3.3851375012865379;  // 6 / sqrt(pi)
+        }
+        acc += ncharge[k] * g;
+    }
+    return acc;
+}
+
 // Phi[u][v][t] (t fastest) of every instance, position (u + u0x, v + u0y, t + u0z) / 6;
-// grid (blocks, instance)
-__global__ void k_nuc_field(const NucInst* __restrict__ inst, const double* __restrict__ npos,
-                            const double* __restrict__ ncharge, double* __restrict__ Phi) {
+// grid (row blocks, instance): a block fills whole (u, v) rows
+__global__ void __launch_bounds__(128) k_nuc_field(const NucInst* __restrict__ inst, const double* __restrict__ npos,
+                                                   const double* __restrict__ ncharge, double* __restrict__ Phi) {
     const NucInst& in = inst[blockIdx.y];
     const int Uy = in.U[1], Uz = in.U[2];
-    const i64 total = (i64)in.U[0] * Uy * Uz;
-    double* phi = Phi + in.phi_off;
-    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
-        const int t = (int)(e % Uz), v = (int)((e / Uz) % Uy), u = (int)(e / ((i64)Uz * Uy));
-        const double px = (u + in.u0[0]) / 6.0, py = (v + in.u0[1]) / 6.0, pz = (t + in.u0[2]) / 6.0;
-        double acc = 0;
-        for (int k = in.nuc0; k < in.nuc0 + in.nnuc; ++k) {
-            const double dx = px - npos[3 * k], dy = py - npos[3 * k + 1], dz = pz - npos[3 * k + 2];
-            const double r = sqrt(dx * dx + dy * dy + dz * dz);
-            // g(r) = erf(r / w) / r with w = 1/3; g(0) = 2 / (sqrt(pi) w)
-            const double g = r > 0 ? erf(3.0 * r) / r : 3.3851375012865379;  // 6 / sqrt(pi)
-            acc += ncharge[k] * g;
-        }
-        phi[e] = acc;
+    const i64 rows = (i64)in.U[0] * Uy;
+    for (i64 row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int u = (int)(row / Uy), v = (int)(row - (i64)u * Uy);
+        double* phi = Phi + in.phi_off + row * Uz;
+        for (int t = threadIdx.x; t < Uz; t += blockDim.x) phi[t] = nuc_field_at(in, npos, ncharge, u, v, t);
     }
 }
 
@@ -193,7 +207,7 @@ static void nuc_contract_mixed(const NucInst& in, const double* W, const double*
     const double* Wy = W + in.w_off[1];
     const double* Wz = W + in.w_off[2];
     DevBuf<double> H((i64)nk[2] * UxUy, s), H2(nzy * U[0], s);
-    {   // A: rows (u v) of Phi against the z keys
+    {   // A: rows (u v) of the field against the z keys
         TiledSlices As, Bs;
         const i64 mb = (UxUy + TC_BM - 1) / TC_BM, nbt = (nk[2] + BN - 1) / BN;
         As.alloc(mb, TC_BM, U[2], S, s);
@@ -295,7 +309,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
     const int ni = (int)hosts.size();
     i64 w_total = 0, phi_total = 0, vk_total = 0;
     int max_nk = 1, max_u = 1;
-    i64 max_cells = 1, max_n = 1;
+    i64 max_rows = 1, max_n = 1;
     for (const NucHost& h : hosts) {
         for (int a = 0; a < 3; ++a) {
             w_total = std::max(w_total, h.d.w_off[a] + (i64)h.d.nk[a] * h.d.U[a]);
@@ -305,16 +319,19 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
         const i64 cells = (i64)h.d.U[0] * h.d.U[1] * h.d.U[2];
         phi_total = std::max(phi_total, h.d.phi_off + cells);
         vk_total = std::max(vk_total, h.d.vk_off + (i64)h.d.nk[0] * h.d.nk[1] * h.d.nk[2]);
-        max_cells = std::max(max_cells, cells);
+        max_rows = std::max(max_rows, (i64)h.d.U[0] * h.d.U[1]);
         max_n = std::max(max_n, h.d.N);
     }
+    const bool mixed = form == FORM_MIXED;
     DevBuf<double> W(w_total, s), Phi(phi_total, s), Vk(vk_total, s);
     k_nuc_weights<<<dim3((unsigned)((max_u + 127) / 128), (unsigned)max_nk, (unsigned)(3 * ni)), 128, 0, s>>>(
         d_inst, F, nf, nb, coords, W.p);
     GLI_CHECK_LAUNCH();
-    const unsigned fb = (unsigned)std::min<i64>((max_cells + 255) / 256, std::max<i64>(1, (i64)num_sms * 8));
-    k_nuc_field<<<dim3(fb, (unsigned)ni), 256, 0, s>>>(d_inst, npos, ncharge, Phi.p);
-    GLI_CHECK_LAUNCH();
+    {
+        const unsigned fb = (unsigned)std::min<i64>(max_rows, std::max<i64>(1, (i64)num_sms * 16));
+        k_nuc_field<<<dim3(fb, (unsigned)ni), 128, 0, s>>>(d_inst, npos, ncharge, Phi.p);
+        GLI_CHECK_LAUNCH();
+    }
     // per-instance contractions, largest first, round-robin over the streams
     std::vector<int> order(ni);
     for (int k = 0; k < ni; ++k) order[k] = k;
@@ -324,7 +341,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
     for (int k = 0; k < ni; ++k) {
         cudaStream_t st = t_ring.streams[k % nstreams];
         const NucInst& in = hosts[order[k]].d;
-        if (form == FORM_MIXED)
+        if (mixed)
             nuc_contract_mixed(in, W.p, Phi.p, Vk.p, err, st);
         else
             nuc_contract_fp64(in, W.p, Phi.p, Vk.p, st);
