@@ -78,7 +78,9 @@ EXPORTS = [
     "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_measure_fp64_peak",
     "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
     "gli_b200_nuclear_batch_dev", "gli_b200_nuclear_batch", "gli_b200_last_nuclear_batch", "gli_b200_autotune_report",
-    "gli_b200_autotune_selftest",
+    "gli_b200_autotune_selftest", "gli_b200_surrogate_train", "gli_b200_surrogate_free", "gli_b200_surrogate_info",
+    "gli_b200_surrogate_params", "gli_b200_erida_surrogate_values", "gli_b200_mlp_loss_grad",
+    "gli_b200_mlp_param_count",
 ]
 
 
@@ -145,4 +147,20 @@ def load(path=LIB_PATH):
     L.gli_b200_autotune_report.argtypes = [C.c_char_p, glong]
     L.gli_b200_autotune_report.restype = glong
     L.gli_b200_autotune_selftest.restype = C.c_int
+    L.gli_b200_surrogate_train.argtypes = [P(GaussletData), C.c_double, C.c_double, C.c_int, C.c_double, C.c_double,
+                                           C.c_ulonglong, P(C.c_void_p)]
+    L.gli_b200_surrogate_train.restype = C.c_int
+    L.gli_b200_surrogate_free.argtypes = [C.c_void_p]
+    L.gli_b200_surrogate_free.restype = None
+    L.gli_b200_surrogate_info.argtypes = [C.c_void_p, P(C.c_double)]
+    L.gli_b200_surrogate_info.restype = C.c_int
+    L.gli_b200_surrogate_params.argtypes = [C.c_void_p, P(C.c_float), glong]
+    L.gli_b200_surrogate_params.restype = glong
+    L.gli_b200_erida_surrogate_values.argtypes = [C.c_void_p, P(GaussletData), P(Grid), lptr, glong, C.c_double,
+                                                  C.c_double, C.c_ulonglong, C.c_double, dptr, dptr, glong]
+    L.gli_b200_erida_surrogate_values.restype = C.c_int
+    L.gli_b200_mlp_loss_grad.argtypes = [P(C.c_float), P(C.c_float), P(C.c_float), P(C.c_float), glong,
+                                         P(C.c_float), P(C.c_float)]
+    L.gli_b200_mlp_loss_grad.restype = C.c_int
+    L.gli_b200_mlp_param_count.restype = C.c_int
     return L

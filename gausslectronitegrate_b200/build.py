@@ -20,7 +20,7 @@ LIB = os.path.join(PKG, "libgli_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["runtime.cu", "tables.cu", "enumerate.cu", "contract.cu", "kinetic.cu", "nuclear.cu", "dense.cu",
-           "tc_gemm.cu", "autotune.cu", "capi.cu"]
+           "tc_gemm.cu", "autotune.cu", "surrogate.cu", "capi.cu"]
 
 
 def _flags(debug):

@@ -312,6 +312,51 @@ glong gli_b200_autotune_report(char* buf, glong len);
  * device; 0 on success.  No reference counterpart. */
 int gli_b200_autotune_selftest(void);
 
+/* ---- ERIDA far-field surrogate (no counterpart in the reference) ----------
+ * A small MLP (features of the sorted displacement |dx| >= |dy| >= |dz| in
+ * grid units: d/16, r/16, d/r; four tanh layers of width 64; FP32) trained on
+ * this device on exact class values of the staged contraction.  It predicts
+ * the residual of an ERIDA class value against the point-charge limit 1/r:
+ *   r <= 6:          exact
+ *   6 < r <= r_mlp:  1/r + s(r) MLP(d),  s(r) = exp(c0 + c1 r + c2 r^2)
+ *   r > r_mlp:       1/r
+ * (values in grid units; a grid of spacing h scales them by 1/h). */
+typedef struct gli_b200_surrogate gli_b200_surrogate;
+
+/* Train on the displacements 6 < r <= r_mlp (exact values on centred cubes of
+ * 25..65 points, the same coefficients and tol as the evaluations it will
+ * serve): `steps` full-batch Adam steps from learning rate lr with cosine
+ * decay; holdout_fraction of the samples (seeded) is kept out of training for
+ * the report.  *out is released with gli_b200_surrogate_free. */
+int gli_b200_surrogate_train(const struct gausslet_data* gdata, double tol, double r_mlp, int steps,
+	double lr, double holdout_fraction, unsigned long long seed, gli_b200_surrogate** out);
+void gli_b200_surrogate_free(gli_b200_surrogate* s);
+/* info: samples, hold-out samples, weighted loss, max |dz| train / hold-out,
+ * max |residual error| train / hold-out (grid units), r_cut, r_mlp,
+ * parameter count, c2, c0, c1 */
+int gli_b200_surrogate_info(const gli_b200_surrogate* s, double info[13]);
+/* copies min(n, count) parameters; returns the count */
+glong gli_b200_surrogate_params(const gli_b200_surrogate* s, float* params, glong n);
+
+/* ERIDA values of a class list (host arrays) from the surrogate with a seeded
+ * audit: every class with r <= 6 and an audit sample of each radial shell
+ * (floor r; audit_fraction of its classes, at least 4; none when
+ * audit_fraction is 0) are evaluated exactly;
+ * a shell whose largest audit error exceeds shell_tol (grid units) is
+ * evaluated exactly in full.  report (optional, max_shells x 4): per shell
+ * classes, audited classes, max audit error, evaluated in full (1/0). */
+int gli_b200_erida_surrogate_values(const gli_b200_surrogate* s, const struct gausslet_data* gdata,
+	const struct cartesian_grid_3d* grid, const glong* indices, glong num, double tol,
+	double audit_fraction, unsigned long long seed, double shell_tol, double* values,
+	double* report, glong max_shells);
+
+/* One forward and backward pass of the training kernels without an update:
+ * weighted mean squared loss and its gradient for params (count from
+ * gli_b200_mlp_param_count), n samples of 7 features X, targets T, weights W. */
+int gli_b200_mlp_loss_grad(const float* params, const float* X, const float* T, const float* W, glong n,
+	float* loss, float* grads);
+int gli_b200_mlp_param_count(void);
+
 /* Symmetry-reduced class list of kind 0/1 into device memory (reference
  * src/eri_integrals.c:382-526, src/erida_integrals.c:300-410).  *d_indices is
  * allocated with cudaMallocAsync on stream; release with gli_b200_free_dev. */

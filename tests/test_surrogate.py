@@ -1,0 +1,150 @@
+"""The ERIDA far-field surrogate: its network's training kernels against a CPU
+restatement (oracle/mlp_oracle.py), the trained network's gain over the
+point-charge limit 1/r, and the audit that keeps every radial shell within its
+tolerance by exact re-evaluation.
+
+Values are in grid units (spacing 1).  The batched workload runs at spacing
+0.3 bohr, where 1e-6 Ha is 3e-7 grid units: SHELL_TOL below.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import mlp_oracle
+from _common import assert_parity, g10, sym_grid
+
+SHELL_TOL = 3e-7
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    p = rng.normal(0, 0.3, mlp_oracle.param_count())
+    d = np.sort(rng.integers(0, 13, size=(20, 3)), axis=1)[:, ::-1] + np.array([7, 0, 0])
+    X = mlp_oracle.features(d)
+    T = rng.normal(size=20)
+    W = rng.uniform(0.1, 1.0, size=20)
+    _, g = mlp_oracle.loss_grad(p, X, T, W)
+    for k in rng.choice(p.size, size=40, replace=False):
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        fd = (mlp_oracle.loss_grad(p + e, X, T, W)[0] - mlp_oracle.loss_grad(p - e, X, T, W)[0]) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k])), (k, fd, g[k])
+
+
+@pytest.fixture(scope="module")
+def gli():
+    import gausslectronitegrate_b200 as m
+    if m.lib().gli_b200_device_count() == 0:
+        pytest.fail("no CUDA device: the gpu tests need a B200")
+    return m
+
+
+def _fp(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+@pytest.mark.gpu
+def test_gpu_loss_and_gradient_match_cpu_oracle(gli):
+    L = gli.lib()
+    n_par = L.gli_b200_mlp_param_count()
+    assert n_par == mlp_oracle.param_count()
+    rng = np.random.default_rng(1)
+    p = _fp(rng.normal(0, 0.25, n_par))
+    d = np.sort(rng.integers(0, 12, size=(300, 3)), axis=1)[:, ::-1] + np.array([7, 0, 0])
+    X = _fp(mlp_oracle.features(d))
+    T = _fp(rng.normal(size=300))
+    W = _fp(rng.uniform(0.01, 1.0, size=300))
+    loss = C.c_float()
+    grads = np.empty(n_par, dtype=np.float32)
+    fptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    rc = L.gli_b200_mlp_loss_grad(fptr(p), fptr(X), fptr(T), fptr(W), 300, C.byref(loss), fptr(grads))
+    assert rc == 0, L.gli_b200_last_error_message().decode()
+    ref_loss, ref_g = mlp_oracle.loss_grad(p.astype(np.float64), X.astype(np.float64), T, W)
+    assert abs(loss.value - ref_loss) <= 1e-5 * abs(ref_loss)
+    assert np.max(np.abs(grads - ref_g)) <= 1e-4 * np.max(np.abs(ref_g))
+
+
+def _train(gli, steps=20000, holdout=0.2, seed=7):
+    from gausslectronitegrate_b200 import _abi
+    gd, keep = gli._parse_coeffs(g10(), "")
+    h = C.c_void_p()
+    rc = gli.lib().gli_b200_surrogate_train(C.byref(gd), 1e-16, 12.0, steps, 2e-3, holdout, seed, C.byref(h))
+    assert rc == 0, gli.lib().gli_b200_last_error_message().decode()
+    info = (C.c_double * 13)()
+    assert gli.lib().gli_b200_surrogate_info(h, info) == 0
+    return h, list(info), gd, keep
+
+
+def _surrogate(gli, h, gd, grid, idx, audit, tol):
+    from gausslectronitegrate_b200 import _abi
+    vals = np.empty(idx.size)
+    rep = np.zeros((64, 4))
+    rc = gli.lib().gli_b200_erida_surrogate_values(h, C.byref(gd), C.byref(gli._grid_struct(grid)),
+                                                   idx.ctypes.data_as(_abi.lptr), idx.size, 1e-16, audit, 11, tol,
+                                                   vals.ctypes.data_as(_abi.dptr), rep.ctypes.data_as(_abi.dptr), 64)
+    assert rc == 0, gli.lib().gli_b200_last_error_message().decode()
+    return vals, rep
+
+
+def _shells(grid, idx):
+    L = grid[0][1]
+    N = L ** 3
+    def pts(lin):
+        return np.stack([lin // (L * L), (lin // L) % L, lin % L], 1)
+    d = np.abs(pts(idx // N) - pts(idx % N))
+    r = np.sqrt((d ** 2).sum(1))
+    return np.floor(r).astype(int), r
+
+
+@pytest.mark.gpu
+def test_trained_network_gains_over_point_charge_limit(gli):
+    # trained with 20% of the displacements held out; evaluated with no audit,
+    # so every class beyond r = 6 carries the network's (or 1/r) prediction
+    h, info, gd, keep = _train(gli)
+    try:
+        assert info[0] > 200 and info[1] > 40
+        grid = sym_grid(33)
+        exact = gli.compute_sparse_erida_gausslet_integrals(g10(), grid, 1e-16)
+        idx = exact.indices
+        vals, _ = _surrogate(gli, h, gd, grid, idx, 0.0, 1e300)
+        shell, r = _shells(grid, idx)
+        err = np.abs(vals - exact.values)
+        base = np.abs(1.0 / np.where(r > 0, r, 1) - exact.values)
+        near = r <= 6
+        assert np.max(err[near]) <= 1e-13  # exact there
+        mlp = (r > 7) & (r <= 11)
+        gain = np.max(base[mlp]) / np.max(err[mlp])
+        print(f"shells 7-10: network max err {np.max(err[mlp]):.2e}, 1/r max err {np.max(base[mlp]):.2e}, "
+              f"gain {gain:.1f}x; info {info}")
+        assert gain >= 10.0
+        assert np.max(err[r > 12]) <= SHELL_TOL  # the 1/r region
+    finally:
+        gli.lib().gli_b200_surrogate_free(h)
+
+
+@pytest.mark.gpu
+def test_audit_falls_back_to_exact_shells(gli):
+    h, info, gd, keep = _train(gli, steps=3000, holdout=0.0)
+    try:
+        grid = sym_grid(25)
+        exact = gli.compute_sparse_erida_gausslet_integrals(g10(), grid, 1e-16)
+        idx = exact.indices
+        # tolerance 0: every far shell with a nonzero audit error is evaluated exactly
+        vals, rep = _surrogate(gli, h, gd, grid, idx, 0.01, 0.0)
+        assert_parity(vals, exact.values, what="surrogate with zero shell tolerance")
+        shells = rep[:, 0] > 0
+        assert np.all(rep[shells, 1] >= np.minimum(4, rep[shells, 0]))
+        # a normal tolerance: audited shells within it, the others redone
+        vals, rep = _surrogate(gli, h, gd, grid, idx, 0.01, SHELL_TOL)
+        shell, r = _shells(grid, idx)
+        err = np.abs(vals - exact.values)
+        for k in range(64):
+            if rep[k, 0] == 0:
+                continue
+            if rep[k, 3] == 1:
+                assert np.max(err[shell == k]) <= 1e-13, k
+            else:
+                assert rep[k, 2] <= SHELL_TOL, k
+    finally:
+        gli.lib().gli_b200_surrogate_free(h)
