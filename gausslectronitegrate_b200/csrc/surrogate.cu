@@ -40,12 +40,16 @@ constexpr int MLP_IN = 7, MLP_W = 64, MLP_HIDDEN = 4;
 // flat parameter layout: for each layer l: W_l (out x in, row-major), then b_l
 __host__ __device__ constexpr int mlp_layer_in(int l) { return l == 0 ? MLP_IN : MLP_W; }
 __host__ __device__ constexpr int mlp_layer_out(int l) { return l == MLP_HIDDEN ? 1 : MLP_W; }
+// closed form (no recursion: kernels keep a statically sized stack)
 __host__ __device__ constexpr int mlp_offset(int l) {
-    return l == 0 ? 0 : mlp_offset(l - 1) + mlp_layer_out(l - 1) * mlp_layer_in(l - 1) + mlp_layer_out(l - 1);
+    return l == 0 ? 0
+                  : (MLP_W * MLP_IN + MLP_W) + (l <= MLP_HIDDEN ? l - 1 : MLP_HIDDEN - 1) * (MLP_W * MLP_W + MLP_W) +
+                        (l > MLP_HIDDEN ? MLP_W + 1 : 0);
 }
 constexpr int MLP_PARAMS = mlp_offset(MLP_HIDDEN + 1);
 constexpr int MLP_ACT = MLP_HIDDEN * MLP_W;  // stored activations per sample
 static_assert(MLP_PARAMS == 7 * 64 + 64 + 3 * (64 * 64 + 64) + 64 + 1, "parameter count");
+static_assert(mlp_offset(1) == 512 && mlp_offset(4) == 12992, "layer offsets");
 
 __host__ __device__ inline void mlp_features(double a, double b, double c, float f[MLP_IN]) {
     const double r = sqrt(a * a + b * b + c * c);
