@@ -58,6 +58,13 @@ SPACING = 0.5        # bohr
 TOL = 1e-16
 WORKLOAD = "ERIDA 32^3 grid (odd stand-in 33^3, 6545 classes), spacing 0.5 bohr, G10, tol 1e-16"
 
+# the other hot-path configurations (--workload); the default line is the metric's
+WORKLOADS = {
+    "erida33": (33, 0.5, WORKLOAD),
+    "erida129": (129, 0.3, "ERIDA 128^3 grid (odd stand-in 129^3, 366145 classes), spacing 0.3 bohr, G10, "
+                           "tol 1e-16"),
+}
+
 
 def g10():
     return np.load(os.path.join(REPO, "tests", "golden", "reference_fixtures.npz"))["g10"]
@@ -132,28 +139,36 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+CPU_SAMPLE = 4000  # classes per pass of the CPU reference when the list is larger
+
+
 def cpu_reference_rate(b, spec, idx, tol, min_seconds=8.0):
-    """Reference C core (oracle/_ref) on all host cores over the full class list,
-    repeated until about min_seconds of CPU work; returns (classes/s, sample)."""
+    """Reference C core (oracle/_ref) on all host cores, repeated until about
+    min_seconds of CPU work; lists longer than CPU_SAMPLE classes are timed on
+    a seeded sample of that many classes.  Returns (classes/s, sample text,
+    values of the whole list or None, indices of the sample)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     from ref_binding import RefLib
     r = RefLib()
+    sample = idx if idx.size <= CPU_SAMPLE else np.sort(
+        np.random.default_rng(0).choice(idx, size=CPU_SAMPLE, replace=False))
     reps, t0 = 0, time.perf_counter()
     vals = None
     while True:
-        vals = r.sparse_values("erida", b, spec, idx, tol)
+        vals = r.sparse_values("erida", b, spec, sample, tol)
         reps += 1
         el = time.perf_counter() - t0
         if el >= min_seconds or reps >= 50:
             break
-    return reps * idx.size / el, f"full {idx.size}-class list x {reps} passes ({el:.1f} s)", vals
+    what = (f"full {idx.size}-class list" if sample is idx else f"seeded sample of {sample.size} of {idx.size} classes")
+    return reps * sample.size / el, f"{what} x {reps} passes ({el:.1f} s)", vals, sample
 
 
-def cpu_baseline_subprocess(gpu_values_path):
+def cpu_baseline_subprocess(gpu_values_path, workload):
     """Times the reference core in a fresh process (no torch, so its OpenMP
     runtime is the only one loaded); compares its values with the GPU's."""
-    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-baseline-json", gpu_values_path],
-                       capture_output=True, text=True, timeout=600)
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-baseline-json", gpu_values_path,
+                        "--workload", workload], capture_output=True, text=True, timeout=600)
     if r.returncode != 0:
         raise RuntimeError(f"CPU baseline process failed: {r.stderr.strip()[-300:]}")
     return json.loads(r.stdout.strip().splitlines()[-1])
@@ -164,11 +179,12 @@ def cpu_baseline_main(gpu_values_path):
     spec = grid_spec()
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     from ref_binding import RefLib
-    idx = RefLib().enumerate("erida", spec)
-    rate, sample, vals = cpu_reference_rate(b, spec, idx, TOL)
     gpu = np.load(gpu_values_path)
-    errs = {f"max_abs_err_ha_gpu_{k}_vs_reference": float(np.max(np.abs(vals - gpu[k])) / SPACING)
-            for k in ("fp64", "mixed") if gpu[k].shape == vals.shape}
+    idx = gpu["indices"]  # the class list the GPU evaluated (its enumeration is tested bit-exact)
+    rate, sample, vals, sidx = cpu_reference_rate(b, spec, idx, TOL)
+    pos = np.searchsorted(idx, sidx)
+    errs = {f"max_abs_err_ha_gpu_{k}_vs_reference": float(np.max(np.abs(vals - gpu[k][pos])) / SPACING)
+            for k in ("fp64", "mixed") if gpu[k].shape == idx.shape}
     print(json.dumps({"value": rate, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
                       "sample": sample, **errs}))
     return 0
@@ -185,7 +201,9 @@ def run_reference(args):
     r = RefLib()
     b = g10()
     spec = grid_spec()
-    idx = r.enumerate("erida", spec)
+    full = r.enumerate("erida", spec)
+    idx = full if full.size <= CPU_SAMPLE else np.sort(
+        np.random.default_rng(0).choice(full, size=CPU_SAMPLE, replace=False))
     for _ in range(min(args.warmup, 1)):
         r.sparse_values("erida", b, spec, idx, TOL)
     times = []
@@ -200,7 +218,9 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "classes": int(idx.size), "form": "fp64 (reference C core)"},
             "cpu_baseline": {"value": value, "unit": "classes/s", "cores": cores, "kind": "reference",
-                             "sample": f"full {idx.size}-class list per step, {args.steps} steps"},
+                             "sample": (f"full {idx.size}-class list per step" if idx is full else
+                                        f"seeded sample of {idx.size} of {full.size} classes per step") +
+                                       f", {args.steps} steps"},
             "e2e": {"value": value, "unit": "classes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -250,6 +270,15 @@ def run_ours(args):
                                           C.c_void_p(out.data_ptr()), sptr)
         if rc:
             raise RuntimeError(L.gli_b200_last_error_message().decode())
+
+    if args.profile_only:
+        # untimed evaluations of the chosen form only (the command profilers run)
+        for _ in range(args.profile_only):
+            step(FORMS[chosen])
+        stream.synchronize()
+        L.gli_b200_free_dev(d_idx, sptr)
+        log(f"{args.profile_only} evaluations of the {chosen} form")
+        return 0
 
     log(f"{m} classes; accuracy check")
     vals = {}
@@ -348,8 +377,8 @@ def run_ours(args):
         log("CPU baseline (reference core, separate process)")
         try:
             tmp = tempfile.mktemp(suffix=".npz")
-            np.savez(tmp, fp64=vals["fp64"], mixed=vals["mixed"])
-            cpu = cpu_baseline_subprocess(tmp)
+            np.savez(tmp, fp64=vals["fp64"], mixed=vals["mixed"], indices=idx_np)
+            cpu = cpu_baseline_subprocess(tmp, args.workload)
             os.unlink(tmp)
         except Exception as ex:  # the reference core must be prebuilt (make -C oracle ref)
             cpu = {"value": None, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
@@ -383,6 +412,136 @@ def run_ours(args):
     }
     print(json.dumps(line), flush=True)
     L.gli_b200_free_dev(d_idx, sptr)
+    return 0
+
+
+def run_nuclear_batch(args):
+    """Config: 256 linear H_n chains (n uniform in 2..8, bonds 1.0-3.0 bohr,
+    jitter N(0, 0.1) bohr), each on its own centred grid of 8^3..24^3 points at
+    0.5 bohr; every matrix written to its own device buffer; one call per step
+    (one CUDA graph per chunk of instances).  Metric: instances per second and
+    matrix GB/s written; the mixed form's max abs error against FP64 in Ha on
+    the first instances."""
+    import torch
+    import gausslectronitegrate_b200 as gli
+    from gausslectronitegrate_b200 import _abi
+    L = gli.lib()
+    count = args.instances
+    grids, pos, q = h_chain_batch(np.random.default_rng(2024), count, 8, 24, 0.5)
+    n = len(grids)
+    specs = [gli._parse_grid(g, "") for g in grids]
+    gstructs = (_abi.Grid * n)(*[gli._grid_struct(sp) for sp in specs])
+    nucs, offs = [], [0]
+    for p_, q_ in zip(pos, q):
+        arr, cnt = gli._parse_nuclei(p_, q_, "")
+        nucs.extend(arr[k] for k in range(cnt))
+        offs.append(offs[-1] + cnt)
+    nuc_arr = (_abi.Nucleus * len(nucs))(*nucs)
+    off = np.asarray(offs, dtype=np.int64)
+    Ns = [sp[0][1] * sp[1][1] * sp[2][1] for sp in specs]
+    total_bytes = 8 * sum(N * N for N in Ns)
+    outs = [torch.empty(N * N, dtype=torch.float64, device="cuda") for N in Ns]
+    ptrs = (C.c_void_p * n)(*[o.data_ptr() for o in outs])
+    gd, keep = gli._parse_coeffs(np.ascontiguousarray(g10()), "")
+    stream = torch.cuda.Stream()
+    forms = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}
+
+    def call(f):
+        rc = L.gli_b200_nuclear_batch_dev(C.byref(gd), n, gstructs, off.ctypes.data_as(_abi.lptr), nuc_arr, 1e-8,
+                                          forms[f], ptrs, C.c_void_p(stream.cuda_stream))
+        if rc:
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+
+    if args.profile_only:
+        for _ in range(args.profile_only):
+            call(args.form)
+        stream.synchronize()
+        return 0
+    res = {}
+    first = {}
+    for f in ("fp64", "mixed"):
+        for _ in range(max(args.warmup, 3)):
+            call(f)
+        stream.synchronize()
+        first[f] = [o[:16384].cpu().numpy().copy() for o in outs[:4]]
+        clocks = Clocks(0) if f == args.form else None
+        ms = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call(f)
+            e1.record(stream)
+            stream.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        res[f] = {"ms_per_step": sum(ms) / len(ms), "instances_per_s": n / (sum(ms) / len(ms) * 1e-3),
+                  "matrix_gb_per_s": total_bytes / (sum(ms) / len(ms) * 1e-3) / 1e9,
+                  "clocks": clocks.stop() if clocks else None}
+    err = max(float(np.max(np.abs(a - b))) for a, b in zip(first["mixed"], first["fp64"])) / 0.5
+    stats = (_abi.glong * 3)()
+    L.gli_b200_last_nuclear_batch(stats)
+    buf = C.create_string_buffer(65536)
+    L.gli_b200_autotune_report(buf, 65536)
+    main_ = res[args.form]
+    line = {"metric": "nuclear matrices/sec on 1 B200 (batched H_n chains)", "value": main_["instances_per_s"],
+            "unit": "instances/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": main_["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.form == "fp64" else "s8 tensor-core slices + f64", "data": "synthetic",
+            "config": {"workload": f"{n} H_n chains (n 2..8), grids 8^3..24^3 at 0.5 bohr, G10, tol 1e-8",
+                       "matrix_bytes_per_step": total_bytes, "forms": res,
+                       "max_abs_err_ha_mixed_vs_fp64_first4": err, "graph_chunks": int(stats[1]),
+                       "streams": int(stats[2]), "autotune": json.loads(buf.value.decode())},
+            "clocks": main_["clocks"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_surrogate(args):
+    """Config: ERIDA 128^3 (odd stand-in 129^3) at 0.3 bohr with the far-field
+    surrogate: train on exact classes, evaluate with a 1% seeded audit at
+    1e-6 Ha, compare with the exact evaluation."""
+    import gausslectronitegrate_b200 as gli
+    from gausslectronitegrate_b200 import _abi
+    L = gli.lib()
+    gd, keep = gli._parse_coeffs(np.ascontiguousarray(g10()), "")
+    t0 = time.perf_counter()
+    h = C.c_void_p()
+    rc = L.gli_b200_surrogate_train(C.byref(gd), TOL, 12.0, args.train_steps, 2e-3, 0.0, 7, C.byref(h))
+    if rc:
+        raise RuntimeError(L.gli_b200_last_error_message().decode())
+    train_s = time.perf_counter() - t0
+    info = (C.c_double * 13)()
+    L.gli_b200_surrogate_info(h, info)
+    grid = [(-64, 129)] * 3
+    gs = gli._grid_struct(grid)
+    ex = gli.compute_sparse_erida_gausslet_integrals(g10(), grid, TOL)
+    idx = ex.indices
+    shell_tol = 1e-6 * 0.3
+    vals = np.empty(idx.size)
+    rep = np.zeros((256, 4))
+    exact_ms, sur_ms = [], []
+    for _ in range(max(args.steps, 2)):
+        t0 = time.perf_counter()
+        L.gli_b200_sparse_values(0, C.byref(gd), C.byref(gs), idx.ctypes.data_as(_abi.lptr), idx.size, TOL, 0,
+                                 vals.ctypes.data_as(_abi.dptr))
+        exact_ms.append(1e3 * (time.perf_counter() - t0))
+        t0 = time.perf_counter()
+        rc = L.gli_b200_erida_surrogate_values(h, C.byref(gd), C.byref(gs), idx.ctypes.data_as(_abi.lptr), idx.size,
+                                               TOL, 0.01, 11, shell_tol, vals.ctypes.data_as(_abi.dptr),
+                                               rep.ctypes.data_as(_abi.dptr), 256)
+        sur_ms.append(1e3 * (time.perf_counter() - t0))
+        if rc:
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+    L.gli_b200_surrogate_free(h)
+    err = np.abs(vals - ex.values)
+    line = {"metric": "ERIDA classes/sec on 1 B200 with the far-field surrogate (1% audit, 1e-6 Ha)",
+            "value": idx.size / (statistics.median(sur_ms[1:]) * 1e-3), "unit": "classes/s", "n_gpus": 1,
+            "steps": len(sur_ms), "warmup": 1, "ms_per_step": statistics.median(sur_ms[1:]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 network + f64 exact", "data": "synthetic",
+            "config": {"workload": WORKLOADS["erida129"][2], "train_s": train_s, "train_steps": args.train_steps,
+                       "surrogate_info": list(info), "exact_ms_host_buffers": statistics.median(exact_ms[1:]),
+                       "max_abs_err_ha": float(err.max() / 0.3), "audited": int(rep[:, 1].sum()),
+                       "shells_evaluated_in_full": [k for k in range(256) if rep[k, 0] > 0 and rep[k, 3] == 1]}}
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -444,9 +603,22 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-json", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--workload", choices=["erida33", "erida129", "nuclear-batch", "erida129-surrogate"],
+                    default="erida33", help="erida33 is the metric's configuration (the default line)")
+    ap.add_argument("--profile-only", type=int, default=0, metavar="K",
+                    help="run K untimed evaluations of --form and print nothing (for profilers)")
+    ap.add_argument("--instances", type=int, default=256, help="nuclear-batch: number of H_n chains")
+    ap.add_argument("--train-steps", type=int, default=40000, help="erida129-surrogate: training steps")
     args = ap.parse_args()
+    global L_GRID, SPACING, WORKLOAD
+    if args.workload in WORKLOADS:
+        L_GRID, SPACING, WORKLOAD = WORKLOADS[args.workload]
     if args.cpu_baseline_json:
         return cpu_baseline_main(args.cpu_baseline_json)
+    if args.workload == "nuclear-batch":
+        return run_nuclear_batch(args)
+    if args.workload == "erida129-surrogate":
+        return run_surrogate(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
