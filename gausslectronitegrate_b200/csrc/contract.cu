@@ -349,8 +349,8 @@ struct LatticeGRows {
     const double* T;
     const int* S;
     __device__ double operator()(i64 r, int k) const { return T[S[r] + k * k]; }
-    __device__ i64 dest(i64 r) const { return r; }
     __device__ bool valid(i64) const { return true; }
+    GLI_IDENTITY_ROWS
 };
 
 struct AKeyRows {  // A key a: row W[aKey[a]]
@@ -359,8 +359,8 @@ struct AKeyRows {  // A key a: row W[aKey[a]]
     const PlanCounts* cnt;
     i64 Up;
     __device__ double operator()(i64 a, int k) const { return W[(i64)aKey[a] * Up + k]; }
-    __device__ i64 dest(i64 a) const { return a; }
     __device__ bool valid(i64 a) const { return a < cnt->nA; }
+    GLI_IDENTITY_ROWS
 };
 
 struct ExpandedHRows {  // row r = a * U + u of the stacked Hf[a], batch a padded to whole tiles
@@ -374,6 +374,10 @@ struct ExpandedHRows {  // row r = a * U + u of the stacked Hf[a], batch a padde
         return H[a * nS + sidx[u * U + k]];
     }
     __device__ i64 dest(i64 r) const { return (r / U) * blocks * TC_BM + r % U; }
+    __device__ i64 source(i64 d, i64 rows) const {
+        const i64 a = d / ((i64)blocks * TC_BM), u = d % ((i64)blocks * TC_BM);
+        return (u < U && a * U + u < rows) ? a * U + u : -1;
+    }
     __device__ bool valid(i64 r) const { return r < cnt->nA * U; }
 };
 
@@ -381,8 +385,10 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
     const double* W;
     const int* pairA;
     const int* pairB;
-    const int* first;  // first pair of each A key
-    const int* tile0;  // first tile of each A key
+    const int* first;       // first pair of each A key
+    const int* tile0;       // first tile of each A key
+    const int* tile_col0;   // first pair of each tile
+    const int* tile_ncols;  // pairs in each tile
     const PlanCounts* cnt;
     i64 Up;
     int bn;  // rows per tile
@@ -390,6 +396,12 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
     __device__ i64 dest(i64 p) const {
         const int a = pairA[p];
         return (i64)tile0[a] * bn + (p - first[a]);
+    }
+    __device__ i64 source(i64 d, i64 rows) const {
+        const i64 t = d / bn;
+        const int j = (int)(d % bn);
+        const i64 p = j < tile_ncols[t] ? (i64)tile_col0[t] + j : -1;
+        return p < rows ? p : -1;
     }
     __device__ bool valid(i64 p) const { return p < (i64)cnt->nP; }
 };
@@ -401,8 +413,8 @@ struct UsedKeyRows {
     const PlanCounts* cnt;
     i64 Up;
     __device__ double operator()(i64 j, int k) const { return W[(i64)keyOf[j] * Up + k]; }
-    __device__ i64 dest(i64 j) const { return j; }
     __device__ bool valid(i64 j) const { return j < cnt->nku; }
+    GLI_IDENTITY_ROWS
 };
 
 // dense rows whose count lives in device memory (PlanCounts::nP)
@@ -411,8 +423,8 @@ struct PairCountedRows {
     const PlanCounts* cnt;
     i64 ld;
     __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
-    __device__ i64 dest(i64 r) const { return r; }
     __device__ bool valid(i64 r) const { return r < (i64)cnt->nP; }
+    GLI_IDENTITY_ROWS
 };
 
 // One block: first pair, pair count and first tile of every A key (pairs are
@@ -491,9 +503,7 @@ static TiledOperand lattice_g_slices(const LatticeTables& t, cudaStream_t s) {
         g->data.alloc((size_t)MIXED_SLICES * rows * nkc * TC_BK);
         g->e.alloc((size_t)rows);
         g->view = TiledOperand{g->data.p, g->e.p, nkc, MIXED_SLICES};
-        k_slice_tiled<LatticeGRows><<<(unsigned)((t.nS * 32 + 255) / 256), 256, 0, s>>>(
-            LatticeGRows{t.T.p, t.S.p}, t.nS, (int)t.U, nkc, MIXED_SLICES, TC_BM, g->data.p, g->e.p);
-        GLI_CHECK_LAUNCH();
+        launch_slice(LatticeGRows{t.T.p, t.S.p}, t.nS, rows, (int)t.U, nkc, MIXED_SLICES, TC_BM, g->data.p, g->e.p, s);
         GLI_CUDA(cudaStreamSynchronize(s));
         t.g_sliced = std::move(g);
     }
@@ -686,7 +696,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
                                         tile_ncols);
         GLI_CHECK_LAUNCH();
         Wb.alloc(max_tiles, BN, U, MIXED_SLICES, s);
-        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, cnt, Up, BN}, nP, U, Wb, s);
+        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, tile_col0, tile_ncols, cnt, Up, BN}, nP, U, Wb,
+                    s);
         TileWork w;
         w.a_rows = U;
         w.a_blocks = mb;

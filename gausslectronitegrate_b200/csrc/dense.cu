@@ -184,8 +184,8 @@ struct KeyedSlabRows {
         point_of(G, l, p[3]);
         return table[eri_key_slot(p, G.L)];
     }
-    __device__ i64 dest(i64 r) const { return r; }
     __device__ bool valid(i64) const { return true; }
+    GLI_IDENTITY_ROWS
 };
 
 // row s of the transpose of a row-major matrix with leading dimension ld
@@ -193,8 +193,8 @@ struct TransposedRows {
     const double* src;
     i64 ld;
     __device__ double operator()(i64 r, int k) const { return src[(i64)k * ld + r]; }
-    __device__ i64 dest(i64 r) const { return r; }
     __device__ bool valid(i64) const { return true; }
+    GLI_IDENTITY_ROWS
 };
 
 // 48 x N permutation tables: perm[g][i] = linear index of O_h element g applied to point i

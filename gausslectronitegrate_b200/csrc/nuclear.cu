@@ -168,6 +168,10 @@ struct BatchedRows {
     int rows, blocks;
     __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
     __device__ i64 dest(i64 r) const { return (r / rows) * blocks * TC_BM + r % rows; }
+    __device__ i64 source(i64 d, i64 total) const {
+        const i64 b = d / ((i64)blocks * TC_BM), i = d % ((i64)blocks * TC_BM);
+        return (i < rows && b * rows + i < total) ? b * rows + i : -1;
+    }
     __device__ bool valid(i64) const { return true; }
 };
 

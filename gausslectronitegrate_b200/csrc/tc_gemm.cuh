@@ -57,82 +57,144 @@ struct TiledSlices {
     TiledOperand view() const { return TiledOperand{data.p, e.p, nkc, S}; }
 };
 
-// Writes the slices of source rows r = 0 .. rows-1 (src(r, k), k < K) to their
-// padded rows src.dest(r); rows with !src.valid(r) (beyond a count that lives
-// in device memory) are skipped.  One warp per row; for K <= 512 each lane
-// gathers one 16-value piece of the row once into registers, longer rows are
-// read twice (maximum, then slices).  Src: device functor with `double
-// operator()(i64 r, int k) const`, `i64 dest(i64 r) const` and `bool valid(i64
-// r) const`.
-template <class Src>
-__global__ void k_slice_tiled(Src src, i64 rows, int K, int nkc, int S, int RB, int8_t* __restrict__ dst,
-                              int* __restrict__ e) {
-    const i64 r = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (r >= rows || !src.valid(r)) return;  // uniform across the warp
-    const int pieces = nkc * (TC_BK / 16);
-    const bool one_pass = pieces <= 32;
-    double x[16];
-    double mx = 0;
-    if (one_pass) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int k = lane * 16 + j;
-            x[j] = (lane < pieces && k < K) ? src(r, k) : 0.0;
-            mx = fmax(mx, fabs(x[j]));
-        }
-    } else {
-        for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(src(r, k)));
-    }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+// Slicing kernels.  Src is a device functor with
+//   double operator()(i64 r, int k) const   value of source row r, column k < K
+//   i64 dest(i64 r) const                   padded row of source row r
+//   i64 source(i64 d, i64 rows) const       source row of padded row d, or -1
+//   bool valid(i64 r) const                 false beyond a count in device memory
+// Every row x is split as 2^e sum_p 2^(-7(p+1)) d_p (|x| 2^-e < 1/2).
+
+__device__ inline int slice_exponent(double mx) {
     int ex = 0;
     if (mx > 0) {
         frexp(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
         ex += 1;         // |x| 2^-ex < 1/2
     }
+    return ex;
+}
+
+// 16 values -> S slices of 16 int8 each (packed in uint4)
+__device__ inline void slice_piece(double (&v)[16], int S, uint4* out) {
+    for (int p = 0; p < S; ++p) {
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const double t = v[j] * 128.0;
+            const double d = rint(t);  // |t| <= 64
+            v[j] = t - d;              // exact in FP64, |v| <= 1/2
+            w[j >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (j & 3));
+        }
+        out[p] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+constexpr int SLICE_GROUP_NKC = 8;  // K <= 512 for the grouped kernel
+constexpr int SLICE_GROUP_S = 7;
+
+// One block per group of 8 padded rows (8 warps, warp w slices row 8 g + w,
+// one 16-value piece per lane).  The slices are staged in shared memory in
+// the tiled order and written out as contiguous 512-byte runs (8 rows x 64
+// bytes of K per slice and chunk); padding rows are written as zeros.
+template <class Src>
+__global__ void __launch_bounds__(256) k_slice_group(Src src, i64 rows, int K, int nkc, int S, int RB,
+                                                     int8_t* __restrict__ dst, int* __restrict__ e) {
+    __shared__ uint4 stage[SLICE_GROUP_NKC][SLICE_GROUP_S][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const i64 d0 = (i64)blockIdx.x * 8, dr = d0 + w;
+    i64 sr = src.source(dr, rows);
+    if (sr >= 0 && !src.valid(sr)) sr = -1;
+    const int pieces = nkc * (TC_BK / 16);
+    double x[16];
+    double mx = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int k = lane * 16 + j;
+        x[j] = (sr >= 0 && lane < pieces && k < K) ? src(sr, k) : 0.0;
+        mx = fmax(mx, fabs(x[j]));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int ex = slice_exponent(mx);
+    if (lane == 0) e[dr] = ex;
+    if (lane < pieces) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = mx > 0 ? ldexp(x[j], -ex) : 0.0;
+        uint4 sl[SLICE_GROUP_S];
+        slice_piece(x, S, sl);
+        // position inside the 512-byte block of (chunk, slice): piece-in-chunk * 128 + row * 16
+        for (int p = 0; p < S; ++p) stage[lane >> 2][p][(lane & 3) * 8 + w] = sl[p];
+    }
+    __syncthreads();
+    const i64 rb = d0 / RB;
+    const int grp = (int)((d0 % RB) >> 3);
+    for (int t = threadIdx.x; t < nkc * S * 32; t += blockDim.x) {
+        const int kc = t / (S * 32), p = (t / 32) % S, q = t % 32;
+        uint4* out = reinterpret_cast<uint4*>(dst + ((rb * nkc + kc) * S + p) * (i64)RB * TC_BK +
+                                              (i64)grp * (TC_BK / 16) * 128);
+        out[q] = stage[kc][p][q];
+    }
+}
+
+// Rows of any length: one warp per source row, two passes over the row
+// (maximum, then slices), 16-byte stores.  Padding rows are left unwritten.
+template <class Src>
+__global__ void k_slice_rows_any(Src src, i64 rows, int K, int nkc, int S, int RB, int8_t* __restrict__ dst,
+                                 int* __restrict__ e) {
+    const i64 r = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows || !src.valid(r)) return;  // uniform across the warp
+    double mx = 0;
+    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(src(r, k)));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int ex = slice_exponent(mx);
     const i64 pr = src.dest(r);
     const i64 rb = pr / RB;
     const int rr = (int)(pr % RB);
     if (lane == 0) e[pr] = ex;
+    const int pieces = nkc * (TC_BK / 16);
     for (int pc = lane; pc < pieces; pc += 32) {
         double v[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int k = pc * 16 + j;
-            const double xv = one_pass ? x[j] : (k < K ? src(r, k) : 0.0);
-            v[j] = mx > 0 ? ldexp(xv, -ex) : 0.0;
+            v[j] = (k < K && mx > 0) ? ldexp(src(r, k), -ex) : 0.0;
         }
         const int kc = pc / (TC_BK / 16), k0 = (pc % (TC_BK / 16)) * 16;
-        for (int p = 0; p < S; ++p) {
-            uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const double t = v[j] * 128.0;
-                const double d = rint(t);  // |t| <= 64
-                v[j] = t - d;              // exact in FP64, |v| <= 1/2
-                w[j >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (j & 3));
-            }
-            *reinterpret_cast<uint4*>(dst + tiled_offset(rb, kc, p, rr, k0, nkc, S, RB)) =
-                make_uint4(w[0], w[1], w[2], w[3]);
-        }
+        uint4 sl[8];
+        slice_piece(v, S, sl);
+        for (int p = 0; p < S; ++p)
+            *reinterpret_cast<uint4*>(dst + tiled_offset(rb, kc, p, rr, k0, nkc, S, RB)) = sl[p];
     }
+}
+
+// slices of source rows 0 .. rows-1 into a tiled operand with padded_rows rows
+template <class Src>
+void launch_slice(const Src& src, i64 rows, i64 padded_rows, int K, int nkc, int S, int RB, int8_t* dst, int* e,
+                  cudaStream_t s) {
+    if (rows <= 0 || padded_rows <= 0) return;
+    if (nkc <= SLICE_GROUP_NKC && S <= SLICE_GROUP_S && RB % 8 == 0)
+        k_slice_group<Src><<<(unsigned)(padded_rows / 8), 256, 0, s>>>(src, rows, K, nkc, S, RB, dst, e);
+    else
+        k_slice_rows_any<Src><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(src, rows, K, nkc, S, RB, dst, e);
+    GLI_CHECK_LAUNCH();
 }
 
 template <class Src>
 void slice_tiled(const Src& src, i64 rows, int K, TiledSlices& out, cudaStream_t s) {
-    if (rows <= 0) return;
-    k_slice_tiled<Src><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, s>>>(src, rows, K, out.nkc, out.S, out.RB,
-                                                                          out.data.p, out.e.p);
-    GLI_CHECK_LAUNCH();
+    launch_slice(src, rows, out.blocks * out.RB, K, out.nkc, out.S, out.RB, out.data.p, out.e.p, s);
 }
+
+// identity row placement (source row r = padded row r), for the functors below
+#define GLI_IDENTITY_ROWS                                          \
+    __device__ i64 dest(i64 r) const { return r; }                 \
+    __device__ i64 source(i64 d, i64 rows) const { return d < rows ? d : -1; }
 
 // source functors ----------------------------------------------------------------
 struct DenseRows {  // row r at src + r * ld
     const double* src;
     i64 ld;
     __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
-    __device__ i64 dest(i64 r) const { return r; }
     __device__ bool valid(i64) const { return true; }
+    GLI_IDENTITY_ROWS
 };
 
 struct GatheredRows {  // row r at src + rowmap[r] * ld
@@ -140,8 +202,8 @@ struct GatheredRows {  // row r at src + rowmap[r] * ld
     const int* rowmap;
     i64 ld;
     __device__ double operator()(i64 r, int k) const { return src[(i64)rowmap[r] * ld + k]; }
-    __device__ i64 dest(i64 r) const { return r; }
     __device__ bool valid(i64) const { return true; }
+    GLI_IDENTITY_ROWS
 };
 
 // Work of one launch.  The A side has a_rows valid rows per batch in a_blocks
