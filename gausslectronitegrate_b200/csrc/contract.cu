@@ -348,7 +348,8 @@ __global__ void k_gather_q(const double* __restrict__ Q, const int2* __restrict_
 struct LatticeGRows {
     const double* T;
     const int* S;
-    __device__ double operator()(i64 r, int k) const { return T[S[r] + k * k]; }
+    __device__ RowBase row(i64 r) const { return {T + S[r]}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k * k]; }
     __device__ bool valid(i64) const { return true; }
     GLI_IDENTITY_ROWS
 };
@@ -358,7 +359,8 @@ struct AKeyRows {  // A key a: row W[aKey[a]]
     const int* aKey;
     const PlanCounts* cnt;
     i64 Up;
-    __device__ double operator()(i64 a, int k) const { return W[(i64)aKey[a] * Up + k]; }
+    __device__ RowBase row(i64 a) const { return {W + (i64)aKey[a] * Up}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ bool valid(i64 a) const { return a < cnt->nA; }
     GLI_IDENTITY_ROWS
 };
@@ -369,10 +371,15 @@ struct ExpandedHRows {  // row r = a * U + u of the stacked Hf[a], batch a padde
     const PlanCounts* cnt;
     i64 nS;
     int U, blocks;
-    __device__ double operator()(i64 r, int k) const {
-        const i64 a = r / U, u = r % U;
-        return H[a * nS + sidx[u * U + k]];
+    struct Ctx {
+        const double* h;  // H row of the A key
+        const int* map;   // sidx row u
+    };
+    __device__ Ctx row(i64 r) const {
+        const i64 a = r / U, u = r - a * U;
+        return {H + a * nS, sidx + u * U};
     }
+    __device__ double at(const Ctx& c, int k) const { return c.h[c.map[k]]; }
     __device__ i64 dest(i64 r) const { return (r / U) * blocks * TC_BM + r % U; }
     __device__ i64 source(i64 d, i64 rows) const {
         const i64 a = d / ((i64)blocks * TC_BM), u = d % ((i64)blocks * TC_BM);
@@ -392,7 +399,8 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
     const PlanCounts* cnt;
     i64 Up;
     int bn;  // rows per tile
-    __device__ double operator()(i64 p, int k) const { return W[(i64)pairB[p] * Up + k]; }
+    __device__ RowBase row(i64 p) const { return {W + (i64)pairB[p] * Up}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ i64 dest(i64 p) const {
         const int a = pairA[p];
         return (i64)tile0[a] * bn + (p - first[a]);
@@ -412,7 +420,8 @@ struct UsedKeyRows {
     const int* keyOf;
     const PlanCounts* cnt;
     i64 Up;
-    __device__ double operator()(i64 j, int k) const { return W[(i64)keyOf[j] * Up + k]; }
+    __device__ RowBase row(i64 j) const { return {W + (i64)keyOf[j] * Up}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ bool valid(i64 j) const { return j < cnt->nku; }
     GLI_IDENTITY_ROWS
 };
@@ -422,7 +431,8 @@ struct PairCountedRows {
     const double* src;
     const PlanCounts* cnt;
     i64 ld;
-    __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
+    __device__ RowBase row(i64 r) const { return {src + r * ld}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ bool valid(i64 r) const { return r < (i64)cnt->nP; }
     GLI_IDENTITY_ROWS
 };

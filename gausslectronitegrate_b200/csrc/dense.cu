@@ -176,11 +176,23 @@ struct KeyedSlabRows {
     SymGrid G;
     const double* table;
     i64 i;
-    __device__ double operator()(i64 r, int l) const {
+    struct Ctx {
+        int p[3][3];  // points i, j, k of the row
+    };
+    __device__ Ctx row(i64 r) const {
+        Ctx c;
+        point_of(G, i, c.p[0]);
+        point_of(G, r / G.N, c.p[1]);
+        point_of(G, r % G.N, c.p[2]);
+        return c;
+    }
+    __device__ double at(const Ctx& c, int l) const {
         int p[4][3];
-        point_of(G, i, p[0]);
-        point_of(G, r / G.N, p[1]);
-        point_of(G, r % G.N, p[2]);
+        for (int a = 0; a < 3; ++a) {
+            p[0][a] = c.p[0][a];
+            p[1][a] = c.p[1][a];
+            p[2][a] = c.p[2][a];
+        }
         point_of(G, l, p[3]);
         return table[eri_key_slot(p, G.L)];
     }
@@ -192,7 +204,11 @@ struct KeyedSlabRows {
 struct TransposedRows {
     const double* src;
     i64 ld;
-    __device__ double operator()(i64 r, int k) const { return src[(i64)k * ld + r]; }
+    struct Ctx {
+        const double* p;
+    };
+    __device__ Ctx row(i64 r) const { return {src + r}; }
+    __device__ double at(const Ctx& c, int k) const { return c.p[(i64)k * ld]; }
     __device__ bool valid(i64) const { return true; }
     GLI_IDENTITY_ROWS
 };

@@ -166,7 +166,8 @@ struct BatchedRows {
     const double* src;
     i64 ld;
     int rows, blocks;
-    __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
+    __device__ RowBase row(i64 r) const { return {src + r * ld}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ i64 dest(i64 r) const { return (r / rows) * blocks * TC_BM + r % rows; }
     __device__ i64 source(i64 d, i64 total) const {
         const i64 b = d / ((i64)blocks * TC_BM), i = d % ((i64)blocks * TC_BM);

@@ -14,7 +14,7 @@
 // the integral stages) and S = 7, R = 8 (about 2^-50: FP64 level).
 //
 // One CTA computes a 128 x N tile of C (N = tile_n(S): 96 for S = 5, 64 for
-// S = 7) with 128 threads:
+// S = 7) with 256 threads:
 //   * warp 0 allocates 512 tensor-memory columns (R regions of N used);
 //   * lane 0 of warp 0 is the producer: for every K chunk of 64 bytes it
 //     issues two bulk copies (all S slices of the A tile, all S slices of the B
@@ -24,8 +24,9 @@
 //     (p, q) two MMAs (K = 32 each) of the A_p tile with the B_q tile into
 //     region p + q, then commits to the stage's `empty` mbarrier, which hands
 //     the stage back to the producer; after the last chunk it commits to `done`;
-//   * all four warps wait on `done`, then read their 32 lanes (rows) of every
-//     region with tcgen05.ld, 16 columns at a time, and write FP64 results.
+//   * all eight warps wait on `done`; warp w reads TMEM lanes 32 (w % 4) ..
+//     +31 (its rows) of every region for half of the columns with tcgen05.ld,
+//     combines the regions exactly in int64 and converts once to FP64.
 // Every mbarrier wait is bounded by wall time (1 s).  On expiry the CTA records
 // an error, stops issuing, waits (bounded) for the work it issued, frees its
 // tensor memory and returns.  The kernel uses no cluster and no multicast.
@@ -133,8 +134,30 @@ __host__ __device__ constexpr int smem_bytes() { return stages_for<S>() * S * (T
 // first slice p of the pairs (p, q) with p + q = r, p, q < S
 __host__ __device__ constexpr int first_p(int r, int S) { return r < S ? 0 : r - (S - 1); }
 
+// 2^e for |e| <= 1000, built from its bit pattern (exact)
+__device__ __forceinline__ double pow2(int e) { return __hiloint2double((1023 + e) << 20, 0); }
+
+// the regions of one output, combined exactly in integers and converted once:
+// region r carries weight 2^(-7 (r + 2))
+template <int R>
+__device__ __forceinline__ double combine_regions(const uint32_t (&v)[R][16], int j) {
+    if constexpr (R <= 5) {
+        long long s = (int32_t)v[0][j];  // |region| < 2^29: R <= 5 regions fit 2^57
+#pragma unroll
+        for (int r = 1; r < R; ++r) s = s * 128 + (int32_t)v[r][j];
+        return (double)s * pow2(-7 * (R + 1));
+    } else {
+        long long hi = (int32_t)v[0][j], lo = (int32_t)v[4][j];
+#pragma unroll
+        for (int r = 1; r < 4; ++r) hi = hi * 128 + (int32_t)v[r][j];
+#pragma unroll
+        for (int r = 5; r < R; ++r) lo = lo * 128 + (int32_t)v[r][j];
+        return fma((double)hi, pow2(-35), (double)lo * pow2(-7 * (R + 1)));
+    }
+}
+
 template <int S, int R>
-__global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand B, TileWork w, int* __restrict__ err) {
+__global__ void __launch_bounds__(256, 1) k_tc_gemm(TiledOperand A, TiledOperand B, TileWork w, int* __restrict__ err) {
     constexpr int TC_BN = tile_n(S);
     static_assert(R * TC_BN <= TC_TMEM_COLS, "tensor-memory regions exceed 512 columns");
     static_assert(TC_BN % 16 == 0 && TC_BN >= 16 && TC_BN <= 256, "MMA N out of range for M = 128");
@@ -238,28 +261,30 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(TiledOperand A, TiledOperand
     __syncthreads();
 
     if (!abort_flag) {
-        const int row = warp * 32 + lane;
+        // eight warps: warp w reads TMEM lanes 32 (w % 4) .. (its rows) and half
+        // of the columns
+        const int quarter = warp & 3, half = warp >> 2;
+        const int row = quarter * 32 + lane;
         const bool live = row < rows_valid;
         const int ea = live ? A.e[a_rb * TC_BM + row] : 0;
         double* crow = w.C + (i64)(mt * TC_BM + row) * w.rs;
         const int* eb = B.e + b_rb * TC_BN;
-        for (int c0 = 0; c0 < TC_BN; c0 += 16) {
-            double acc[16];
+        constexpr int HALF = TC_BN / 2;
+        static_assert(HALF % 16 == 0, "column halves of whole 16-column loads");
+        for (int c0 = half * HALF; c0 < (half + 1) * HALF; c0 += 16) {
+            uint32_t v[R][16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                uint32_t v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * TC_BN + c0), v);
-                const double sc = ldexp(1.0, -7 * (r + 2));
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = fma((double)(int32_t)v[j], sc, acc[j]);
-            }
+            for (int r = 0; r < R; ++r)
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(r * TC_BN + c0), v[r]);
             if (live) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int c = c0 + j;
-                    if (c < ncols) crow[(i64)(col0 + c) * w.cs] = ldexp(acc[j], ea + eb[c]);
+                    if (c < ncols) {
+                        const int ex = ea + eb[c];
+                        const double acc = combine_regions<R>(v, j);
+                        crow[(i64)(col0 + c) * w.cs] = (ex >= -1000 && ex <= 1000) ? acc * pow2(ex) : ldexp(acc, ex);
+                    }
                 }
             }
         }
@@ -288,7 +313,7 @@ static void launch_variant(const TiledOperand& A, const TiledOperand& B, const T
                            cudaStream_t s) {
     constexpr int smem = smem_bytes<S>();
     dim3 grid((unsigned)ntiles, (unsigned)w.a_blocks);
-    k_tc_gemm<S, R><<<grid, 128, smem, s>>>(A, B, w, err);
+    k_tc_gemm<S, R><<<grid, 256, smem, s>>>(A, B, w, err);
     GLI_CHECK_LAUNCH();
 }
 

@@ -58,7 +58,9 @@ struct TiledSlices {
 };
 
 // Slicing kernels.  Src is a device functor with
-//   double operator()(i64 r, int k) const   value of source row r, column k < K
+//   Ctx row(i64 r) const                    per-row context of source row r (bases,
+//                                           maps: whatever is computed once per row)
+//   double at(const Ctx& c, int k) const    value of that row at column k < K
 //   i64 dest(i64 r) const                   padded row of source row r
 //   i64 source(i64 d, i64 rows) const       source row of padded row d, or -1
 //   bool valid(i64 r) const                 false beyond a count in device memory
@@ -91,37 +93,45 @@ __device__ inline void slice_piece(double (&v)[16], int S, uint4* out) {
 constexpr int SLICE_GROUP_NKC = 8;  // K <= 512 for the grouped kernel
 constexpr int SLICE_GROUP_S = 7;
 
-// One block per group of 8 padded rows (8 warps, warp w slices row 8 g + w,
-// one 16-value piece per lane).  The slices are staged in shared memory in
-// the tiled order and written out as contiguous 512-byte runs (8 rows x 64
-// bytes of K per slice and chunk); padding rows are written as zeros.
+// One block per group of 8 padded rows (8 warps, warp w slices row 8 g + w).
+// Lane l holds columns k = l + 32 j (coalesced reads of the source row); each
+// value's slices go byte by byte into a shared-memory stage laid out in the
+// tiled order, which the block then writes as contiguous 512-byte runs (8 rows
+// x 64 bytes of K per slice and chunk).  Padding rows are written as zeros.
 template <class Src>
 __global__ void __launch_bounds__(256) k_slice_group(Src src, i64 rows, int K, int nkc, int S, int RB,
                                                      int8_t* __restrict__ dst, int* __restrict__ e) {
-    __shared__ uint4 stage[SLICE_GROUP_NKC][SLICE_GROUP_S][32];
+    __shared__ __align__(16) int8_t stage[SLICE_GROUP_NKC][SLICE_GROUP_S][512];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const i64 d0 = (i64)blockIdx.x * 8, dr = d0 + w;
     i64 sr = src.source(dr, rows);
     if (sr >= 0 && !src.valid(sr)) sr = -1;
-    const int pieces = nkc * (TC_BK / 16);
+    const int Kp = nkc * TC_BK;
     double x[16];
     double mx = 0;
+    const auto rc = src.row(sr < 0 ? 0 : sr);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        const int k = lane * 16 + j;
-        x[j] = (sr >= 0 && lane < pieces && k < K) ? src(sr, k) : 0.0;
+        const int k = lane + 32 * j;
+        x[j] = (sr >= 0 && k < K) ? src.at(rc, k) : 0.0;
         mx = fmax(mx, fabs(x[j]));
     }
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const int ex = slice_exponent(mx);
     if (lane == 0) e[dr] = ex;
-    if (lane < pieces) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = mx > 0 ? ldexp(x[j], -ex) : 0.0;
-        uint4 sl[SLICE_GROUP_S];
-        slice_piece(x, S, sl);
-        // position inside the 512-byte block of (chunk, slice): piece-in-chunk * 128 + row * 16
-        for (int p = 0; p < S; ++p) stage[lane >> 2][p][(lane & 3) * 8 + w] = sl[p];
+    for (int j = 0; j < 16; ++j) {
+        const int k = lane + 32 * j;
+        if (k >= Kp) break;
+        double v = mx > 0 ? ldexp(x[j], -ex) : 0.0;
+        // byte of column k: chunk k / 64, core matrix (k % 64) / 16, row w, byte k % 16
+        int8_t* out = &stage[k >> 6][0][((k & 63) >> 4) * 128 + w * 16 + (k & 15)];
+        for (int p = 0; p < S; ++p) {
+            const double t = v * 128.0;
+            const double d = rint(t);  // |t| <= 64
+            v = t - d;                 // exact in FP64, |v| <= 1/2
+            out[p * 512] = (int8_t)(int)d;
+        }
     }
     __syncthreads();
     const i64 rb = d0 / RB;
@@ -130,7 +140,7 @@ __global__ void __launch_bounds__(256) k_slice_group(Src src, i64 rows, int K, i
         const int kc = t / (S * 32), p = (t / 32) % S, q = t % 32;
         uint4* out = reinterpret_cast<uint4*>(dst + ((rb * nkc + kc) * S + p) * (i64)RB * TC_BK +
                                               (i64)grp * (TC_BK / 16) * 128);
-        out[q] = stage[kc][p][q];
+        out[q] = reinterpret_cast<const uint4*>(&stage[kc][p][0])[q];
     }
 }
 
@@ -142,8 +152,9 @@ __global__ void k_slice_rows_any(Src src, i64 rows, int K, int nkc, int S, int R
     const i64 r = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (r >= rows || !src.valid(r)) return;  // uniform across the warp
+    const auto rc = src.row(r);
     double mx = 0;
-    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(src(r, k)));
+    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(src.at(rc, k)));
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const int ex = slice_exponent(mx);
     const i64 pr = src.dest(r);
@@ -156,7 +167,7 @@ __global__ void k_slice_rows_any(Src src, i64 rows, int K, int nkc, int S, int R
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int k = pc * 16 + j;
-            v[j] = (k < K && mx > 0) ? ldexp(src(r, k), -ex) : 0.0;
+            v[j] = (k < K && mx > 0) ? ldexp(src.at(rc, k), -ex) : 0.0;
         }
         const int kc = pc / (TC_BK / 16), k0 = (pc % (TC_BK / 16)) * 16;
         uint4 sl[8];
@@ -189,10 +200,16 @@ void slice_tiled(const Src& src, i64 rows, int K, TiledSlices& out, cudaStream_t
     __device__ i64 source(i64 d, i64 rows) const { return d < rows ? d : -1; }
 
 // source functors ----------------------------------------------------------------
+// context of rows read contiguously from a base pointer
+struct RowBase {
+    const double* p;
+};
+
 struct DenseRows {  // row r at src + r * ld
     const double* src;
     i64 ld;
-    __device__ double operator()(i64 r, int k) const { return src[r * ld + k]; }
+    __device__ RowBase row(i64 r) const { return {src + r * ld}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ bool valid(i64) const { return true; }
     GLI_IDENTITY_ROWS
 };
@@ -201,7 +218,8 @@ struct GatheredRows {  // row r at src + rowmap[r] * ld
     const double* src;
     const int* rowmap;
     i64 ld;
-    __device__ double operator()(i64 r, int k) const { return src[(i64)rowmap[r] * ld + k]; }
+    __device__ RowBase row(i64 r) const { return {src + (i64)rowmap[r] * ld}; }
+    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
     __device__ bool valid(i64) const { return true; }
     GLI_IDENTITY_ROWS
 };
