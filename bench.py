@@ -74,6 +74,22 @@ def grid_spec():
     return [(-(L_GRID // 2), L_GRID)] * 3
 
 
+def weak_scaling_value(my_ms, classes_per_rank, steps, world_size, device):
+    """Whole-job throughput of a weak-scaling run: every rank evaluated its own
+    copy of the workload (classes_per_rank classes per step) in my_ms device
+    milliseconds; the job's time is the slowest rank's (all-reduce MAX), so the
+    value is world_size * classes_per_rank * steps / max time.  Returns (value,
+    max total ms); every rank takes the same collective steps."""
+    import torch
+    t = torch.tensor([float(my_ms)], dtype=torch.float64, device=device)
+    if world_size > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    total_ms = float(t.item())
+    return world_size * classes_per_rank * steps / (total_ms * 1e-3), total_ms
+
+
 def h_chain_batch(rng, count, edge_lo, edge_hi, spacing):
     """Synthetic batch of linear H_n chains (the batched-nuclear workload):
     n uniform in 2..8, bond lengths uniform in 1.0-3.0 bohr, every nucleus
@@ -327,13 +343,9 @@ def run_ours(args):
             clk["window"] = "1 s of untimed steps of the same form ending where the timed steps begin, and the timed steps"
         launches = L.gli_b200_launch_count() - launches0
         my_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
-        t = torch.tensor([my_ms], dtype=torch.float64, device=f"cuda:{local}")
-        if ws > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            torch.distributed.barrier()
-        total_ms = float(t.item())
-        return {"value": ws * m * steps / (total_ms * 1e-3), "ms_per_step": total_ms / steps, "wall_s": wall,
-                "launches": launches, "clocks": clk}
+        value, total_ms = weak_scaling_value(my_ms, m, steps, ws, f"cuda:{local}")
+        return {"value": value, "ms_per_step": total_ms / steps, "wall_s": wall, "launches": launches,
+                "clocks": clk}
 
     log("timed steps")
     main = timed(chosen, args.steps, True)
