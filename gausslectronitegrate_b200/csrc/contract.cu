@@ -177,8 +177,11 @@ template <int KT>
 __global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict__ W, const double* __restrict__ T,
                                                         const int* __restrict__ S, const int* __restrict__ aKey,
                                                         const PlanCounts* __restrict__ cnt, int nS, int U, int Up,
-                                                        double* __restrict__ H) {
+                                                        int t_chunk, i64 part_stride, double* __restrict__ H) {
     __shared__ __align__(16) double ws[A_TC][KT];
+    // blockIdx.z: chunk of t (partial sums of small problems, summed afterwards)
+    const int t_begin = blockIdx.z * t_chunk, t_end = min(U, t_begin + t_chunk);
+    H += (i64)blockIdx.z * part_stride;
     const int j0 = blockIdx.x * A_STILE + threadIdx.x;
     const int j1 = j0 + A_THREADS;
     const int a0 = blockIdx.y * KT;
@@ -189,14 +192,14 @@ __global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict_
     double acc0[KT], acc1[KT];
 #pragma unroll
     for (int k = 0; k < KT; ++k) acc0[k] = acc1[k] = 0;
-    for (int t0 = 0; t0 < U; t0 += A_TC) {
+    for (int t0 = t_begin; t0 < t_end; t0 += A_TC) {
         __syncthreads();
         for (int e = threadIdx.x; e < A_TC * KT; e += A_THREADS) {
             const int k = e / A_TC, tt = e % A_TC, t = t0 + tt;
-            ws[tt][k] = (a0 + k < nA && t < U) ? W[(i64)aKey[a0 + k] * Up + t] : 0.0;
+            ws[tt][k] = (a0 + k < nA && t < t_end) ? W[(i64)aKey[a0 + k] * Up + t] : 0.0;
         }
         __syncthreads();
-        const int tmax = min(A_TC, U - t0);
+        const int tmax = min(A_TC, t_end - t0);
         for (int tt = 0; tt < tmax; ++tt) {
             const int t2 = (t0 + tt) * (t0 + tt);
             const double g0 = __ldg(&T[s0 + t2]);
@@ -243,11 +246,15 @@ __global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__
 
 __global__ void __launch_bounds__(B_THREADS) k_stage_b(const double* __restrict__ W, const double* __restrict__ Hf,
                                                         const int* __restrict__ pairA, const int* __restrict__ pairB,
-                                                        const PlanCounts* __restrict__ cnt, int U, int Up,
-                                                        double* __restrict__ H2) {
+                                                        const PlanCounts* __restrict__ cnt, int U, int Up, int nub,
+                                                        int v_chunk, i64 part_stride, double* __restrict__ H2) {
     __shared__ __align__(16) double wb[B_VC][B_PAIRS];
     __shared__ int range[2];
     const int a = blockIdx.x;
+    // blockIdx.z = u block + nub * (chunk of v): partial sums of small problems
+    const int ub = blockIdx.z % nub, vz = blockIdx.z / nub;
+    const int v_begin = vz * v_chunk, v_end = min(U, v_begin + v_chunk);
+    H2 += (i64)vz * part_stride;
     if (a >= cnt->nA) return;  // grids are sized by a bound on nA
     const int nP = (int)cnt->nP;
     if (threadIdx.x == 0) {
@@ -268,21 +275,21 @@ __global__ void __launch_bounds__(B_THREADS) k_stage_b(const double* __restrict_
     const int pc = range[0] + blockIdx.y * B_PAIRS;
     if (pc >= range[1]) return;  // uniform across the block
     const int np = min(B_PAIRS, range[1] - pc);
-    const int u = blockIdx.z * B_THREADS + threadIdx.x;
+    const int u = ub * B_THREADS + threadIdx.x;
     const bool live = u < U;
     const double* h = Hf + (i64)a * U * U + u;
     double acc[B_PAIRS];
 #pragma unroll
     for (int k = 0; k < B_PAIRS; ++k) acc[k] = 0;
-    for (int v0 = 0; v0 < U; v0 += B_VC) {
+    for (int v0 = v_begin; v0 < v_end; v0 += B_VC) {
         __syncthreads();
         for (int e = threadIdx.x; e < B_VC * B_PAIRS; e += B_THREADS) {
             const int k = e / B_VC, vv = e % B_VC, v = v0 + vv;
-            wb[vv][k] = (k < np && v < U) ? W[(i64)pairB[pc + k] * Up + v] : 0.0;
+            wb[vv][k] = (k < np && v < v_end) ? W[(i64)pairB[pc + k] * Up + v] : 0.0;
         }
         __syncthreads();
         if (live) {
-            const int vmax = min(B_VC, U - v0);
+            const int vmax = min(B_VC, v_end - v0);
             for (int vv = 0; vv < vmax; ++vv) {
                 const double g = h[(i64)(v0 + vv) * U];
                 const double2* w2 = reinterpret_cast<const double2*>(&wb[vv][0]);
@@ -299,6 +306,27 @@ __global__ void __launch_bounds__(B_THREADS) k_stage_b(const double* __restrict_
 #pragma unroll
         for (int k = 0; k < B_PAIRS; ++k)
             if (k < np) H2[(i64)(pc + k) * Up + u] = acc[k];
+}
+
+// out[i] = sum_p parts[p n + i], in order of p (deterministic)
+__global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, double* __restrict__ out) {
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        double acc = parts[i];
+        for (int p = 1; p < P; ++p) acc += parts[(i64)p * n + i];
+        out[i] = acc;
+    }
+}
+
+// Splits of a reduction loop of length U into P chunks (chunk a multiple of
+// `grain`) so that a launch of `blocks` blocks reaches about eight blocks per
+// SM: small problems otherwise leave most SMs idle while each block walks the
+// whole loop.
+static int split_count(i64 blocks, int U, int grain, int num_sms, int* chunk) {
+    int P = (int)std::min<i64>((8LL * num_sms + blocks - 1) / blocks, (U + grain - 1) / grain);
+    P = std::max(1, std::min(P, 8));
+    *chunk = ((U + P - 1) / P + grain - 1) / grain * grain;
+    P = (U + *chunk - 1) / *chunk;
+    return P;
 }
 
 // ---------------------------------------------------------------------------
@@ -653,9 +681,13 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     if (nA * (i64)U * U > ((i64)1 << 31))
         fail(GLI_ERR_LIMIT, "stage buffers exceed 16 GB (%lld A keys, lattice extent %d)", (long long)nA, U);
     DevBuf<double> H(nA * (i64)nS, s);
+    // the mixed form runs a stage on the tensor cores when it is large enough for
+    // them to pay off; smaller stages (latency-bound either way) stay FP64
+    const bool tc_a = a.mixed && nA * (i64)nS >= 1000000;
+    const bool tc_b = a.mixed && nA * (i64)U * U >= 4000000;
     timer.mark();
     // ---- stage A
-    if (a.mixed) {
+    if (tc_a) {
         constexpr int BN = tile_n(MIXED_SLICES);
         TiledSlices Wa;
         const int nbt = (int)((nA + BN - 1) / BN);
@@ -672,24 +704,39 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         tc_gemm_tiled(a.G, Wa.view(), w, nbt, &st->tc_err, s);
     } else {
         // keys per thread: fewer when the problem is small, so that enough
-        // warps exist to hide the table-gather latency
+        // warps exist to hide the table-gather latency; small problems also
+        // split the t loop (partial sums, then one summing pass)
         const i64 outputs = nA * (i64)nS;
         const unsigned sb = (unsigned)((nS + A_STILE - 1) / A_STILE);
-        if (outputs >= 4000000 && nA >= 32)
-            k_stage_a<32><<<dim3(sb, (unsigned)((nA + 31) / 32)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt,
-                                                                                    nS, U, Up, H.p);
-        else if (outputs >= 1000000)
-            k_stage_a<16><<<dim3(sb, (unsigned)((nA + 15) / 16)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt,
-                                                                                    nS, U, Up, H.p);
+        const int KT = (outputs >= 4000000 && nA >= 32) ? 32 : outputs >= 1000000 ? 16 : 4;
+        const unsigned kb = (unsigned)((nA + KT - 1) / KT);
+        int t_chunk = U;
+        const int P = split_count((i64)sb * kb, U, A_TC, a.num_sms, &t_chunk);
+        DevBuf<double> parts;
+        double* dst = H.p;
+        if (P > 1) {
+            parts.alloc((i64)P * nA * nS, s);
+            dst = parts.p;
+        }
+        const dim3 grid(sb, kb, (unsigned)P);
+        const i64 ps = nA * (i64)nS;
+        if (KT == 32)
+            k_stage_a<32><<<grid, A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst);
+        else if (KT == 16)
+            k_stage_a<16><<<grid, A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst);
         else
-            k_stage_a<4><<<dim3(sb, (unsigned)((nA + 3) / 4)), A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt,
-                                                                                 nS, U, Up, H.p);
+            k_stage_a<4><<<grid, A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst);
         GLI_CHECK_LAUNCH();
+        if (P > 1) {
+            k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
+                                                                                                      H.p);
+            GLI_CHECK_LAUNCH();
+        }
     }
     timer.mark();
     // ---- stage B
     DevBuf<double> H2(nP * (i64)Up, s);
-    if (a.mixed) {
+    if (tc_b) {
         constexpr int BN = tile_n(MIXED_SLICES);
         const int mb = (U + TC_BM - 1) / TC_BM;
         TiledSlices Hs, Wb;
@@ -727,9 +774,24 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         GLI_CHECK_LAUNCH();
         // chunk slots per A key: at most nku pairs share one A key
         const unsigned chunks = (unsigned)((nku + B_PAIRS - 1) / B_PAIRS);
-        k_stage_b<<<dim3((unsigned)nA, chunks, (unsigned)((U + B_THREADS - 1) / B_THREADS)), B_THREADS, 0, s>>>(
-            t.W.p, Hf.p, pairA.p, pairB.p, cnt, U, Up, H2.p);
+        const int nub = (U + B_THREADS - 1) / B_THREADS;
+        int v_chunk = U;
+        const int P = split_count(nA * (i64)chunks * nub, U, 32, a.num_sms, &v_chunk);
+        const i64 ps = nP * (i64)Up;
+        DevBuf<double> parts;
+        double* dst = H2.p;
+        if (P > 1) {
+            parts.alloc(P * ps, s);
+            dst = parts.p;
+        }
+        k_stage_b<<<dim3((unsigned)nA, chunks, (unsigned)(nub * P)), B_THREADS, 0, s>>>(
+            t.W.p, Hf.p, pairA.p, pairB.p, cnt, U, Up, nub, v_chunk, ps, dst);
         GLI_CHECK_LAUNCH();
+        if (P > 1) {
+            k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
+                                                                                                      H2.p);
+            GLI_CHECK_LAUNCH();
+        }
     }
     timer.mark();
     // ---- stage C: the product form computes every (pair, key) dot product --
