@@ -128,6 +128,81 @@ __global__ void k_plan_keys(i64 nk, const uint32_t* __restrict__ used, const uin
     }
 }
 
+// block-wide exclusive sum of one value per thread (blockDim.x = 1024)
+__device__ inline uint32_t block_scan_1024(uint32_t v, uint32_t* warp_sums, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warp_sums[lane];
+        uint32_t wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        warp_sums[lane] = wi - w;
+        if (lane == 31) *total = wi;
+    }
+    __syncthreads();
+    return warp_sums[warp] + incl - v;
+}
+
+// Bounded plans (at most 512 key flags, 65,536 pair slots): one block scans the
+// key flags and records the key maps and counts -- the joint scan and
+// k_plan_keys in one launch.
+__global__ void __launch_bounds__(1024) k_plan_keys_small(i64 nk, const uint32_t* __restrict__ used,
+                                                          uint64_t* __restrict__ ids, int* __restrict__ keyOf,
+                                                          int* __restrict__ aId, int* __restrict__ aKey,
+                                                          PlanCounts* __restrict__ cnt) {
+    __shared__ uint32_t ws[32], total, nku_s;
+    const int k = threadIdx.x;  // flag k of 2 nk (<= 512)
+    const uint32_t f = k < 2 * nk ? used[k] : 0u;
+    const uint32_t ex = block_scan_1024(f, ws, &total);
+    if (k < 2 * nk) ids[k] = ex;
+    if (k == nk) nku_s = ex;  // exclusive count at nk = used keys
+    __syncthreads();
+    const uint32_t nku = nk > 0 ? nku_s : 0u;
+    if (k == 0) {
+        cnt->key_total = total;
+        cnt->nku = nku;
+        cnt->nA = (int64_t)total - nku;
+    }
+    if (k < nk && f) keyOf[ex] = k;
+    if (k >= nk && k < 2 * nk && f) {
+        const int a = (int)(ex - nku);
+        aId[k - nk] = a;
+        aKey[a] = (int)(k - nk);
+    }
+}
+
+// ... and the pair flags: exclusive ids of the used slots, the pair lists in
+// slot order, and the pair count.  Thread t owns slots [t * per, (t + 1) * per).
+__global__ void __launch_bounds__(1024) k_pairs_small(i64 slots, i64 stride, const uint32_t* __restrict__ usedPair,
+                                                      const int* __restrict__ keyOf, const int* __restrict__ aId,
+                                                      uint64_t* __restrict__ pairId, int* __restrict__ pairA,
+                                                      int* __restrict__ pairB, PlanCounts* __restrict__ cnt) {
+    __shared__ uint32_t ws[32], total;
+    const i64 per = (slots + blockDim.x - 1) / blockDim.x;
+    const i64 b = (i64)threadIdx.x * per, e = b + per < slots ? b + per : slots;
+    uint32_t c = 0;
+    for (i64 q = b; q < e; ++q) c += usedPair[q];
+    uint32_t run = block_scan_1024(c, ws, &total);
+    for (i64 q = b; q < e; ++q) {
+        pairId[q] = run;
+        if (usedPair[q]) {
+            pairA[run] = aId[keyOf[q / stride]];
+            pairB[run] = keyOf[q % stride];
+            ++run;
+        }
+    }
+    if (threadIdx.x == 0) cnt->nP = total;
+}
+
 // (A, B) pairs over the compacted key ids: slot = kid(k2) * stride + kid(k1)
 __global__ void k_mark_pairs(ClassDecode d, const int64_t* __restrict__ idx, i64 m, const uint64_t* __restrict__ kid,
                              i64 stride, uint32_t* __restrict__ usedPair) {
@@ -229,7 +304,8 @@ __global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict_
 // Hf is H expanded back to the full (v, u) square (coalesced reads over u).
 // Pairs are ordered by their A key; block (A key, chunk of 16 of its pairs,
 // 128 u) keeps 16 accumulators per thread, so each Hf value feeds 16 FMAs and
-// the 16 B-key weights are double2 shared-memory broadcasts.
+// the 16 B-key weights are double2 shared-memory broadcasts (32 pairs per block
+// measured slower: 0.66 against 0.615 ms at ERIDA 129^3).
 constexpr int B_THREADS = 128;
 constexpr int B_PAIRS = 16;
 constexpr int B_VC = 64;                  // v chunk staged in shared memory
@@ -638,10 +714,16 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     k_mark_keys<<<cb, 256, 0, s>>>(a.d, a.idx, m, used.p, used.p + nk, &st->bad);
     GLI_CHECK_LAUNCH();
     DevBuf<uint64_t> ids(2 * nk, s);
-    exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
     DevBuf<int> keyOf(nk, s), aId(nk, s), aKey(nk, s);
-    k_plan_keys<<<kb, 256, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
-    GLI_CHECK_LAUNCH();
+    const bool small = 2 * nk <= 1024;
+    if (small) {
+        k_plan_keys_small<<<1, 1024, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
+        GLI_CHECK_LAUNCH();
+    } else {
+        exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
+        k_plan_keys<<<kb, 256, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
+        GLI_CHECK_LAUNCH();
+    }
     if (bounded) {
         sz.nku = nk;
         sz.nA = nk;
@@ -660,7 +742,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     k_mark_pairs<<<cb, 256, 0, s>>>(a.d, a.idx, m, ids.p, stride, usedPair.p);
     GLI_CHECK_LAUNCH();
     DevBuf<uint64_t> pairId(slots, s);
-    exclusive_scan_u32_dev(usedPair.p, pairId.p, slots, &cnt->nP, s);
+    const bool small_pairs = bounded && slots <= 65536;
+    if (!small_pairs) exclusive_scan_u32_dev(usedPair.p, pairId.p, slots, &cnt->nP, s);
     if (bounded) {
         // pairs (A, B) have kid(A) >= kid(B); every class has one pair
         sz.nP = std::min(sz.nku * (sz.nku + 1) / 2, m);
@@ -670,8 +753,11 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         sz.nP = (i64)h.cnt.nP;
     }
     DevBuf<int> pairA(sz.nP, s), pairB(sz.nP, s);
-    k_pair_lists<<<(unsigned)((slots + 255) / 256), 256, 0, s>>>(slots, stride, usedPair.p, pairId.p, keyOf.p, aId.p,
-                                                                  pairA.p, pairB.p);
+    if (small_pairs)
+        k_pairs_small<<<1, 1024, 0, s>>>(slots, stride, usedPair.p, keyOf.p, aId.p, pairId.p, pairA.p, pairB.p, cnt);
+    else
+        k_pair_lists<<<(unsigned)((slots + 255) / 256), 256, 0, s>>>(slots, stride, usedPair.p, pairId.p, keyOf.p,
+                                                                      aId.p, pairA.p, pairB.p);
     GLI_CHECK_LAUNCH();
     DevBuf<int2> cls(m, s);
     k_class_pairs<<<cb, 256, 0, s>>>(a.d, a.idx, m, ids.p, stride, pairId.p, cls.p);

@@ -172,23 +172,32 @@ __global__ void scan_tiles_apply(const uint32_t* __restrict__ in, i64 n, const u
     }
 }
 
-// small arrays: one block, each thread scans a contiguous run; total at tot[0]
+// small arrays: one block walks the array in tiles of 4096 (4 consecutive
+// items per thread, coalesced), carrying the running total; total at tot[0]
 constexpr i64 SCAN_SMALL = 1 << 16;
 
 __global__ void scan_small(const uint32_t* __restrict__ in, i64 n, uint64_t* __restrict__ out,
                            uint64_t* __restrict__ tot) {
     __shared__ uint64_t ws[32];
     __shared__ uint64_t total;
-    const i64 per = (n + blockDim.x - 1) / blockDim.x;
-    const i64 b = (i64)threadIdx.x * per, e = b + per < n ? b + per : n;
-    uint64_t sum = 0;
-    for (i64 k = b; k < e; ++k) sum += in[k];
-    uint64_t run = block_exclusive_sum(sum, ws, &total);
-    for (i64 k = b; k < e; ++k) {
-        out[k] = run;
-        run += in[k];
+    uint64_t carry = 0;
+    for (i64 base = 0; base < n; base += SCAN_TILE) {
+        const i64 i0 = base + (i64)threadIdx.x * SCAN_ITEMS;
+        uint32_t v[SCAN_ITEMS];
+        uint64_t sum = 0;
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            v[k] = i0 + k < n ? in[i0 + k] : 0u;
+            sum += v[k];
+        }
+        uint64_t run = carry + block_exclusive_sum(sum, ws, &total);
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            if (i0 + k < n) out[i0 + k] = run;
+            run += v[k];
+        }
+        carry += total;
+        __syncthreads();
     }
-    if (threadIdx.x == 0) tot[0] = total;
+    if (threadIdx.x == 0) tot[0] = carry;
 }
 
 i64 exclusive_scan_u32(const uint32_t* d_in, uint64_t* d_out, i64 n, cudaStream_t s) {
