@@ -577,14 +577,18 @@ def lattice_nS(U):
 
 def roofline(form, dom, st, nA, nP, U, m, fp64_peak):
     """Roofline entry of the dominant stage (from the library's stage events).
-    FP64 form: the stage's FP64 FLOPs against the measured FP64 FMA peak.  Mixed
-    form: the stage's sliced tensor-core work is bound by the bytes it must move
-    (FP64 sources, int8 slices written and read, FP64 results) against the
-    measured HBM bandwidth."""
+    FP64 kernels: the stage's FP64 FLOPs against the measured FP64 FMA peak.
+    Tensor-core stages of the mixed form: the sliced work is bound by the bytes
+    it must move (FP64 sources, int8 slices written and read, FP64 results)
+    against the measured HBM bandwidth.  The mixed form runs a stage on the
+    tensor cores only when it is large (stage A: nA nS >= 1e6 outputs; stage
+    B: nA U^2 >= 4e6), the same rule as the library."""
     ms = st[dom]
     nS = lattice_nS(U)
     kp = (U + 63) // 64 * 64
-    if form == "fp64":
+    on_tensor_cores = form == "mixed" and ((dom == "A" and nA * nS >= 1000000) or
+                                           (dom == "B" and nA * U * U >= 4000000))
+    if not on_tensor_cores and dom != "C":
         flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U, "C": 2.0 * m * U}[dom]
         achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
         return {"bound": "fp64", "stage": dom,
@@ -601,7 +605,7 @@ def roofline(form, dom, st, nA, nP, U, m, fp64_peak):
     achieved = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
     peak = measured_peaks()["hbm_gbs"]
     return {"bound": "hbm", "stage": dom,
-            "kernel": {"A": "k_tc_gemm<5,5> (stage A)", "B": "k_slice_tiled + k_tc_gemm<5,5> (stage B)",
+            "kernel": {"A": "k_tc_gemm<5,5> (stage A)", "B": "k_slice_group + k_tc_gemm<5,5> (stage B)",
                        "C": "k_stage_c"}[dom],
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved and peak else None,

@@ -130,14 +130,8 @@ void sparse_compute(int kind, const struct gausslet_data* gdata, const struct ca
         try {
             if (num) {
                 gli::Context& ctx = gli::context();
-                cudaStream_t s = ctx.stream;
-                DevBuf<int64_t> d_idx;
-                to_device(d_idx, (const int64_t*)indices, num, s);
-                DevBuf<double> d_val(num, s);
-                gli::sparse_values_device(kind, gdata->coefficients, gdata->indices.num, g, d_idx.p, num, tol, form,
-                                          d_val.p, s, nullptr);
-                to_host(h_val, d_val.p, num, s);
-                GLI_CUDA(cudaStreamSynchronize(s));
+                gli::sparse_values_host(kind, gdata->coefficients, gdata->indices.num, g, (const int64_t*)indices, num,
+                                        tol, form, h_val, ctx.stream);
             }
         } catch (...) {
             aligned_free(h_idx);
@@ -694,15 +688,10 @@ int gli_b200_sparse_values(int kind, const struct gausslet_data* gdata, const st
         check_gdata(gdata);
         const gli::GridDesc g = gli::grid_desc(grid);
         if (num <= 0) return;
+        if (!indices || !values) gli::fail(GLI_ERR_ARGUMENT, "indices and values must not be NULL");
         gli::Context& ctx = gli::context();
-        cudaStream_t s = ctx.stream;
-        DevBuf<int64_t> di;
-        to_device(di, (const int64_t*)indices, num, s);
-        DevBuf<double> dv(num, s);
-        gli::sparse_values_device(kind, gdata->coefficients, gdata->indices.num, g, di.p, num, tol, form, dv.p, s,
-                                  nullptr);
-        to_host(values, dv.p, num, s);
-        GLI_CUDA(cudaStreamSynchronize(s));
+        gli::sparse_values_host(kind, gdata->coefficients, gdata->indices.num, g, (const int64_t*)indices, num, tol,
+                                form, values, ctx.stream);
     });
     return gli::last_error();
 }

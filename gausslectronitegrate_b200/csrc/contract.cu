@@ -21,6 +21,7 @@
 #include <math.h>
 
 #include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <list>
@@ -1001,16 +1002,36 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     return t_graphs.front().get();
 }
 
-void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
-                          i64 m, double tol, int form, double* d_out, cudaStream_t s, ContractStats* stats) {
+// pinned host memory that grows on demand (per thread)
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void* get(size_t need) {
+        if (need > bytes) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            bytes = 0;
+            GLI_CUDA(cudaHostAlloc(&p, need, cudaHostAllocDefault));
+            bytes = need;
+        }
+        return p;
+    }
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// Queues one evaluation on stream s and an asynchronous copy of its status
+// block into h_status (pinned); the caller synchronises and checks it.
+static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
+                                  const int64_t* d_indices, i64 m, double tol, int form, double* d_out, cudaStream_t s,
+                                  EvalStatus* h_status, std::shared_ptr<const LatticeTables>& tp, StageTimer& timer) {
     if (form != FORM_FP64 && form != FORM_MIXED)
         fail(GLI_ERR_ARGUMENT, "form %d is not a sparse evaluation form (0 = FP64, 1 = mixed)", form);
     if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
-    if (m == 0) return;
     const Context& ctx = context();
-    StageTimer timer(t_timing, s);
     timer.mark();
-    const std::shared_ptr<const LatticeTables> tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
+    tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
     const LatticeTables& t = *tp;
     EvalArgs a;
     a.mixed = form == FORM_MIXED;
@@ -1029,21 +1050,24 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     a.m = m;
     a.out = d_out;
     a.num_sms = ctx.num_sms;
-
     const bool bounded = t.nkeys <= BOUNDED_KEYS;
-    EvalStatus h;
     if (bounded && !t_timing && g_graphs_enabled) {
         GraphEntry* e = find_graph(a, ctx.device);
         if (!e) e = capture_graph(a, tp, ctx.device, s);
         GLI_CUDA(cudaGraphLaunch(e->exec, s));
         add_launches(e->launches);
-        read_status(e->status.p, h, s);
+        GLI_CUDA(cudaMemcpyAsync(h_status, e->status.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
     } else {
         DevBuf<EvalStatus> st(1, s);
         EvalSizes sz;
         enqueue_eval(a, bounded, st.p, timer, sz, s);
-        read_status(st.p, h, s);
+        GLI_CUDA(cudaMemcpyAsync(h_status, st.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
     }
+}
+
+// after the stream synchronised: errors of the evaluation, and the statistics
+static void check_status(int kind, const EvalStatus& h, const LatticeTables& t, StageTimer& timer,
+                         ContractStats* stats) {
     if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
     if (h.tc_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired (code %d)", h.tc_err);
     if (h.cnt.nku > 16384)
@@ -1060,6 +1084,62 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     }
     t_last = st;
     if (stats) *stats = st;
+}
+
+static thread_local PinnedBuf t_pin_status, t_pin_idx, t_pin_val;
+
+void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
+                          i64 m, double tol, int form, double* d_out, cudaStream_t s, ContractStats* stats) {
+    if (m == 0) return;
+    EvalStatus* h = (EvalStatus*)t_pin_status.get(sizeof(EvalStatus));
+    std::shared_ptr<const LatticeTables> tp;
+    StageTimer timer(t_timing, s);
+    sparse_values_enqueue(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, h, tp, timer);
+    GLI_CUDA(cudaStreamSynchronize(s));
+    check_status(kind, *h, *tp, timer, stats);
+}
+
+// Device copies of a host class list and its values, kept per thread and
+// device between calls (grown on demand), so that repeated calls reuse the
+// same device pointers and therefore the same captured evaluation.
+struct HostCallBuffers {
+    int device = -1;
+    std::unique_ptr<DevMem<int64_t>> idx;
+    std::unique_ptr<DevMem<double>> val;
+    i64 cap = 0;
+    void ensure(int dev, i64 m) {
+        if (dev != device || m > cap) {
+            idx.reset();
+            val.reset();
+            idx = std::make_unique<DevMem<int64_t>>();
+            val = std::make_unique<DevMem<double>>();
+            idx->alloc((size_t)m);
+            val->alloc((size_t)m);
+            cap = m;
+            device = dev;
+        }
+    }
+};
+static thread_local HostCallBuffers t_host_call;
+
+void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices, i64 m,
+                        double tol, int form, double* h_out, cudaStream_t s) {
+    if (m == 0) return;
+    const Context& ctx = context();
+    EvalStatus* hs = (EvalStatus*)t_pin_status.get(sizeof(EvalStatus));
+    int64_t* pin_idx = (int64_t*)t_pin_idx.get((size_t)m * sizeof(int64_t));
+    double* pin_val = (double*)t_pin_val.get((size_t)m * sizeof(double));
+    t_host_call.ensure(ctx.device, m);
+    memcpy(pin_idx, h_indices, (size_t)m * sizeof(int64_t));
+    GLI_CUDA(cudaMemcpyAsync(t_host_call.idx->p, pin_idx, (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    std::shared_ptr<const LatticeTables> tp;
+    StageTimer timer(t_timing, s);
+    sparse_values_enqueue(kind, h_coeffs, nb, g, t_host_call.idx->p, m, tol, form, t_host_call.val->p, s, hs, tp,
+                          timer);
+    GLI_CUDA(cudaMemcpyAsync(pin_val, t_host_call.val->p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GLI_CUDA(cudaStreamSynchronize(s));
+    check_status(kind, *hs, *tp, timer, nullptr);
+    memcpy(h_out, pin_val, (size_t)m * sizeof(double));
 }
 
 }  // namespace gli

@@ -144,6 +144,9 @@ struct ContractStats {
 void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
                           const int64_t* d_indices, i64 m, double tol, int form,
                           double* d_out, cudaStream_t s, ContractStats* stats);
+// the same from host buffers (pinned staging, one synchronisation)
+void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices, i64 m,
+                        double tol, int form, double* h_out, cudaStream_t s);
 
 // enumeration (enumerate.cu); returns a device array (caller frees with cudaFreeAsync)
 i64 enumerate_device(int kind, const GridDesc& g, int64_t** d_out, cudaStream_t s);
