@@ -276,10 +276,16 @@ __global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict_
         }
         __syncthreads();
         const int tmax = min(A_TC, t_end - t0);
+        // the table gathers of t + 1 are issued before the FMAs of t
+        double g0n = __ldg(&T[s0 + t0 * t0]);
+        double g1n = __ldg(&T[s1 + t0 * t0]);
         for (int tt = 0; tt < tmax; ++tt) {
-            const int t2 = (t0 + tt) * (t0 + tt);
-            const double g0 = __ldg(&T[s0 + t2]);
-            const double g1 = __ldg(&T[s1 + t2]);
+            const double g0 = g0n, g1 = g1n;
+            if (tt + 1 < tmax) {
+                const int t2n = (t0 + tt + 1) * (t0 + tt + 1);
+                g0n = __ldg(&T[s0 + t2n]);
+                g1n = __ldg(&T[s1 + t2n]);
+            }
             const double2* w2 = reinterpret_cast<const double2*>(&ws[tt][0]);
 #pragma unroll
             for (int k = 0; k < KT / 2; ++k) {

@@ -174,7 +174,7 @@ __global__ void scan_tiles_apply(const uint32_t* __restrict__ in, i64 n, const u
 
 // small arrays: one block walks the array in tiles of 4096 (4 consecutive
 // items per thread, coalesced), carrying the running total; total at tot[0]
-constexpr i64 SCAN_SMALL = 1 << 16;
+constexpr i64 SCAN_SMALL = 1 << 13;
 
 __global__ void scan_small(const uint32_t* __restrict__ in, i64 n, uint64_t* __restrict__ out,
                            uint64_t* __restrict__ tot) {
