@@ -27,6 +27,7 @@
 #include <list>
 #include <memory>
 
+#include "dmma.cuh"
 #include "tables.cuh"
 
 namespace gli {
@@ -40,49 +41,98 @@ struct ClassDecode {
     i64 istart[3];
     i64 num[3];
     i64 nkeys;
+    // device decode: 32-bit point arithmetic (N < 2^31; ERI N^2 < 2^32), the
+    // 64-bit quotient by a double estimate when the index is below 2^53, and
+    // for ERI a table of point coordinates
+    uint32_t n32, n1, n2;
+    int is[3];
+    uint64_t N2;
+    double invN, invN2;
+    int fast;
+    const short4* pt;
+    void finish() {
+        n32 = (uint32_t)N;
+        n1 = (uint32_t)num[1];
+        n2 = (uint32_t)num[2];
+        for (int a = 0; a < 3; ++a) is[a] = (int)istart[a];
+        N2 = (uint64_t)N * (uint64_t)N;
+        invN = 1.0 / (double)N;
+        invN2 = 1.0 / (double)N2;
+        // largest class index + 1: N^2 (ERIDA), N^4 (ERI)
+        const double top = kind == 0 ? (double)N2 : (double)N2 * (double)N2;
+        fast = top <= 9007199254740992.0 ? 1 : 0;  // 2^53
+    }
 };
 
-__device__ inline void decode_pt(const ClassDecode& d, i64 lin, i64 p[3]) {
-    const i64 z = lin % d.num[2];
-    lin /= d.num[2];
-    const i64 y = lin % d.num[1];
-    const i64 x = lin / d.num[1];
-    p[0] = d.istart[0] + x;
-    p[1] = d.istart[1] + y;
-    p[2] = d.istart[2] + z;
+// floor(u / d) for u < 2^53: the double estimate u * (1/d) is within one of
+// the quotient, and one correction step lands on it
+__device__ inline uint64_t div_est(uint64_t u, uint64_t d, double inv) {
+    uint64_t q = (uint64_t)((double)u * inv);
+    const int64_t r = (int64_t)(u - q * d);
+    if (r < 0)
+        --q;
+    else if (r >= (int64_t)d)
+        ++q;
+    return q;
 }
 
-// returns false for an index outside the tensor
-__device__ inline bool class_keys(const ClassDecode& d, i64 idx, i64 k[3]) {
+// grid point lin (x-major) -> coordinates; 32-bit arithmetic
+__device__ inline void decode_pt(const ClassDecode& d, uint32_t lin, int p[3]) {
+    const uint32_t r = lin / d.n2;
+    p[2] = d.is[2] + (int)(lin - r * d.n2);
+    const uint32_t x = r / d.n1;
+    p[1] = d.is[1] + (int)(r - x * d.n1);
+    p[0] = d.is[0] + (int)x;
+}
+
+// coordinates of every grid point (ERI decoding)
+__global__ void k_point_table(ClassDecode d, short4* __restrict__ pt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n32) return;
+    int p[3];
+    decode_pt(d, i, p);
+    pt[i] = make_short4((short)p[0], (short)p[1], (short)p[2], 0);
+}
+
+// sorted axis keys of class idx; false for an index outside the tensor
+__device__ inline bool class_keys(const ClassDecode& d, i64 idx, int k[3]) {
+    if (idx < 0) return false;
+    const uint64_t u = (uint64_t)idx;
     if (d.kind == 0) {
-        if (idx < 0 || idx >= d.N * d.N) return false;
-        i64 pi[3], pj[3];
-        decode_pt(d, idx / d.N, pi);
-        decode_pt(d, idx % d.N, pj);
-        for (int a = 0; a < 3; ++a) {
-            const i64 dd = pi[a] - pj[a];
-            k[a] = dd < 0 ? -dd : dd;
-        }
+        if (u >= d.N2) return false;
+        const uint64_t pi = d.fast ? div_est(u, d.n32, d.invN) : u / d.n32;
+        int a[3], b[3];
+        decode_pt(d, (uint32_t)pi, a);
+        decode_pt(d, (uint32_t)(u - pi * d.n32), b);
+        for (int x = 0; x < 3; ++x) k[x] = abs(a[x] - b[x]);
     } else {
-        const i64 N2 = d.N * d.N;
-        if (idx < 0 || idx / N2 >= N2) return false;
-        i64 r = idx;
-        const i64 il = r % d.N; r /= d.N;
-        const i64 ik = r % d.N; r /= d.N;
-        const i64 ij = r % d.N; r /= d.N;
-        i64 p0[3], p1[3], p2[3], p3[3];
-        decode_pt(d, r, p0);
-        decode_pt(d, ij, p1);
-        decode_pt(d, ik, p2);
-        decode_pt(d, il, p3);
-        for (int a = 0; a < 3; ++a)
-            k[a] = eri_axis_key(p0[a] - p1[a], p2[a] - p3[a], (p0[a] + p1[a]) - (p2[a] + p3[a]), d.L);
+        const uint64_t hi = d.fast ? div_est(u, d.N2, d.invN2) : u / d.N2;  // point pair (p0, p1)
+        if (hi >= d.N2) return false;
+        const uint64_t lo = u - hi * d.N2;                                   // point pair (p2, p3)
+        const uint64_t i0 = div_est(hi, d.n32, d.invN), i2 = div_est(lo, d.n32, d.invN);
+        const short4 p0 = d.pt[i0], p1 = d.pt[hi - i0 * d.n32], p2 = d.pt[i2], p3 = d.pt[lo - i2 * d.n32];
+        const int L = (int)d.L;
+        k[0] = eri_axis_key32(p0.x - p1.x, p2.x - p3.x, (p0.x + p1.x) - (p2.x + p3.x), L);
+        k[1] = eri_axis_key32(p0.y - p1.y, p2.y - p3.y, (p0.y + p1.y) - (p2.y + p3.y), L);
+        k[2] = eri_axis_key32(p0.z - p1.z, p2.z - p3.z, (p0.z + p1.z) - (p2.z + p3.z), L);
     }
     // sort ascending
-    if (k[0] > k[1]) { i64 t = k[0]; k[0] = k[1]; k[1] = t; }
-    if (k[1] > k[2]) { i64 t = k[1]; k[1] = k[2]; k[2] = t; }
-    if (k[0] > k[1]) { i64 t = k[0]; k[0] = k[1]; k[1] = t; }
+    if (k[0] > k[1]) { const int t = k[0]; k[0] = k[1]; k[1] = t; }
+    if (k[1] > k[2]) { const int t = k[1]; k[1] = k[2]; k[2] = t; }
+    if (k[0] > k[1]) { const int t = k[0]; k[0] = k[1]; k[1] = t; }
     return true;
+}
+
+// a class's sorted key triple, packed 21 bits per key (keys < 2^21, checked
+// on the host); all ones for an index outside the tensor
+constexpr uint64_t BAD_KEYS = ~(uint64_t)0;
+__device__ inline uint64_t pack_keys(const int k[3]) {
+    return (uint64_t)k[0] | ((uint64_t)k[1] << 21) | ((uint64_t)k[2] << 42);
+}
+__device__ inline void unpack_keys(uint64_t p, int k[3]) {
+    k[0] = (int)(p & 0x1fffff);
+    k[1] = (int)((p >> 21) & 0x1fffff);
+    k[2] = (int)(p >> 42);
 }
 
 // counts of one evaluation, kept in device memory so that kernels can size their
@@ -93,20 +143,77 @@ struct PlanCounts {
     int64_t nku, nA;     // used keys, used A keys
 };
 
-// mark every key the class list uses (any role) and the A keys (k2)
-__global__ void k_mark_keys(ClassDecode d, const int64_t* __restrict__ idx, i64 m, uint32_t* __restrict__ usedKey,
-                            uint32_t* __restrict__ usedA, int* __restrict__ bad) {
-    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m) return;
-    i64 k[3];
-    if (!class_keys(d, idx[n], k)) {
-        atomicOr(bad, 1);
-        return;
+// Decodes every class once (its packed keys are kept for the later passes)
+// and marks the keys it uses (any role: usedKey; as A = k2: usedA) and its
+// (A, B) = (k2, k1) key pair (bit k2 * nk + k1 of pairBits).  Millions of
+// classes share a few hundred keys and a few thousand pairs, so writes of the
+// same flag from every block would queue on a few cache lines: with `local`
+// set each block collects its key flags and pair bits in shared memory and
+// merges them once.  used = [usedKey | usedA], 2 nk flags.
+__global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
+                                              uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
+                                              uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
+    extern __shared__ uint32_t sflag[];
+    const int nk = (int)d.nkeys;
+    const int words = (nk * nk + 31) >> 5;
+    uint32_t* sbits = sflag + 2 * nk;
+    if (local) {
+        for (int i = threadIdx.x; i < 2 * nk + words; i += blockDim.x) sflag[i] = 0;
+        __syncthreads();
     }
-    usedKey[k[0]] = 1;
-    usedKey[k[1]] = 1;
-    usedKey[k[2]] = 1;
-    usedA[k[1]] = 1;
+    uint32_t* flags = local ? sflag : used;
+    uint32_t* bits = local ? sbits : pairBits;
+    // four classes per thread and step, their index loads issued together
+    constexpr int V = 4;
+    const i64 step = (i64)gridDim.x * blockDim.x;
+    for (i64 n0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; n0 < m; n0 += V * step) {
+        i64 cls[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const i64 n = n0 + v * step;
+            cls[v] = n < m ? __ldg(&idx[n]) : -1;
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const i64 n = n0 + v * step;
+            if (n >= m) break;
+            int k[3];
+            if (!class_keys(d, cls[v], k)) {
+                keys[n] = BAD_KEYS;
+                atomicOr(bad, 1);
+                continue;
+            }
+            keys[n] = pack_keys(k);
+            flags[k[0]] = 1;
+            flags[k[1]] = 1;
+            flags[k[2]] = 1;
+            flags[nk + k[1]] = 1;
+            // neighbouring classes share their pair: a read first, so that the
+            // serialising atomic runs only for a new bit
+            const int slot = k[1] * nk + k[0];
+            const uint32_t bit = 1u << (slot & 31);
+            if (!(bits[slot >> 5] & bit)) atomicOr(&bits[slot >> 5], bit);
+        }
+    }
+    if (local) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 2 * nk; i += blockDim.x)
+            if (sflag[i]) used[i] = 1;
+        for (int w = threadIdx.x; w < words; w += blockDim.x)
+            if (sbits[w]) atomicOr(&pairBits[w], sbits[w]);
+    }
+}
+
+// id of the pair in bit `slot` of the pair bitmap: the set bits before it
+__device__ inline i64 pair_id(const uint32_t* __restrict__ bits, const uint64_t* __restrict__ pre, i64 slot) {
+    const i64 w = slot >> 5;
+    return (i64)pre[w] + __popc(bits[w] & ((1u << (slot & 31)) - 1u));
+}
+
+// dynamic shared memory of k_mark's local variant, 0 when it does not fit
+static size_t mark_local_bytes(i64 nk) {
+    const i64 bytes = (2 * nk + (nk * nk + 31) / 32) * (i64)sizeof(uint32_t);  // key flags + pair bits
+    return bytes <= 48 * 1024 ? (size_t)bytes : 0;
 }
 
 // After the joint scan of (usedKey | usedA): compact key id kid[k] = ids[k],
@@ -181,215 +288,225 @@ __global__ void __launch_bounds__(1024) k_plan_keys_small(i64 nk, const uint32_t
     }
 }
 
-// ... and the pair flags: exclusive ids of the used slots, the pair lists in
-// slot order, and the pair count.  Thread t owns slots [t * per, (t + 1) * per).
-__global__ void __launch_bounds__(1024) k_pairs_small(i64 slots, i64 stride, const uint32_t* __restrict__ usedPair,
-                                                      const int* __restrict__ keyOf, const int* __restrict__ aId,
-                                                      uint64_t* __restrict__ pairId, int* __restrict__ pairA,
-                                                      int* __restrict__ pairB, PlanCounts* __restrict__ cnt) {
+// ... and the pair bitmap (bit k2 * nk + k1): the exclusive count of set bits
+// before every word, the pair lists in bit order (sorted by A key, then B
+// key), and the pair count.  Tiles of 1024 words, scanned with a running carry.
+__global__ void __launch_bounds__(1024) k_pairs_small(i64 words, int nk, const uint32_t* __restrict__ bits,
+                                                      const int* __restrict__ aId, uint64_t* __restrict__ pre,
+                                                      int* __restrict__ pairA, int* __restrict__ pairB,
+                                                      PlanCounts* __restrict__ cnt) {
     __shared__ uint32_t ws[32], total;
-    const i64 per = (slots + blockDim.x - 1) / blockDim.x;
-    const i64 b = (i64)threadIdx.x * per, e = b + per < slots ? b + per : slots;
-    uint32_t c = 0;
-    for (i64 q = b; q < e; ++q) c += usedPair[q];
-    uint32_t run = block_scan_1024(c, ws, &total);
-    for (i64 q = b; q < e; ++q) {
-        pairId[q] = run;
-        if (usedPair[q]) {
-            pairA[run] = aId[keyOf[q / stride]];
-            pairB[run] = keyOf[q % stride];
-            ++run;
+    uint32_t carry = 0;
+    for (i64 base = 0; base < words; base += 1024) {
+        const i64 w = base + threadIdx.x;
+        uint32_t b = w < words ? bits[w] : 0u;
+        uint32_t id = carry + block_scan_1024(__popc(b), ws, &total);
+        if (w < words) pre[w] = id;
+        while (b) {
+            const int bit = __ffs(b) - 1;
+            b &= b - 1;
+            const i64 slot = w * 32 + bit;
+            pairA[id] = aId[slot / nk];
+            pairB[id] = (int)(slot % nk);
+            ++id;
         }
+        carry += total;
+        __syncthreads();  // total and ws are rewritten by the next tile's scan
     }
-    if (threadIdx.x == 0) cnt->nP = total;
+    if (threadIdx.x == 0) cnt->nP = carry;
 }
 
-// (A, B) pairs over the compacted key ids: slot = kid(k2) * stride + kid(k1)
-__global__ void k_mark_pairs(ClassDecode d, const int64_t* __restrict__ idx, i64 m, const uint64_t* __restrict__ kid,
-                             i64 stride, uint32_t* __restrict__ usedPair) {
-    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m) return;
-    i64 k[3];
-    if (!class_keys(d, idx[n], k)) return;
-    usedPair[(i64)kid[k[1]] * stride + (i64)kid[k[0]]] = 1;
+// set bits per word of the pair bitmap (the exclusive scan of which gives pre)
+__global__ void k_word_counts(i64 words, const uint32_t* __restrict__ bits, uint32_t* __restrict__ counts) {
+    const i64 w = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < words) counts[w] = __popc(bits[w]);
 }
 
-__global__ void k_pair_lists(i64 slots, i64 stride, const uint32_t* __restrict__ usedPair,
-                             const uint64_t* __restrict__ pairId, const int* __restrict__ keyOf,
+__global__ void k_pair_lists(i64 words, int nk, const uint32_t* __restrict__ bits, const uint64_t* __restrict__ pre,
                              const int* __restrict__ aId, int* __restrict__ pairA, int* __restrict__ pairB) {
-    const i64 slot = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= slots || !usedPair[slot]) return;
-    const i64 ka = keyOf[slot / stride], kb = keyOf[slot % stride];
-    pairA[pairId[slot]] = aId[ka];
-    pairB[pairId[slot]] = (int)kb;
-}
-
-__global__ void k_class_pairs(ClassDecode d, const int64_t* __restrict__ idx, i64 m, const uint64_t* __restrict__ kid,
-                              i64 stride, const uint64_t* __restrict__ pairId, int2* __restrict__ cls) {
-    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m) return;
-    i64 k[3];
-    if (!class_keys(d, idx[n], k)) {
-        cls[n] = make_int2(-1, 0);
-        return;
+    const i64 w = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    uint32_t b = bits[w];
+    i64 id = (i64)pre[w];
+    while (b) {
+        const int bit = __ffs(b) - 1;
+        b &= b - 1;
+        const i64 slot = w * 32 + bit;
+        pairA[id] = aId[slot / nk];
+        pairB[id] = (int)(slot % nk);
+        ++id;
     }
-    cls[n] = make_int2((int)pairId[(i64)kid[k[1]] * stride + (i64)kid[k[0]]], (int)kid[k[2]]);
 }
 
 // ---------------------------------------------------------------------------
 // stage A: H[a][j] = sum_t W[aKey[a]][t] T[S[j] + t^2]
 // H depends on (u, v) only through s = u^2 + v^2, so it is evaluated once per
 // distinct s (S, ascending; 10,823 values instead of 31,329 (u, v) at U = 177).
-// Block: 64 threads x 2 s-values, KT keys held in registers per thread; the
-// keys' weights for a chunk of t sit in shared memory, read as double2
-// broadcasts.  Per t a thread issues 2 table gathers and KT/2 shared loads for
-// 2*KT FMAs.
-constexpr int A_THREADS = 128;
-constexpr int A_SPT = 2;                  // s-values per thread
-constexpr int A_STILE = A_THREADS * A_SPT;
-constexpr int A_TC = 32;                  // t chunk
-
-template <int KT>
-__global__ void __launch_bounds__(A_THREADS) k_stage_a(const double* __restrict__ W, const double* __restrict__ T,
-                                                        const int* __restrict__ S, const int* __restrict__ aKey,
-                                                        const PlanCounts* __restrict__ cnt, int nS, int U, int Up,
-                                                        int t_chunk, i64 part_stride, double* __restrict__ H) {
-    __shared__ __align__(16) double ws[A_TC][KT];
-    // blockIdx.z: chunk of t (partial sums of small problems, summed afterwards)
-    const int t_begin = blockIdx.z * t_chunk, t_end = min(U, t_begin + t_chunk);
-    H += (i64)blockIdx.z * part_stride;
-    const int j0 = blockIdx.x * A_STILE + threadIdx.x;
-    const int j1 = j0 + A_THREADS;
-    const int a0 = blockIdx.y * KT;
-    const int nA = (int)cnt->nA;
-    if (a0 >= nA) return;  // grids are sized by a bound on nA
-    const int s0 = j0 < nS ? S[j0] : 0;
-    const int s1 = j1 < nS ? S[j1] : 0;
-    double acc0[KT], acc1[KT];
+// As a GEMM: C[j][a] = sum_t G[j][t] W[aKey[a]][t] with G[j][t] = T[S[j] + t^2]
+// gathered tile by tile into shared memory (consecutive j read neighbouring
+// table entries, so a warp's 32 gathers touch a few cache lines), and the
+// FP64 tensor-core tiles of dmma.cuh.  blockIdx.z selects a chunk of t: small
+// problems sum partial products afterwards (k_sum_parts).
+struct StageAOp {
+    static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
+    const double* W;
+    const double* T;
+    const int* S;
+    const int* aKey;
+    const PlanCounts* cnt;
+    int nS, U, Up, t_chunk;
+    i64 part_stride;
+    double* H;
+    struct Block {
+        int mvalid, nvalid, nk;
+        int m0, n0, t0, t1;
+        double* H;
+    };
+    struct AState {
+        const double* base;  // T + S[j] of this thread's row j
+        bool ok;
+    };
+    struct BState {
+        i64 off[DM_ELEMS];  // aKey * Up of this thread's rows, -1 past nA
+    };
+    __device__ bool begin(Block& b) const {
+        const int nA = (int)cnt->nA;
+        b.n0 = blockIdx.y * DM_BN;
+        if (b.n0 >= nA) return false;  // grids are sized by a bound on nA
+        b.m0 = blockIdx.x * DM_BM;
+        b.mvalid = min(DM_BM, nS - b.m0);
+        b.nvalid = min(DM_BN, nA - b.n0);
+        b.t0 = blockIdx.z * t_chunk;
+        b.t1 = min(U, b.t0 + t_chunk);
+        b.nk = (b.t1 - b.t0 + DM_BK - 1) / DM_BK;
+        b.H = H + (i64)blockIdx.z * part_stride;
+        return b.nk > 0;
+    }
+    __device__ void a_init(const Block& b, AState& st) const {
+        const int r = dm_kmajor_row(threadIdx.x);
+        st.ok = r < b.mvalid;
+        st.base = T + (st.ok ? S[b.m0 + r] : 0);
+    }
+    __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
+        const int r = dm_kmajor_row(threadIdx.x);
 #pragma unroll
-    for (int k = 0; k < KT; ++k) acc0[k] = acc1[k] = 0;
-    for (int t0 = t_begin; t0 < t_end; t0 += A_TC) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < A_TC * KT; e += A_THREADS) {
-            const int k = e / A_TC, tt = e % A_TC, t = t0 + tt;
-            ws[tt][k] = (a0 + k < nA && t < t_end) ? W[(i64)aKey[a0 + k] * Up + t] : 0.0;
-        }
-        __syncthreads();
-        const int tmax = min(A_TC, t_end - t0);
-        // the table gathers of t + 1 are issued before the FMAs of t
-        double g0n = __ldg(&T[s0 + t0 * t0]);
-        double g1n = __ldg(&T[s1 + t0 * t0]);
-        for (int tt = 0; tt < tmax; ++tt) {
-            const double g0 = g0n, g1 = g1n;
-            if (tt + 1 < tmax) {
-                const int t2n = (t0 + tt + 1) * (t0 + tt + 1);
-                g0n = __ldg(&T[s0 + t2n]);
-                g1n = __ldg(&T[s1 + t2n]);
-            }
-            const double2* w2 = reinterpret_cast<const double2*>(&ws[tt][0]);
-#pragma unroll
-            for (int k = 0; k < KT / 2; ++k) {
-                const double2 w = w2[k];
-                acc0[2 * k] = fma(w.x, g0, acc0[2 * k]);
-                acc0[2 * k + 1] = fma(w.y, g0, acc0[2 * k + 1]);
-                acc1[2 * k] = fma(w.x, g1, acc1[2 * k]);
-                acc1[2 * k + 1] = fma(w.y, g1, acc1[2 * k + 1]);
-            }
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int k = dm_kmajor_k(threadIdx.x, q), t = b.t0 + kc * DM_BK + k;
+            const bool v = st.ok && t < b.t1;
+            dm_cp8(tile + dm_kmajor_at(r, k), v ? st.base + t * t : T, v);
         }
     }
+    __device__ void b_init(const Block& b, BState& st) const {
 #pragma unroll
-    for (int k = 0; k < KT; ++k) {
-        if (a0 + k >= nA) break;
-        double* h = H + (i64)(a0 + k) * nS;
-        if (j0 < nS) h[j0] = acc0[k];
-        if (j1 < nS) h[j1] = acc1[k];
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int r = dm_rowmajor_row(threadIdx.x, q);
+            st.off[q] = r < b.nvalid ? (i64)aKey[b.n0 + r] * Up : -1;
+        }
     }
-}
+    __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
+        const int k = dm_rowmajor_k(threadIdx.x), t = b.t0 + kc * DM_BK + k;
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const bool v = st.off[q] >= 0 && t < b.t1;
+            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), v ? W + st.off[q] + t : W, v);
+        }
+    }
+    __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
+        if (m >= b.mvalid) return;
+        double* h = b.H + (i64)(b.n0 + n) * nS + b.m0 + m;
+        if (n < b.nvalid) h[0] = v0;
+        if (n + 1 < b.nvalid) h[nS] = v1;
+    }
+};
 
 // ---------------------------------------------------------------------------
-// stage B: H2[p][u] = sum_v W[pairB[p]][v] Hf[pairA[p]][v][u]
-// Hf is H expanded back to the full (v, u) square (coalesced reads over u).
-// Pairs are ordered by their A key; block (A key, chunk of 16 of its pairs,
-// 128 u) keeps 16 accumulators per thread, so each Hf value feeds 16 FMAs and
-// the 16 B-key weights are double2 shared-memory broadcasts (32 pairs per block
-// measured slower: 0.66 against 0.615 ms at ERIDA 129^3).
-constexpr int B_THREADS = 128;
-constexpr int B_PAIRS = 16;
-constexpr int B_VC = 64;                  // v chunk staged in shared memory
-
-__global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__ sidx,
-                           const PlanCounts* __restrict__ cnt, int nS, int U, double* __restrict__ Hf) {
-    const i64 plane = (i64)U * U;
-    const i64 total = cnt->nA * plane;
-    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
-        const i64 a = e / plane, vu = e % plane;
-        Hf[e] = H[a * nS + sidx[vu]];
+// stage B: H2[p][u] = sum_v W[pairB[p]][v] Hf[a(p)][v][u],  Hf[a][v][u] = H[a][sidx[v U + u]]
+// Pairs are ordered by their A key and cut into tiles of 64 pairs of one A key
+// (k_pair_tiles); block (pair tile, 64 u, chunk of v) is one GEMM tile with the
+// pair weights as A (rows read along v) and the expanded H of the tile's A key
+// as B, gathered through sidx straight from H (no expanded copy in memory).
+// The sidx values of the next chunk are loaded one chunk ahead, so the
+// dependent gathers do not wait on them.
+struct StageBOp {
+    static constexpr bool A_KMAJOR = false, B_KMAJOR = true;
+    const double* W;
+    const double* H;
+    const int* sidx;
+    const int* pairB;
+    const int* tile_batch;
+    const int* tile_col0;
+    const int* tile_ncols;
+    int nS, U, Up, v_chunk;
+    i64 part_stride;
+    double* H2;
+    struct Block {
+        int mvalid, nvalid, nk;
+        int p0, u0, v0, v1;
+        const double* h;  // H row of the tile's A key
+        double* H2;
+    };
+    struct AState {
+        i64 off[DM_ELEMS];  // pairB * Up of this thread's pair rows, -1 past the tile
+    };
+    struct BState {
+        int sv[DM_ELEMS];  // sidx of the next chunk's elements (-1: zero fill)
+    };
+    __device__ bool begin(Block& b) const {
+        const int tile = blockIdx.x;
+        b.mvalid = tile_ncols[tile];
+        if (b.mvalid <= 0) return false;  // tiles past the last one
+        b.p0 = tile_col0[tile];
+        b.h = H + (i64)tile_batch[tile] * nS;
+        b.u0 = blockIdx.y * DM_BN;
+        b.nvalid = min(DM_BN, U - b.u0);
+        b.v0 = blockIdx.z * v_chunk;
+        b.v1 = min(U, b.v0 + v_chunk);
+        b.nk = (b.v1 - b.v0 + DM_BK - 1) / DM_BK;
+        b.H2 = H2 + (i64)blockIdx.z * part_stride;
+        return b.nk > 0;
     }
-}
-
-__global__ void __launch_bounds__(B_THREADS) k_stage_b(const double* __restrict__ W, const double* __restrict__ Hf,
-                                                        const int* __restrict__ pairA, const int* __restrict__ pairB,
-                                                        const PlanCounts* __restrict__ cnt, int U, int Up, int nub,
-                                                        int v_chunk, i64 part_stride, double* __restrict__ H2) {
-    __shared__ __align__(16) double wb[B_VC][B_PAIRS];
-    __shared__ int range[2];
-    const int a = blockIdx.x;
-    // blockIdx.z = u block + nub * (chunk of v): partial sums of small problems
-    const int ub = blockIdx.z % nub, vz = blockIdx.z / nub;
-    const int v_begin = vz * v_chunk, v_end = min(U, v_begin + v_chunk);
-    H2 += (i64)vz * part_stride;
-    if (a >= cnt->nA) return;  // grids are sized by a bound on nA
-    const int nP = (int)cnt->nP;
-    if (threadIdx.x == 0) {
-        int lo = 0, hi = nP;  // first pair with pairA >= a
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (pairA[mid] < a) lo = mid + 1; else hi = mid;
-        }
-        int lo2 = lo, hi2 = nP;  // first pair with pairA > a
-        while (lo2 < hi2) {
-            const int mid = (lo2 + hi2) >> 1;
-            if (pairA[mid] <= a) lo2 = mid + 1; else hi2 = mid;
-        }
-        range[0] = lo;
-        range[1] = lo2;
-    }
-    __syncthreads();
-    const int pc = range[0] + blockIdx.y * B_PAIRS;
-    if (pc >= range[1]) return;  // uniform across the block
-    const int np = min(B_PAIRS, range[1] - pc);
-    const int u = ub * B_THREADS + threadIdx.x;
-    const bool live = u < U;
-    const double* h = Hf + (i64)a * U * U + u;
-    double acc[B_PAIRS];
+    __device__ void a_init(const Block& b, AState& st) const {
 #pragma unroll
-    for (int k = 0; k < B_PAIRS; ++k) acc[k] = 0;
-    for (int v0 = v_begin; v0 < v_end; v0 += B_VC) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < B_VC * B_PAIRS; e += B_THREADS) {
-            const int k = e / B_VC, vv = e % B_VC, v = v0 + vv;
-            wb[vv][k] = (k < np && v < v_end) ? W[(i64)pairB[pc + k] * Up + v] : 0.0;
-        }
-        __syncthreads();
-        if (live) {
-            const int vmax = min(B_VC, v_end - v0);
-            for (int vv = 0; vv < vmax; ++vv) {
-                const double g = h[(i64)(v0 + vv) * U];
-                const double2* w2 = reinterpret_cast<const double2*>(&wb[vv][0]);
-#pragma unroll
-                for (int k = 0; k < B_PAIRS / 2; ++k) {
-                    const double2 w = w2[k];
-                    acc[2 * k] = fma(w.x, g, acc[2 * k]);
-                    acc[2 * k + 1] = fma(w.y, g, acc[2 * k + 1]);
-                }
-            }
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int r = dm_rowmajor_row(threadIdx.x, q);
+            st.off[q] = r < b.mvalid ? (i64)pairB[b.p0 + r] * Up : -1;
         }
     }
-    if (live)
+    __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
+        const int k = dm_rowmajor_k(threadIdx.x), v = b.v0 + kc * DM_BK + k;
 #pragma unroll
-        for (int k = 0; k < B_PAIRS; ++k)
-            if (k < np) H2[(i64)(pc + k) * Up + u] = acc[k];
-}
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const bool ok = st.off[q] >= 0 && v < b.v1;
+            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? W + st.off[q] + v : W, ok);
+        }
+    }
+    __device__ void b_load(const Block& b, BState& st, int kc) const {
+        const int n = dm_kmajor_row(threadIdx.x), u = b.u0 + n;
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int v = b.v0 + kc * DM_BK + dm_kmajor_k(threadIdx.x, q);
+            st.sv[q] = (n < b.nvalid && v < b.v1) ? __ldg(&sidx[v * U + u]) : -1;
+        }
+    }
+    __device__ void b_init(const Block& b, BState& st) const { b_load(b, st, 0); }
+    __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
+        const int n = dm_kmajor_row(threadIdx.x);
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int sv = st.sv[q];
+            dm_cp8(tile + dm_kmajor_at(n, dm_kmajor_k(threadIdx.x, q)), sv >= 0 ? b.h + sv : b.h, sv >= 0);
+        }
+        if (kc + 1 < b.nk) b_load(b, st, kc + 1);
+    }
+    __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
+        if (m >= b.mvalid) return;
+        double* h2 = b.H2 + (i64)(b.p0 + m) * Up + b.u0 + n;
+        if (n + 1 < b.nvalid)
+            *reinterpret_cast<double2*>(h2) = make_double2(v0, v1);  // Up, u0 and n are even
+        else if (n < b.nvalid)
+            h2[0] = v0;
+    }
+};
 
 // out[i] = sum_p parts[p n + i], in order of p (deterministic)
 __global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, double* __restrict__ out) {
@@ -401,22 +518,65 @@ __global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, doub
 }
 
 // Splits of a reduction loop of length U into P chunks (chunk a multiple of
-// `grain`) so that a launch of `blocks` blocks reaches about eight blocks per
-// SM: small problems otherwise leave most SMs idle while each block walks the
+// `grain`) so that a launch of `blocks` blocks reaches about `target` blocks:
+// small problems otherwise leave most SMs idle while each block walks the
 // whole loop.
-static int split_count(i64 blocks, int U, int grain, int num_sms, int* chunk) {
-    int P = (int)std::min<i64>((8LL * num_sms + blocks - 1) / blocks, (U + grain - 1) / grain);
+static int split_count(i64 blocks, int U, int grain, i64 target, int* chunk) {
+    int P = (int)std::min<i64>((target + blocks - 1) / blocks, (U + grain - 1) / grain);
     P = std::max(1, std::min(P, 8));
     *chunk = ((U + P - 1) / P + grain - 1) / grain * grain;
     P = (U + *chunk - 1) / *chunk;
     return P;
 }
 
+// blocks per SM that the split aims at for the FP64 tensor-core tiles: one
+// wave (three fit on an SM by shared memory)
+constexpr int DM_SPLIT_TARGET = 3;
+
 // ---------------------------------------------------------------------------
 // stage C, per class: one warp per class, lanes stride over u, shuffle reduction
+// Stage C computes either every class's dot product (k_class_pairs + k_stage_c)
+// or every (pair, used key) product as one GEMM and gathers the classes from it
+// (ProductOp + k_gather_q): the GEMM reuses each H2 row across keys at
+// tensor-core rate, the per-class dots re-read an H2 row per class from L2 at
+// about a tenth of that rate.  The product wins while it computes at most
+// eight times as many dot products as there are classes, and the class list
+// is long enough (65,536) for the GEMM's latency not to dominate.  With bounded plans
+// the counts are known on the device only, so both paths are queued and each
+// kernel checks the choice (`choice`: 0 run, 1 run if the product is chosen,
+// 2 run if it is not).
+__device__ __host__ inline bool product_pays(double pairs, double keys, i64 m) {
+    return m >= 65536 && pairs * keys <= 8.0 * (double)m;
+}
+__device__ inline bool product_chosen(const PlanCounts* c, i64 m) {
+    return product_pays((double)c->nP, (double)c->nku, m);
+}
+__device__ inline bool choice_runs(int choice, const PlanCounts* c, i64 m) {
+    return choice == 0 || (choice == 1) == product_chosen(c, m);
+}
+
+__global__ void k_class_pairs(const uint64_t* keys, i64 m, const uint64_t* __restrict__ kid, int nk,
+                              const uint32_t* __restrict__ pairBits, const uint64_t* __restrict__ pairPre,
+                              const PlanCounts* __restrict__ cnt, int choice, int2* cls) {
+    // cls may alias keys: each thread reads its own entry before writing it
+    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m || !choice_runs(choice, cnt, m)) return;
+    const uint64_t p = keys[n];
+    if (p == BAD_KEYS) {
+        cls[n] = make_int2(-1, 0);
+        return;
+    }
+    int k[3];
+    unpack_keys(p, k);
+    cls[n] = make_int2((int)pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]), (int)kid[k[2]]);
+}
+
+// per class: one warp per class, lanes stride over u, shuffle reduction
 __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, const double* __restrict__ H2,
                                                   const int2* __restrict__ cls, const int* __restrict__ keyOf, i64 m,
-                                                  int U, int Up, double* __restrict__ out) {
+                                                  int U, int Up, const PlanCounts* __restrict__ cnt, int choice,
+                                                  double* __restrict__ out) {
+    if (!choice_runs(choice, cnt, m)) return;
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
     for (i64 n = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); n < m; n += warps) {
@@ -433,29 +593,98 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
     }
 }
 
-// stage C as a product: Q[p][j] = sum_u H2[p][u] Wu[j][u] for every (pair, used key),
-// then a gather val[n] = Q[p(n)][j(n)].  Chosen when nP * nku is small against m.
-__global__ void k_gather_rows(const double* __restrict__ W, const int* __restrict__ keyOf,
-                              const PlanCounts* __restrict__ cnt, int Up, double* __restrict__ Wu) {
-    const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= cnt->nku * Up) return;
-    Wu[e] = W[(i64)keyOf[e / Up] * Up + e % Up];
-}
+// Q[p][j] = sum_u H2[p][u] W[keyOf[j]][u] over the pairs and used keys (their
+// counts read on the device: blocks past them return at once)
+struct ProductOp {
+    static constexpr bool A_KMAJOR = false, B_KMAJOR = false;
+    const double* H2;
+    const double* W;
+    const int* keyOf;
+    const PlanCounts* cnt;
+    i64 m;
+    int choice, U, Up, ldq;
+    double* Q;
+    struct Block {
+        int mvalid, nvalid, nk;
+        int m0, n0;
+    };
+    struct AState {
+        i64 off[DM_ELEMS];
+    };
+    struct BState {
+        i64 off[DM_ELEMS];
+    };
+    __device__ bool begin(Block& b) const {
+        if (!choice_runs(choice, cnt, m)) return false;
+        b.m0 = blockIdx.x * DM_BM;
+        b.n0 = blockIdx.y * DM_BN;
+        b.mvalid = min(DM_BM, (int)cnt->nP - b.m0);
+        b.nvalid = min(DM_BN, (int)cnt->nku - b.n0);
+        b.nk = (U + DM_BK - 1) / DM_BK;
+        return b.mvalid > 0 && b.nvalid > 0;
+    }
+    __device__ void a_init(const Block& b, AState& st) const {
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int r = dm_rowmajor_row(threadIdx.x, q);
+            st.off[q] = r < b.mvalid ? (i64)(b.m0 + r) * Up : -1;
+        }
+    }
+    __device__ void b_init(const Block& b, BState& st) const {
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int r = dm_rowmajor_row(threadIdx.x, q);
+            st.off[q] = r < b.nvalid ? (i64)keyOf[b.n0 + r] * Up : -1;
+        }
+    }
+    __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
+        const int k = dm_rowmajor_k(threadIdx.x), u = kc * DM_BK + k;
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const bool ok = st.off[q] >= 0 && u < U;
+            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? H2 + st.off[q] + u : H2, ok);
+        }
+    }
+    __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
+        const int k = dm_rowmajor_k(threadIdx.x), u = kc * DM_BK + k;
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const bool ok = st.off[q] >= 0 && u < U;
+            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? W + st.off[q] + u : W, ok);
+        }
+    }
+    __device__ void store(const Block& b, int mm, int n, double v0, double v1) const {
+        if (mm >= b.mvalid) return;
+        double* q = Q + (i64)(b.m0 + mm) * ldq + b.n0 + n;
+        if (n < b.nvalid) q[0] = v0;
+        if (n + 1 < b.nvalid) q[1] = v1;
+    }
+};
 
-__global__ void k_gather_q(const double* __restrict__ Q, const int2* __restrict__ cls, i64 m, int nku,
-                           double* __restrict__ out) {
+// val[n] = Q[pair(n)][kid(k3)], the class's (pair, key) found from its packed keys
+__global__ void k_gather_q(const double* __restrict__ Q, const uint64_t* __restrict__ keys, i64 m,
+                           const uint64_t* __restrict__ kid, int nk, const uint32_t* __restrict__ pairBits,
+                           const uint64_t* __restrict__ pairPre, int ldq, const PlanCounts* __restrict__ cnt,
+                           int choice, double* __restrict__ out) {
     const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m) return;
-    const int2 c = cls[n];
-    out[n] = c.x >= 0 ? Q[(i64)c.x * nku + c.y] : 0.0;
+    if (n >= m || !choice_runs(choice, cnt, m)) return;
+    const uint64_t p = keys[n];
+    if (p == BAD_KEYS) {
+        out[n] = 0.0;
+        return;
+    }
+    int k[3];
+    unpack_keys(p, k);
+    const i64 pair = pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]);
+    out[n] = Q[pair * ldq + (i64)kid[k[2]]];
 }
 
 // ---------------------------------------------------------------------------
 // mixed form: stages A and B as int8-sliced products on the tensor cores
 //   stage A:  H^T[j][a] = sum_t G[j][t] W[aKey[a]][t],   G[j][t] = T[S[j] + t^2]
 //   stage B:  H2[p][u]  = sum_v Hf[a][u][v] W[pairB[p]][v]  for the pairs p of A key a
-// (Hf[a] is symmetric, so its rows serve as the K-major operand), and stage C
-// in its product form Q = H2 Wu^T with the FP64-level slicing.
+// (Hf[a] is symmetric, so its rows serve as the K-major operand); stage C
+// stays FP64 (its product form is a small DMMA GEMM).
 struct LatticeGRows {
     const double* T;
     const int* S;
@@ -525,29 +754,6 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
     __device__ bool valid(i64 p) const { return p < (i64)cnt->nP; }
 };
 
-// used key j: row W[keyOf[j]], for j below the used-key count in device memory
-struct UsedKeyRows {
-    const double* W;
-    const int* keyOf;
-    const PlanCounts* cnt;
-    i64 Up;
-    __device__ RowBase row(i64 j) const { return {W + (i64)keyOf[j] * Up}; }
-    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
-    __device__ bool valid(i64 j) const { return j < cnt->nku; }
-    GLI_IDENTITY_ROWS
-};
-
-// dense rows whose count lives in device memory (PlanCounts::nP)
-struct PairCountedRows {
-    const double* src;
-    const PlanCounts* cnt;
-    i64 ld;
-    __device__ RowBase row(i64 r) const { return {src + r * ld}; }
-    __device__ double at(const RowBase& c, int k) const { return c.p[k]; }
-    __device__ bool valid(i64 r) const { return r < (i64)cnt->nP; }
-    GLI_IDENTITY_ROWS
-};
-
 // One block: first pair, pair count and first tile of every A key (pairs are
 // ordered by A key), and the tile list of stage B (tiles of bn pairs, each in
 // one A key); tiles past the last one get no columns.
@@ -560,22 +766,17 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
     const int nP = (int)cnt->nP, nA = (int)cnt->nA;
     if (threadIdx.x == 0) carry = 0;
     for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;
+    // every A key has at least one pair, and pairs are sorted by A key: the
+    // first pair of each key is where the key changes
+    for (int p = threadIdx.x; p < nP; p += blockDim.x)
+        if (p == 0 || pairA[p] != pairA[p - 1]) first[pairA[p]] = p;
     __syncthreads();
     for (int base = 0; base < nA; base += blockDim.x) {
         const int a = base + threadIdx.x;
         int lo = 0, npairs = 0;
         if (a < nA) {
-            int hi = nP;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (pairA[mid] < a) lo = mid + 1; else hi = mid;
-            }
-            int lo2 = lo, hi2 = nP;
-            while (lo2 < hi2) {
-                const int mid = (lo2 + hi2) >> 1;
-                if (pairA[mid] <= a) lo2 = mid + 1; else hi2 = mid;
-            }
-            npairs = lo2 - lo;
+            lo = first[a];
+            npairs = (a + 1 < nA ? first[a + 1] : nP) - lo;
         }
         const int nt = (npairs + bn - 1) / bn;
         // block exclusive scan of nt
@@ -599,7 +800,6 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
         __syncthreads();
         const int t0 = carry + warp_sums[warp] + incl - nt;
         if (a < nA) {
-            first[a] = lo;
             tile0[a] = t0;
             for (int k = 0; k < nt; ++k) {
                 tile_batch[t0 + k] = a;
@@ -631,8 +831,7 @@ static TiledOperand lattice_g_slices(const LatticeTables& t, cudaStream_t s) {
     return t.g_sliced->view;
 }
 
-void dgemm_strided(int M, int N, int K, const double* A, i64 asb, i64 ar, i64 ac, const double* B, i64 bsb, i64 br,
-                   i64 bc, double* C, i64 csb, i64 cr, i64 cc, int batch, bool accumulate, cudaStream_t s);
+void dgemm_prepare();  // dense.cu: attributes of the strided FP64 GEMM
 
 static thread_local bool t_timing = false;
 static thread_local ContractStats t_last;
@@ -713,17 +912,33 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
     GLI_CUDA(cudaMemsetAsync(st, 0, sizeof(EvalStatus), s));
     PlanCounts* cnt = &st->cnt;
-    // usedKey and usedA side by side so that one scan serves both
-    DevBuf<uint32_t> used(2 * nk, s);
+    // usedKey and usedA side by side so that one scan serves both; pair flags
+    // over all key pairs (slot k2 * nk + k1)
+    const i64 words = (nk * nk + 31) / 32;
+    DevBuf<uint32_t> used(2 * nk, s), pairBits(words, s);
     used.zero();
+    pairBits.zero();
     const unsigned cb = (unsigned)((m + 255) / 256);
     const unsigned kb = (unsigned)((nk + 255) / 256);
-    k_mark_keys<<<cb, 256, 0, s>>>(a.d, a.idx, m, used.p, used.p + nk, &st->bad);
-    GLI_CHECK_LAUNCH();
+    DevBuf<short4> pts;
+    ClassDecode dec = a.d;
+    if (dec.kind == 1) {
+        pts.alloc(dec.N, s);
+        k_point_table<<<(unsigned)((dec.N + 255) / 256), 256, 0, s>>>(dec, pts.p);
+        GLI_CHECK_LAUNCH();
+        dec.pt = pts.p;
+    }
+    // packed key triple per class; reused in place for the class -> (pair, key) map
+    DevBuf<uint64_t> keys(m, s);
+    {
+        const size_t lb = mark_local_bytes(nk);
+        const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
+        k_mark<<<mb, 256, lb, s>>>(dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad, lb ? 1 : 0);
+        GLI_CHECK_LAUNCH();
+    }
     DevBuf<uint64_t> ids(2 * nk, s);
     DevBuf<int> keyOf(nk, s), aId(nk, s), aKey(nk, s);
-    const bool small = 2 * nk <= 1024;
-    if (small) {
+    if (2 * nk <= 1024) {
         k_plan_keys_small<<<1, 1024, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
         GLI_CHECK_LAUNCH();
     } else {
@@ -731,43 +946,34 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         k_plan_keys<<<kb, 256, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
         GLI_CHECK_LAUNCH();
     }
+    DevBuf<uint64_t> pairPre(words, s);
+    const bool small_pairs = bounded && words <= 8 * 1024;
+    DevBuf<uint32_t> counts;
+    if (!small_pairs) {
+        counts.alloc(words, s);
+        k_word_counts<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(words, pairBits.p, counts.p);
+        GLI_CHECK_LAUNCH();
+        exclusive_scan_u32_dev(counts.p, pairPre.p, words, &cnt->nP, s);
+    }
     if (bounded) {
         sz.nku = nk;
         sz.nA = nk;
+        // pairs (A, B) have A >= B; every class has one pair
+        sz.nP = std::min(nk * (nk + 1) / 2, m);
     } else {
         EvalStatus h;
         read_status(st, h, s);
         if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", t.kind ? "ERI" : "ERIDA");
         sz.nku = h.cnt.nku;
         sz.nA = h.cnt.nA;
-        if (sz.nku > 16384)
-            fail(GLI_ERR_LIMIT, "class list uses %lld distinct axis keys (limit 16384)", (long long)sz.nku);
-    }
-    const i64 stride = sz.nku, slots = sz.nku * sz.nku;
-    DevBuf<uint32_t> usedPair(slots, s);
-    usedPair.zero();
-    k_mark_pairs<<<cb, 256, 0, s>>>(a.d, a.idx, m, ids.p, stride, usedPair.p);
-    GLI_CHECK_LAUNCH();
-    DevBuf<uint64_t> pairId(slots, s);
-    const bool small_pairs = bounded && slots <= 65536;
-    if (!small_pairs) exclusive_scan_u32_dev(usedPair.p, pairId.p, slots, &cnt->nP, s);
-    if (bounded) {
-        // pairs (A, B) have kid(A) >= kid(B); every class has one pair
-        sz.nP = std::min(sz.nku * (sz.nku + 1) / 2, m);
-    } else {
-        EvalStatus h;
-        read_status(st, h, s);
         sz.nP = (i64)h.cnt.nP;
     }
     DevBuf<int> pairA(sz.nP, s), pairB(sz.nP, s);
     if (small_pairs)
-        k_pairs_small<<<1, 1024, 0, s>>>(slots, stride, usedPair.p, keyOf.p, aId.p, pairId.p, pairA.p, pairB.p, cnt);
+        k_pairs_small<<<1, 1024, 0, s>>>(words, (int)nk, pairBits.p, aId.p, pairPre.p, pairA.p, pairB.p, cnt);
     else
-        k_pair_lists<<<(unsigned)((slots + 255) / 256), 256, 0, s>>>(slots, stride, usedPair.p, pairId.p, keyOf.p,
-                                                                      aId.p, pairA.p, pairB.p);
-    GLI_CHECK_LAUNCH();
-    DevBuf<int2> cls(m, s);
-    k_class_pairs<<<cb, 256, 0, s>>>(a.d, a.idx, m, ids.p, stride, pairId.p, cls.p);
+        k_pair_lists<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(words, (int)nk, pairBits.p, pairPre.p, aId.p,
+                                                                      pairA.p, pairB.p);
     GLI_CHECK_LAUNCH();
 
     const i64 nA = sz.nA, nP = sz.nP, nku = sz.nku;
@@ -777,7 +983,11 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     // the mixed form runs a stage on the tensor cores when it is large enough for
     // them to pay off; smaller stages (latency-bound either way) stay FP64
     const bool tc_a = a.mixed && nA * (i64)nS >= 1000000;
-    const bool tc_b = a.mixed && nA * (i64)U * U >= 4000000;
+    // stage B on the tensor cores slices every row of the expanded Hf (nA U^2
+    // gathered values) against an FP64 product of nP U^2 FMAs: measured at
+    // ERIDA 129^3 (nP = 65 nA) the two cost the same, so the sliced form is
+    // taken only when the pairs per A key are clearly more
+    const bool tc_b = a.mixed && nA * (i64)U * U >= 4000000 && nP >= 80 * nA;
     timer.mark();
     // ---- stage A
     if (tc_a) {
@@ -796,30 +1006,21 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         w.cs = nS;
         tc_gemm_tiled(a.G, Wa.view(), w, nbt, &st->tc_err, s);
     } else {
-        // keys per thread: fewer when the problem is small, so that enough
-        // warps exist to hide the table-gather latency; small problems also
-        // split the t loop (partial sums, then one summing pass)
-        const i64 outputs = nA * (i64)nS;
-        const unsigned sb = (unsigned)((nS + A_STILE - 1) / A_STILE);
-        const int KT = (outputs >= 4000000 && nA >= 32) ? 32 : outputs >= 1000000 ? 16 : 4;
-        const unsigned kb = (unsigned)((nA + KT - 1) / KT);
+        // small problems split the t loop so that enough blocks exist
+        // (partial sums, then one summing pass)
+        const unsigned mb = (unsigned)((nS + DM_BM - 1) / DM_BM);
+        const unsigned nb = (unsigned)((nA + DM_BN - 1) / DM_BN);
         int t_chunk = U;
-        const int P = split_count((i64)sb * kb, U, A_TC, a.num_sms, &t_chunk);
+        const int P = split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
+        const i64 ps = nA * (i64)nS;
         DevBuf<double> parts;
         double* dst = H.p;
         if (P > 1) {
-            parts.alloc((i64)P * nA * nS, s);
+            parts.alloc((i64)P * ps, s);
             dst = parts.p;
         }
-        const dim3 grid(sb, kb, (unsigned)P);
-        const i64 ps = nA * (i64)nS;
-        if (KT == 32)
-            k_stage_a<32><<<grid, A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst);
-        else if (KT == 16)
-            k_stage_a<16><<<grid, A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst);
-        else
-            k_stage_a<4><<<grid, A_THREADS, 0, s>>>(t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst);
-        GLI_CHECK_LAUNCH();
+        dmma_launch(StageAOp{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst}, dim3(mb, nb, (unsigned)P),
+                    s);
         if (P > 1) {
             k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
                                                                                                       H.p);
@@ -860,16 +1061,19 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         w.cs = Up;
         tc_gemm_tiled(Hs.view(), Wb.view(), w, (int)max_tiles, &st->tc_err, s);
     } else {
-        DevBuf<double> Hf(nA * (i64)U * U, s);
-        const i64 ework = nA * (i64)U * U;
-        const i64 eb = std::min<i64>((ework + 255) / 256, (i64)a.num_sms * 32);
-        k_expand_h<<<(unsigned)eb, 256, 0, s>>>(H.p, t.sidx.p, cnt, nS, U, Hf.p);
+        // tiles of 64 pairs of one A key, then (tile, 64 u, chunk of v) blocks
+        const i64 max_tiles = nP / DM_BM + nA + 1;
+        DevBuf<int> grp(2 * nA + 3 * max_tiles, s);
+        int* tile_batch = grp.p + 2 * nA;
+        int* tile_col0 = tile_batch + max_tiles;
+        int* tile_ncols = tile_col0 + max_tiles;
+        k_pair_tiles<<<1, 1024, 0, s>>>(pairA.p, cnt, DM_BM, (int)max_tiles, grp.p, grp.p + nA, tile_batch,
+                                        tile_col0, tile_ncols);
         GLI_CHECK_LAUNCH();
-        // chunk slots per A key: at most nku pairs share one A key
-        const unsigned chunks = (unsigned)((nku + B_PAIRS - 1) / B_PAIRS);
-        const int nub = (U + B_THREADS - 1) / B_THREADS;
+        // the tile count is known on the device only: the split follows its bound
+        const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
-        const int P = split_count(nA * (i64)chunks * nub, U, 32, a.num_sms, &v_chunk);
+        const int P = split_count(max_tiles * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
         const i64 ps = nP * (i64)Up;
         DevBuf<double> parts;
         double* dst = H2.p;
@@ -877,9 +1081,9 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             parts.alloc(P * ps, s);
             dst = parts.p;
         }
-        k_stage_b<<<dim3((unsigned)nA, chunks, (unsigned)(nub * P)), B_THREADS, 0, s>>>(
-            t.W.p, Hf.p, pairA.p, pairB.p, cnt, U, Up, nub, v_chunk, ps, dst);
-        GLI_CHECK_LAUNCH();
+        dmma_launch(StageBOp{t.W.p, H.p, t.sidx.p, pairB.p, tile_batch, tile_col0, tile_ncols, nS, U, Up, v_chunk, ps,
+                             dst},
+                    dim3((unsigned)max_tiles, ub, (unsigned)P), s);
         if (P > 1) {
             k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
                                                                                                       H2.p);
@@ -891,37 +1095,26 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     // up to 16x more than the classes need on the tensor cores, as many as the
     // classes in FP64 -- but as a GEMM it reuses each H2 row across keys instead
     // of re-reading it per class; small class lists keep the per-class kernel
-    const bool product = a.mixed ? (m >= 65536 && nP * nku <= 16 * m) : (nP * nku <= m);
-    if (product) {
+    // exact plans choose here; bounded plans (whose counts are upper bounds)
+    // queue both paths and let the device choose, unless the bounds decide
+    const bool product_host = product_pays((double)nP, (double)nku, m);
+    const bool undecided = bounded && !product_host && m >= 65536;
+    const int c_prod = undecided ? 1 : 0, c_class = undecided ? 2 : 0;
+    if (undecided || product_host) {
         DevBuf<double> Q(nP * nku, s);
-        if (a.mixed) {
-            constexpr int BN = tile_n(FP64_SLICES);
-            TiledSlices Hs2, Wus;
-            const i64 pb = (nP + TC_BM - 1) / TC_BM, kb2 = (nku + BN - 1) / BN;
-            Hs2.alloc(pb, TC_BM, U, FP64_SLICES, s);
-            slice_tiled(PairCountedRows{H2.p, cnt, Up}, nP, U, Hs2, s);
-            Wus.alloc(kb2, BN, U, FP64_SLICES, s);
-            slice_tiled(UsedKeyRows{t.W.p, keyOf.p, cnt, Up}, nku, U, Wus, s);
-            TileWork w;
-            w.a_rows = (int)nP;
-            w.a_blocks = (int)pb;
-            w.n_total = (int)nku;
-            w.C = Q.p;
-            w.rs = nku;
-            w.cs = 1;
-            tc_gemm_tiled(Hs2.view(), Wus.view(), w, (int)kb2, &st->tc_err, s);
-        } else {
-            DevBuf<double> Wu(nku * (i64)Up, s);
-            k_gather_rows<<<(unsigned)((nku * Up + 255) / 256), 256, 0, s>>>(t.W.p, keyOf.p, cnt, Up, Wu.p);
-            GLI_CHECK_LAUNCH();
-            dgemm_strided((int)nP, (int)nku, U, H2.p, 0, Up, 1, Wu.p, 0, 1, Up, Q.p, 0, nku, 1, 1, false, s);
-        }
-        k_gather_q<<<cb, 256, 0, s>>>(Q.p, cls.p, m, (int)nku, a.out);
+        dmma_launch(ProductOp{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p},
+                    dim3((unsigned)((nP + DM_BM - 1) / DM_BM), (unsigned)((nku + DM_BN - 1) / DM_BN)), s);
+        k_gather_q<<<cb, 256, 0, s>>>(Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
+                                      a.out);
         GLI_CHECK_LAUNCH();
-    } else {
+    }
+    if (undecided || !product_host) {
+        int2* cls = reinterpret_cast<int2*>(keys.p);
+        k_class_pairs<<<cb, 256, 0, s>>>(keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, cnt, c_class, cls);
+        GLI_CHECK_LAUNCH();
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
-        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls.p, keyOf.p, m, U, Up, a.out);
+        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls, keyOf.p, m, U, Up, cnt, c_class, a.out);
         GLI_CHECK_LAUNCH();
     }
     timer.mark();
@@ -984,7 +1177,12 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
         e->num[k] = a.d.num[k];
     }
     e->status.alloc(1);
-    tc_gemm_prepare();  // function attributes are set outside the capture
+    // function attributes are set outside the capture
+    tc_gemm_prepare();
+    dgemm_prepare();
+    dmma_prepare<StageAOp>();
+    dmma_prepare<StageBOp>();
+    dmma_prepare<ProductOp>();
     const long long l0 = launch_count();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
@@ -1052,6 +1250,14 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
         a.d.num[k] = g.num[k];
     }
     a.d.nkeys = t.nkeys;
+    bool decodable = a.d.N < ((i64)1 << 31);
+    if (kind == 1)  // ERI: N^2 < 2^32, coordinates in 16 bits
+        for (int k = 0; k < 3; ++k)
+            decodable = decodable && a.d.N <= 65535 && std::llabs(g.istart[k]) + g.num[k] < 32767;
+    if (!decodable) fail(GLI_ERR_LIMIT, "grid of %lld points is beyond the class decoder's range", (long long)a.d.N);
+    if (t.nkeys > 8192)
+        fail(GLI_ERR_LIMIT, "grid spans %lld axis keys (limit 8192)", (long long)t.nkeys);
+    a.d.finish();
     a.idx = d_indices;
     a.m = m;
     a.out = d_out;
@@ -1076,8 +1282,6 @@ static void check_status(int kind, const EvalStatus& h, const LatticeTables& t, 
                          ContractStats* stats) {
     if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
     if (h.tc_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired (code %d)", h.tc_err);
-    if (h.cnt.nku > 16384)
-        fail(GLI_ERR_LIMIT, "class list uses %lld distinct axis keys (limit 16384)", (long long)h.cnt.nku);
     ContractStats st;
     st.keys_a = h.cnt.nA;
     st.pairs = (i64)h.cnt.nP;

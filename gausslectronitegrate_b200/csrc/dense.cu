@@ -32,6 +32,7 @@
 #include <map>
 #include <mutex>
 
+#include "dmma.cuh"
 #include "symmetry.cuh"
 #include "tables.cuh"
 #include "tc_gemm.cuh"
@@ -228,74 +229,94 @@ __global__ void k_grid_perms(SymGrid G, int64_t* __restrict__ perm) {
 // ---------------------------------------------------------------------------
 // FP64 strided batched GEMM: C[b] = A[b] * B[b] (+ C[b] when accumulate).
 // Element (i, k) of A sits at A + b*sa + i*ar + k*ac (likewise B, C), so
-// transposed operands are expressed through strides.  64 x 64 tiles, 4 x 4 per
-// thread, K staged through shared memory in chunks of 16.
+// transposed operands are expressed through strides.  The FP64 tensor-core
+// tiles of dmma.cuh; each operand tile is staged in the shared-memory layout
+// whose thread mapping reads its unit-stride direction contiguously.
 struct MatView {
     const double* p;
     i64 sb, r, c;
 };
 
-constexpr int GT = 64, GK = 16;
-
-__global__ void __launch_bounds__(256) k_dgemm(int M, int N, int K, MatView A, MatView B, double* __restrict__ C,
-                                                i64 csb, i64 cr, i64 cc, int accumulate) {
-    __shared__ double as[GK][GT + 1];
-    __shared__ double bs[GK][GT + 1];
-    const int b = blockIdx.z;
-    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-    const int i0 = blockIdx.y * GT, j0 = blockIdx.x * GT;
-    const double* Ab = A.p + (i64)b * A.sb;
-    const double* Bb = B.p + (i64)b * B.sb;
-    double acc[4][4] = {};
-    // consecutive threads walk the operand's unit-stride direction, so tile
-    // loads are coalesced for row-major, column-major and transposed views
-    const bool a_k_fast = (A.c == 1 && A.r != 1), b_k_fast = (B.r == 1 && B.c != 1);
-    for (int k0 = 0; k0 < K; k0 += GK) {
-        for (int e = threadIdx.x; e < GK * GT; e += 256) {
-            const int kk = a_k_fast ? e % GK : e / GT, ii = a_k_fast ? e / GK : e % GT;
-            const int gi = i0 + ii, gk = k0 + kk;
-            as[kk][ii] = (gi < M && gk < K) ? Ab[(i64)gi * A.r + (i64)gk * A.c] : 0.0;
-        }
-        for (int e = threadIdx.x; e < GK * GT; e += 256) {
-            const int kk = b_k_fast ? e % GK : e / GT, jj = b_k_fast ? e / GK : e % GT;
-            const int gj = j0 + jj, gk = k0 + kk;
-            bs[kk][jj] = (gj < N && gk < K) ? Bb[(i64)gk * B.r + (i64)gj * B.c] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < GK; ++kk) {
-            double a[4], bv[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[q] = as[kk][ty + 16 * q];
-                bv[q] = bs[kk][tx + 16 * q];
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int r = 0; r < 4; ++r) acc[q][r] = fma(a[q], bv[r], acc[q][r]);
-        }
-        __syncthreads();
+template <bool AK, bool BK>
+struct StridedOp {
+    static constexpr bool A_KMAJOR = AK, B_KMAJOR = BK;
+    int M, N, K;
+    MatView A, B;
+    double* C;
+    i64 csb, cr, cc;
+    int accumulate;
+    struct Block {
+        int mvalid, nvalid, nk;
+        int m0, n0;
+        const double* a;
+        const double* b;
+        double* c;
+    };
+    struct AState {};
+    struct BState {};
+    __device__ bool begin(Block& b) const {
+        b.m0 = blockIdx.y * DM_BM;
+        b.n0 = blockIdx.x * DM_BN;
+        b.mvalid = min(DM_BM, M - b.m0);
+        b.nvalid = min(DM_BN, N - b.n0);
+        b.nk = (K + DM_BK - 1) / DM_BK;
+        b.a = A.p + (i64)blockIdx.z * A.sb + (i64)b.m0 * A.r;
+        b.b = B.p + (i64)blockIdx.z * B.sb + (i64)b.n0 * B.c;
+        b.c = C + (i64)blockIdx.z * csb + (i64)b.m0 * cr + (i64)b.n0 * cc;
+        return b.mvalid > 0 && b.nvalid > 0;
     }
-    double* Cb = C + (i64)b * csb;
+    __device__ void a_init(const Block&, AState&) const {}
+    __device__ void b_init(const Block&, BState&) const {}
+    __device__ void a_issue(const Block& b, AState&, int kc, double* tile) const {
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int gi = i0 + ty + 16 * q, gj = j0 + tx + 16 * r;
-            if (gi < M && gj < N) {
-                double* c = Cb + (i64)gi * cr + (i64)gj * cc;
-                *c = accumulate ? *c + acc[q][r] : acc[q][r];
-            }
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int r = AK ? dm_kmajor_row(threadIdx.x) : dm_rowmajor_row(threadIdx.x, q);
+            const int k = AK ? dm_kmajor_k(threadIdx.x, q) : dm_rowmajor_k(threadIdx.x);
+            const int kk = kc * DM_BK + k;
+            const bool v = r < b.mvalid && kk < K;
+            dm_cp8(tile + (AK ? dm_kmajor_at(r, k) : dm_rowmajor_at(r, k)), v ? b.a + r * A.r + kk * A.c : A.p, v);
         }
-}
+    }
+    __device__ void b_issue(const Block& b, BState&, int kc, double* tile) const {
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int r = BK ? dm_kmajor_row(threadIdx.x) : dm_rowmajor_row(threadIdx.x, q);
+            const int k = BK ? dm_kmajor_k(threadIdx.x, q) : dm_rowmajor_k(threadIdx.x);
+            const int kk = kc * DM_BK + k;
+            const bool v = r < b.nvalid && kk < K;
+            dm_cp8(tile + (BK ? dm_kmajor_at(r, k) : dm_rowmajor_at(r, k)), v ? b.b + r * B.c + kk * B.r : B.p, v);
+        }
+    }
+    __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
+        if (m >= b.mvalid) return;
+        double* c = b.c + (i64)m * cr + (i64)n * cc;
+        if (n < b.nvalid) c[0] = accumulate ? c[0] + v0 : v0;
+        if (n + 1 < b.nvalid) c[cc] = accumulate ? c[cc] + v1 : v1;
+    }
+};
 
 static void dgemm(int M, int N, int K, MatView A, MatView B, double* C, i64 csb, i64 cr, i64 cc, int batch,
                   bool accumulate, cudaStream_t s) {
     if (M <= 0 || N <= 0 || batch <= 0) return;
-    dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, batch);
-    k_dgemm<<<grid, 256, 0, s>>>(M, N, K, A, B, C, csb, cr, cc, accumulate ? 1 : 0);
-    GLI_CHECK_LAUNCH();
+    const dim3 grid((N + DM_BN - 1) / DM_BN, (M + DM_BM - 1) / DM_BM, batch);
+    // stage an operand K-major when its row index is the unit-stride direction
+    const bool ak = A.r == 1 && A.c != 1, bk = B.c == 1 && B.r != 1;
+    const int acc = accumulate ? 1 : 0;
+    if (ak && bk)
+        dmma_launch(StridedOp<true, true>{M, N, K, A, B, C, csb, cr, cc, acc}, grid, s);
+    else if (ak)
+        dmma_launch(StridedOp<true, false>{M, N, K, A, B, C, csb, cr, cc, acc}, grid, s);
+    else if (bk)
+        dmma_launch(StridedOp<false, true>{M, N, K, A, B, C, csb, cr, cc, acc}, grid, s);
+    else
+        dmma_launch(StridedOp<false, false>{M, N, K, A, B, C, csb, cr, cc, acc}, grid, s);
+}
+
+void dgemm_prepare() {
+    dmma_prepare<StridedOp<true, true>>();
+    dmma_prepare<StridedOp<true, false>>();
+    dmma_prepare<StridedOp<false, true>>();
+    dmma_prepare<StridedOp<false, false>>();
 }
 
 void dgemm_strided(int M, int N, int K, const double* A, i64 asb, i64 ar, i64 ac, const double* B, i64 bsb, i64 br,

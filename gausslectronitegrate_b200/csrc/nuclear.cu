@@ -176,9 +176,11 @@ struct BatchedRows {
     __device__ bool valid(i64) const { return true; }
 };
 
-// FP64 strided batched GEMM (dense.cu)
+// FP64 strided batched GEMM (dense.cu); dgemm_prepare sets its kernel
+// attributes, outside any graph capture
 void dgemm_strided(int M, int N, int K, const double* A, i64 asb, i64 ar, i64 ac, const double* B, i64 bsb, i64 br,
                    i64 bc, double* C, i64 csb, i64 cr, i64 cc, int batch, bool accumulate, cudaStream_t s);
+void dgemm_prepare();
 
 // host copy of an instance
 struct NucHost {
@@ -366,6 +368,7 @@ static void run_chunk_graph(const std::vector<NucHost>& hosts, const NucInst* d_
                             int nb, const int* coords, const double* npos, const double* ncharge, int form,
                             int nstreams, int num_sms, int* err, cudaStream_t s) {
     tc_gemm_prepare();
+    dgemm_prepare();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     try {

@@ -71,4 +71,13 @@ __host__ __device__ inline i64 eri_axis_key(i64 s01, i64 s23, i64 cc, i64 L) {
     return (b * (b + 1) / 2 + a) * (2 * L - 1) + c;
 }
 
+// the same key in 32-bit arithmetic (keys < 2^21)
+__host__ __device__ inline int eri_axis_key32(int s01, int s23, int cc, int L) {
+    int a = s01 < 0 ? -s01 : s01;
+    int b = s23 < 0 ? -s23 : s23;
+    if (a > b) { const int t = a; a = b; b = t; }
+    const int c = cc < 0 ? -cc : cc;
+    return (b * (b + 1) / 2 + a) * (2 * L - 1) + c;
+}
+
 }  // namespace gli

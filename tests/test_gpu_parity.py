@@ -107,6 +107,40 @@ def test_eri_values_arbitrary_list(gli):
     assert_parity(vals, ref, what="ERI arbitrary list")
 
 
+@pytest.mark.parametrize("form", [0, 1])
+def test_eri_values_large_key_space(gli, form):
+    # 9^3 grid: 765 axis keys, so the plan takes exact sizes (host-read counts)
+    # and the class decode marks its key pairs in global memory; a seeded sample
+    # of indices (any order) in both forms against the oracle
+    import ctypes as C
+    from gausslectronitegrate_b200 import _abi
+    g = sym_grid(9)
+    N = 9 ** 3
+    rng = np.random.default_rng(11)
+    # half random indices, half with the four points within two spacings of
+    # one another (the large values)
+    far = rng.integers(0, N ** 4, size=150)
+    base = rng.integers(0, 9, size=(150, 1, 3))
+    pts = np.clip(base + rng.integers(-2, 3, size=(150, 4, 3)), 0, 8)
+    lin = (pts[..., 0] * 9 + pts[..., 1]) * 9 + pts[..., 2]
+    lin[::2, 1] = lin[::2, 0]  # density-density classes (i i | k k)
+    lin[::2, 3] = lin[::2, 2]
+    near = ((lin[:, 0] * N + lin[:, 1]) * N + lin[:, 2]) * N + lin[:, 3]
+    idx = np.concatenate([far, near]).astype(np.int64)
+    ref = ORACLE.values("eri", g10(), g, idx, 1e-5)
+    assert np.max(np.abs(ref)) > 0.1
+    gd, keep = gli._parse_coeffs(g10(), "")
+    vals = np.empty(idx.size)
+    rc = gli.lib().gli_b200_sparse_values(_abi.GLI_KIND_ERI, C.byref(gd), C.byref(gli._grid_struct(g)),
+                                          idx.ctypes.data_as(_abi.lptr), idx.size, 1e-5, form,
+                                          vals.ctypes.data_as(_abi.dptr))
+    assert rc == 0, gli.lib().gli_b200_last_error_message()
+    if form == 0:
+        assert_parity(vals, ref, what="ERI 9^3 sample")
+    else:
+        assert np.max(np.abs(vals - ref)) <= 1e-8
+
+
 def test_erida_values_sample_129(gli):
     # ERIDA on 129^3: enumeration count, sortedness and a seeded sample of
     # classes against the oracle (the full CPU reference takes minutes)
