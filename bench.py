@@ -364,8 +364,10 @@ def run_ours(args):
         sz3 = (_abi.glong * 3)()
         L.gli_b200_last_stage_times(ms4, sz3)
         L.gli_b200_set_timing(0)
+        plan4 = (_abi.glong * 4)()
+        L.gli_b200_last_plan(plan4)
         stage[name] = {"tables": float(ms4[0]), "A": float(ms4[1]), "B": float(ms4[2]), "C": float(ms4[3]),
-                       "sizes": (int(sz3[0]), int(sz3[1]), int(sz3[2]))}
+                       "sizes": (int(sz3[0]), int(sz3[1]), int(sz3[2])), "plan": tuple(int(x) for x in plan4)}
     nA, nP, U = stage["fp64"]["sizes"]
     peak = C.c_double()
     L.gli_b200_measure_fp64_peak(C.byref(peak))
@@ -409,7 +411,7 @@ def run_ours(args):
                    "sample": f"unavailable: {ex}"}
     st = stage[chosen]
     dom = max(("A", "B", "C"), key=lambda k: st[k])
-    roof = roofline(chosen, dom, st, nA, nP, U, m, peak.value)
+    roof = roofline(chosen, dom, st, st["plan"], U, m, peak.value)
     line = {
         "metric": METRIC, "value": main["value"], "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": main["ms_per_step"], "higher_is_better": True,
@@ -575,38 +577,42 @@ def lattice_nS(U):
     return int(np.unique((u[:, None] ** 2 + u[None, :] ** 2).ravel()).size)
 
 
-def roofline(form, dom, st, nA, nP, U, m, fp64_peak):
+def roofline(form, dom, st, plan, U, m, fp64_peak):
     """Roofline entry of the dominant stage (from the library's stage events).
-    FP64 kernels: the stage's FP64 FLOPs against the measured FP64 FMA peak.
+    FP64 stages (the FP64 tensor-core GEMM k_dmma, or the per-class dots of
+    stage C): the stage's algorithmic FP64 FLOPs against the measured FP64 peak
+    (gli_b200_measure_fp64_peak: the faster of the FMA and m8n8k4 MMA probes).
     Tensor-core stages of the mixed form: the sliced work is bound by the bytes
-    it must move (FP64 sources, int8 slices written and read, FP64 results)
-    against the measured HBM bandwidth.  The mixed form runs a stage on the
-    tensor cores only when it is large (stage A: nA nS >= 1e6 outputs; stage
-    B: nA U^2 >= 4e6), the same rule as the library."""
+    it must move (int8 slices read, FP64 results written) against the measured
+    HBM bandwidth.  The mixed form runs stage A on the tensor cores when
+    nA nS >= 1e6, stage B when nA U^2 >= 4e6 and nP >= 80 nA (the library's
+    rule); plan = (nA, nP, used keys, stage C product flag) of the step."""
+    nA, nP, nku, product = plan
     ms = st[dom]
     nS = lattice_nS(U)
     kp = (U + 63) // 64 * 64
     on_tensor_cores = form == "mixed" and ((dom == "A" and nA * nS >= 1000000) or
-                                           (dom == "B" and nA * U * U >= 4000000))
-    if not on_tensor_cores and dom != "C":
-        flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U, "C": 2.0 * m * U}[dom]
+                                           (dom == "B" and nA * U * U >= 4000000 and nP >= 80 * nA))
+    if not on_tensor_cores:
+        flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U,
+                 "C": 2.0 * (nP * nku if product else m) * U}[dom]
+        kernel = {"A": "k_dmma<StageAOp>", "B": "k_dmma<StageBOp>",
+                  "C": "k_dmma<ProductOp> + k_gather_q" if product else "k_stage_c"}[dom]
         achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
-        return {"bound": "fp64", "stage": dom,
-                "kernel": {"A": "k_stage_a", "B": "k_stage_b", "C": "k_stage_c"}[dom],
+        return {"bound": "fp64", "stage": dom, "kernel": kernel,
                 "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if achieved and fp64_peak else None,
-                "peak_source": "measured FP64 FMA probe on this device (gli_b200_measure_fp64_peak)",
+                "peak_source": "measured FP64 peak on this device (gli_b200_measure_fp64_peak: "
+                               "max of FMA and m8n8k4 MMA probes)",
                 "algorithmic_flops_per_launch": flops, "traffic": None}
     S, BN = 5, 96
     nsp = (nS + 127) // 128 * 128
     bytes_ = {"A": S * nsp * kp + S * ((nA + BN - 1) // BN * BN) * kp + 8 * nA * nS,
-              "B": 8.0 * nA * nS + 2 * S * nA * ((U + 127) // 128 * 128) * kp + 2 * S * nP * kp + 8 * nP * U,
-              "C": 8.0 * nP * U + 16 * m}[dom]
+              "B": 8.0 * nA * nS + 2 * S * nA * ((U + 127) // 128 * 128) * kp + 2 * S * nP * kp + 8 * nP * U}[dom]
     achieved = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
     peak = measured_peaks()["hbm_gbs"]
     return {"bound": "hbm", "stage": dom,
-            "kernel": {"A": "k_tc_gemm<5,5> (stage A)", "B": "k_slice_group + k_tc_gemm<5,5> (stage B)",
-                       "C": "k_stage_c"}[dom],
+            "kernel": {"A": "k_tc_gemm<5,5> (stage A)", "B": "k_slice_group + k_tc_gemm<5,5> (stage B)"}[dom],
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved and peak else None,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",

@@ -75,7 +75,8 @@ EXPORTS = [
     # extensions
     "gli_b200_last_error", "gli_b200_last_error_message", "gli_b200_device_count", "gli_b200_set_device",
     "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
-    "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_measure_fp64_peak",
+    "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_last_plan",
+    "gli_b200_measure_fp64_peak",
     "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
     "gli_b200_nuclear_batch_dev", "gli_b200_nuclear_batch", "gli_b200_last_nuclear_batch", "gli_b200_autotune_report",
     "gli_b200_autotune_selftest", "gli_b200_surrogate_train", "gli_b200_surrogate_free", "gli_b200_surrogate_info",
@@ -129,6 +130,7 @@ def load(path=LIB_PATH):
     L.gli_b200_free_dev.argtypes = [C.c_void_p, C.c_void_p]
     L.gli_b200_set_timing.argtypes = [C.c_int]
     L.gli_b200_last_stage_times.argtypes = [P(C.c_float), P(glong)]
+    L.gli_b200_last_plan.argtypes = [P(glong)]
     L.gli_b200_measure_fp64_peak.argtypes = [P(C.c_double)]
     L.gli_b200_kinetic_matrix_noalloc.argtypes = [C.c_void_p, glong, P(Grid), C.c_void_p, C.c_void_p]
     L.gli_b200_kinetic_matrix_noalloc.restype = C.c_int

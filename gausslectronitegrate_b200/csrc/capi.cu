@@ -239,6 +239,15 @@ int gli_b200_last_stage_times(float ms[4], glong sizes[3]) {
     return GLI_OK;
 }
 
+int gli_b200_last_plan(glong out[4]) {
+    const gli::ContractStats& st = gli::last_stats();
+    out[0] = st.keys_a;
+    out[1] = st.pairs;
+    out[2] = st.keys_used;
+    out[3] = st.product;
+    return GLI_OK;
+}
+
 // ---------------------------------------------------------------------------
 // kinetic (reference src/kinetic_integrals.c)
 void compute_kinetic_gausslet_integrals(const struct gausslet_data* gdata, const struct cartesian_grid_3d* grid,

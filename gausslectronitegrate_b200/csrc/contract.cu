@@ -1278,7 +1278,7 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
 }
 
 // after the stream synchronised: errors of the evaluation, and the statistics
-static void check_status(int kind, const EvalStatus& h, const LatticeTables& t, StageTimer& timer,
+static void check_status(int kind, i64 m, const EvalStatus& h, const LatticeTables& t, StageTimer& timer,
                          ContractStats* stats) {
     if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
     if (h.tc_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired (code %d)", h.tc_err);
@@ -1286,6 +1286,8 @@ static void check_status(int kind, const EvalStatus& h, const LatticeTables& t, 
     st.keys_a = h.cnt.nA;
     st.pairs = (i64)h.cnt.nP;
     st.U = t.U;
+    st.keys_used = h.cnt.nku;
+    st.product = product_pays((double)h.cnt.nP, (double)h.cnt.nku, m) ? 1 : 0;
     if (t_timing) {
         st.ms_tables = timer.between(0, 1);
         st.ms_a = timer.between(2, 3);
@@ -1306,7 +1308,7 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     StageTimer timer(t_timing, s);
     sparse_values_enqueue(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, h, tp, timer);
     GLI_CUDA(cudaStreamSynchronize(s));
-    check_status(kind, *h, *tp, timer, stats);
+    check_status(kind, m, *h, *tp, timer, stats);
 }
 
 // Device copies of a host class list and its values, kept per thread and
@@ -1348,7 +1350,7 @@ void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc
                           timer);
     GLI_CUDA(cudaMemcpyAsync(pin_val, t_host_call.val->p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
     GLI_CUDA(cudaStreamSynchronize(s));
-    check_status(kind, *hs, *tp, timer, nullptr);
+    check_status(kind, m, *hs, *tp, timer, nullptr);
     memcpy(h_out, pin_val, (size_t)m * sizeof(double));
 }
 

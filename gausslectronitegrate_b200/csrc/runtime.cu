@@ -268,6 +268,27 @@ __global__ void k_fp64_probe(double seed, int iters, double* __restrict__ sink) 
     if (s == 12345.678) sink[0] = s;  // keeps the chains live
 }
 
+// ... and the FP64 tensor-core path (mma.sync m8n8k4 f64: 256 FMAs per warp
+// instruction), 16 independent accumulator tiles per warp
+__global__ void k_dmma_probe(double seed, int iters, double* __restrict__ sink) {
+    double c[16][2];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) c[k][0] = c[k][1] = 0.0;
+    const double a = seed + threadIdx.x * 1e-9, b = 0.999999999;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                         : "+d"(c[k][0]), "+d"(c[k][1])
+                         : "d"(a), "d"(b));
+    }
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += c[k][0] + c[k][1];
+    if (s == 12345.678) sink[0] = s;
+}
+
+// FP64 peak of the device: the faster of the FMA and the tensor-core probes
 double fp64_probe_tflops() {
     Context& c = context();
     cudaStream_t s = c.stream;
@@ -276,6 +297,7 @@ double fp64_probe_tflops() {
     cudaEvent_t e0, e1;
     GLI_CUDA(cudaEventCreate(&e0));
     GLI_CUDA(cudaEventCreate(&e1));
+    float ms = 0;
     k_fp64_probe<<<blocks, threads, 0, s>>>(1.0, iters / 16, sink.p);  // warm-up
     GLI_CHECK_LAUNCH();
     GLI_CUDA(cudaEventRecord(e0, s));
@@ -283,12 +305,21 @@ double fp64_probe_tflops() {
     GLI_CHECK_LAUNCH();
     GLI_CUDA(cudaEventRecord(e1, s));
     GLI_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
     GLI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double fma_tf = 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12;
+    const int mblocks = c.num_sms * 4, miters = 1 << 11;
+    k_dmma_probe<<<mblocks, 128, 0, s>>>(1.0, miters / 16, sink.p);
+    GLI_CHECK_LAUNCH();
+    GLI_CUDA(cudaEventRecord(e0, s));
+    k_dmma_probe<<<mblocks, 128, 0, s>>>(1.0, miters, sink.p);
+    GLI_CHECK_LAUNCH();
+    GLI_CUDA(cudaEventRecord(e1, s));
+    GLI_CUDA(cudaEventSynchronize(e1));
+    GLI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double mma_tf = 2.0 * 256.0 * 16.0 * miters * (double)mblocks * 4 / (ms * 1e-3) / 1e12;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
-    return flops / (ms * 1e-3) / 1e12;
+    return fma_tf > mma_tf ? fma_tf : mma_tf;
 }
 
 }  // namespace gli

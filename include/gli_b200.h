@@ -369,8 +369,9 @@ int gli_b200_free_dev(void* d_ptr, void* stream);
  * Filled only when timing is enabled with gli_b200_set_timing(1). */
 int gli_b200_set_timing(int enable);
 
-/* Measured FP64 FMA throughput of the current device (TFLOP/s), from a
- * compute-only probe kernel; the denominator of the FP64 roofline. */
+/* Measured FP64 throughput of the current device (TFLOP/s): the faster of two
+ * compute-only probes, scalar FMA chains and FP64 tensor-core MMAs (m8n8k4);
+ * the denominator of the FP64 roofline. */
 int gli_b200_measure_fp64_peak(double* tflops);
 
 /* Number of kernels this library launched on the calling thread so far
@@ -405,6 +406,11 @@ int gli_b200_dgemm_sliced_dev(const double* d_A, glong lda, const double* d_B, g
 int gli_b200_kinetic_matrix_noalloc(const double* d_coeffs, glong num_coeffs,
 	const struct cartesian_grid_3d* grid, double* d_matrix, void* stream);
 int gli_b200_last_stage_times(float ms[4], glong sizes[3]);
+
+/* Plan of the calling thread's last sparse evaluation: out[0] A keys, out[1]
+ * (A, B) key pairs, out[2] distinct axis keys, out[3] 1 when stage C ran as
+ * the (pair, key) product GEMM, 0 when per class. */
+int gli_b200_last_plan(glong out[4]);
 
 #ifdef __cplusplus
 }
