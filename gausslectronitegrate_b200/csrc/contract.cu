@@ -535,7 +535,7 @@ constexpr int DM_SPLIT_TARGET = 3;
 
 // ---------------------------------------------------------------------------
 // stage C, per class: one warp per class, lanes stride over u, shuffle reduction
-// Stage C computes either every class's dot product (k_class_pairs + k_stage_c)
+// Stage C computes either every class's dot product (k_stage_c)
 // or every (pair, used key) product as one GEMM and gathers the classes from it
 // (ProductOp + k_gather_q): the GEMM reuses each H2 row across keys at
 // tensor-core rate, the per-class dots re-read an H2 row per class from L2 at
@@ -555,41 +555,30 @@ __device__ inline bool choice_runs(int choice, const PlanCounts* c, i64 m) {
     return choice == 0 || (choice == 1) == product_chosen(c, m);
 }
 
-__global__ void k_class_pairs(const uint64_t* keys, i64 m, const uint64_t* __restrict__ kid, int nk,
-                              const uint32_t* __restrict__ pairBits, const uint64_t* __restrict__ pairPre,
-                              const PlanCounts* __restrict__ cnt, int choice, int2* cls) {
-    // cls may alias keys: each thread reads its own entry before writing it
-    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m || !choice_runs(choice, cnt, m)) return;
-    const uint64_t p = keys[n];
-    if (p == BAD_KEYS) {
-        cls[n] = make_int2(-1, 0);
-        return;
-    }
-    int k[3];
-    unpack_keys(p, k);
-    cls[n] = make_int2((int)pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]), (int)kid[k[2]]);
-}
-
-// per class: one warp per class, lanes stride over u, shuffle reduction
+// per class: one warp per class (its pair and C key found from the packed
+// keys), lanes stride over u, shuffle reduction
 __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, const double* __restrict__ H2,
-                                                  const int2* __restrict__ cls, const int* __restrict__ keyOf, i64 m,
-                                                  int U, int Up, const PlanCounts* __restrict__ cnt, int choice,
+                                                  const uint64_t* __restrict__ keys, int nk,
+                                                  const uint32_t* __restrict__ pairBits,
+                                                  const uint64_t* __restrict__ pairPre, i64 m, int U, int Up,
+                                                  const PlanCounts* __restrict__ cnt, int choice,
                                                   double* __restrict__ out) {
     if (!choice_runs(choice, cnt, m)) return;
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
     for (i64 n = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); n < m; n += warps) {
-        const int2 c = cls[n];
+        const uint64_t p = keys[n];
         double acc = 0;
-        if (c.x >= 0) {
-            const double* w = W + (i64)keyOf[c.y] * Up;
-            const double* h = H2 + (i64)c.x * Up;
+        if (p != BAD_KEYS) {
+            int k[3];
+            unpack_keys(p, k);
+            const double* w = W + (i64)k[2] * Up;
+            const double* h = H2 + pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]) * Up;
             for (int u = lane; u < U; u += 32) acc = fma(w[u], h[u], acc);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) out[n] = (c.x >= 0) ? acc : 0.0;
+        if (lane == 0) out[n] = acc;
     }
 }
 
@@ -928,7 +917,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         GLI_CHECK_LAUNCH();
         dec.pt = pts.p;
     }
-    // packed key triple per class; reused in place for the class -> (pair, key) map
+    // packed key triple per class
     DevBuf<uint64_t> keys(m, s);
     {
         const size_t lb = mark_local_bytes(nk);
@@ -1109,12 +1098,10 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         GLI_CHECK_LAUNCH();
     }
     if (undecided || !product_host) {
-        int2* cls = reinterpret_cast<int2*>(keys.p);
-        k_class_pairs<<<cb, 256, 0, s>>>(keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, cnt, c_class, cls);
-        GLI_CHECK_LAUNCH();
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
-        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, cls, keyOf.p, m, U, Up, cnt, c_class, a.out);
+        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, keys.p, (int)nk, pairBits.p, pairPre.p, m, U, Up, cnt, c_class,
+                                     a.out);
         GLI_CHECK_LAUNCH();
     }
     timer.mark();
