@@ -25,6 +25,12 @@ are bracketed by a barrier and device synchronisation, and the slowest rank's
 time counts.  N > 1 (torchrun, one process per GPU): every rank evaluates its
 own copy of the workload (weak scaling, no data-path collective).
 
+Other hot-path configurations (--workload): erida129 (ERIDA 128^3, odd
+stand-in 129^3, spacing 0.3), eri7 (ERI on the 6x6x6 configuration's odd
+stand-in 7^3, 3,571,977 classes, spacing 0.7), nuclear-batch (256 H_n chains)
+and erida129-surrogate (MLP far field); --profile-only K runs K untimed
+evaluations for profilers.
+
 --impl reference times the reference's own CPU implementation (the reference C
 core compiled under oracle/_ref, OpenMP on all host cores) on the same
 workload and prints the same JSON line with "impl": "reference".
@@ -58,11 +64,15 @@ SPACING = 0.5        # bohr
 TOL = 1e-16
 WORKLOAD = "ERIDA 32^3 grid (odd stand-in 33^3, 6545 classes), spacing 0.5 bohr, G10, tol 1e-16"
 
+KIND = "erida"       # class type of the workload: "erida" (two-index) or "eri" (four-index)
+
 # the other hot-path configurations (--workload); the default line is the metric's
 WORKLOADS = {
-    "erida33": (33, 0.5, WORKLOAD),
+    "erida33": (33, 0.5, WORKLOAD, "erida"),
     "erida129": (129, 0.3, "ERIDA 128^3 grid (odd stand-in 129^3, 366145 classes), spacing 0.3 bohr, G10, "
-                           "tol 1e-16"),
+                           "tol 1e-16", "erida"),
+    "eri7": (7, 0.7, "ERI 6x6x6 grid (odd stand-in 7^3, 3571977 classes), spacing 0.7 bohr, G10, tol 1e-16",
+             "eri"),
 }
 
 
@@ -171,7 +181,7 @@ def cpu_reference_rate(b, spec, idx, tol, min_seconds=8.0):
     reps, t0 = 0, time.perf_counter()
     vals = None
     while True:
-        vals = r.sparse_values("erida", b, spec, sample, tol)
+        vals = r.sparse_values(KIND, b, spec, sample, tol)
         reps += 1
         el = time.perf_counter() - t0
         if el >= min_seconds or reps >= 50:
@@ -217,15 +227,15 @@ def run_reference(args):
     r = RefLib()
     b = g10()
     spec = grid_spec()
-    full = r.enumerate("erida", spec)
+    full = r.enumerate(KIND, spec)
     idx = full if full.size <= CPU_SAMPLE else np.sort(
         np.random.default_rng(0).choice(full, size=CPU_SAMPLE, replace=False))
     for _ in range(min(args.warmup, 1)):
-        r.sparse_values("erida", b, spec, idx, TOL)
+        r.sparse_values(KIND, b, spec, idx, TOL)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        r.sparse_values("erida", b, spec, idx, TOL)
+        r.sparse_values(KIND, b, spec, idx, TOL)
         times.append(time.perf_counter() - t0)
     tot = sum(times)
     value = args.steps * idx.size / tot
@@ -255,6 +265,7 @@ def run_ours(args):
     L = gli.lib()
     L.gli_b200_set_device(local)
     FORMS = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}
+    KIND_ID = _abi.GLI_KIND_ERI if KIND == "eri" else _abi.GLI_KIND_ERIDA
     chosen = args.form
     other = "fp64" if chosen == "mixed" else "mixed"
     b = np.ascontiguousarray(g10())
@@ -270,7 +281,7 @@ def run_ours(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
-        rc = L.gli_b200_enumerate_dev(0, C.byref(gs), C.byref(d_idx), C.byref(num), sptr)
+        rc = L.gli_b200_enumerate_dev(KIND_ID, C.byref(gs), C.byref(d_idx), C.byref(num), sptr)
         e1.record(stream)
     if rc:
         raise RuntimeError(L.gli_b200_last_error_message().decode())
@@ -282,7 +293,7 @@ def run_ours(args):
     coeff_p = b.ctypes.data_as(_abi.dptr)
 
     def step(f):
-        rc = L.gli_b200_sparse_values_dev(0, coeff_p, b.size, C.byref(gs), d_idx, m, TOL, f,
+        rc = L.gli_b200_sparse_values_dev(KIND_ID, coeff_p, b.size, C.byref(gs), d_idx, m, TOL, f,
                                           C.c_void_p(out.data_ptr()), sptr)
         if rc:
             raise RuntimeError(L.gli_b200_last_error_message().decode())
@@ -377,15 +388,15 @@ def run_ours(args):
     # device->host copy of the values inside the timed call); the host class
     # list comes from the reference-facing enumeration call
     idx_s = _abi.SparseIndices()
-    L.enumerate_symmetry_reduced_erida_indices(C.byref(gs), C.byref(idx_s))
+    getattr(L, f"enumerate_symmetry_reduced_{KIND}_indices")(C.byref(gs), C.byref(idx_s))
     idx_np = np.ctypeslib.as_array(idx_s.indices, shape=(idx_s.num,)).copy()
-    L.delete_sparse_erida_indices(C.byref(idx_s))
+    getattr(L, f"delete_sparse_{KIND}_indices")(C.byref(idx_s))
     gd, keep = gli._parse_coeffs(b, "")
     host_vals = np.empty(m)
     e2e_times = []
     for k in range(max(3, args.steps) + 1):
         t0 = time.perf_counter()
-        rc = L.gli_b200_sparse_values(_abi.GLI_KIND_ERIDA, C.byref(gd), C.byref(gs), idx_np.ctypes.data_as(_abi.lptr),
+        rc = L.gli_b200_sparse_values(KIND_ID, C.byref(gd), C.byref(gs), idx_np.ctypes.data_as(_abi.lptr),
                                       m, TOL, FORMS[chosen], host_vals.ctypes.data_as(_abi.dptr))
         e2e_times.append(time.perf_counter() - t0)
         if rc:
@@ -637,16 +648,16 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-json", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["erida33", "erida129", "nuclear-batch", "erida129-surrogate"],
+    ap.add_argument("--workload", choices=["erida33", "erida129", "eri7", "nuclear-batch", "erida129-surrogate"],
                     default="erida33", help="erida33 is the metric's configuration (the default line)")
     ap.add_argument("--profile-only", type=int, default=0, metavar="K",
                     help="run K untimed evaluations of --form and print nothing (for profilers)")
     ap.add_argument("--instances", type=int, default=256, help="nuclear-batch: number of H_n chains")
     ap.add_argument("--train-steps", type=int, default=40000, help="erida129-surrogate: training steps")
     args = ap.parse_args()
-    global L_GRID, SPACING, WORKLOAD
+    global L_GRID, SPACING, WORKLOAD, KIND
     if args.workload in WORKLOADS:
-        L_GRID, SPACING, WORKLOAD = WORKLOADS[args.workload]
+        L_GRID, SPACING, WORKLOAD, KIND = WORKLOADS[args.workload]
     if args.cpu_baseline_json:
         return cpu_baseline_main(args.cpu_baseline_json)
     if args.workload == "nuclear-batch":

@@ -887,6 +887,9 @@ struct EvalSizes {
 // product form of stage C.
 constexpr i64 BOUNDED_KEYS = 256;
 
+// stage A runs on the tensor cores (mixed form) from this many outputs nA nS
+constexpr i64 TC_A_OUTPUTS = 1000000;
+
 static void read_status(EvalStatus* d_st, EvalStatus& h, cudaStream_t s) {
     GLI_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
     GLI_CUDA(cudaStreamSynchronize(s));
@@ -971,7 +974,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     DevBuf<double> H(nA * (i64)nS, s);
     // the mixed form runs a stage on the tensor cores when it is large enough for
     // them to pay off; smaller stages (latency-bound either way) stay FP64
-    const bool tc_a = a.mixed && nA * (i64)nS >= 1000000;
+    const bool tc_a = a.mixed && nA * (i64)nS >= TC_A_OUTPUTS;
     // stage B on the tensor cores slices every row of the expanded Hf (nA U^2
     // gathered values) against an FP64 product of nP U^2 FMAs: measured at
     // ERIDA 129^3 (nP = 65 nA) the two cost the same, so the sliced form is
@@ -1227,7 +1230,9 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     EvalArgs a;
     a.mixed = form == FORM_MIXED;
     a.t = &t;
-    if (a.mixed) a.G = lattice_g_slices(t, s);
+    // the G slices exist for stage A on the tensor cores, which needs at least
+    // 1e6 stage-A outputs (nA <= nkeys A keys); built once per table set
+    if (a.mixed && t.nkeys * t.nS >= TC_A_OUTPUTS) a.G = lattice_g_slices(t, s);
     timer.mark();
     a.d.kind = kind;
     a.d.N = g.points();
