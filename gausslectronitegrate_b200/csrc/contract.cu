@@ -347,8 +347,11 @@ __global__ void k_pair_lists(i64 words, int nk, const uint32_t* __restrict__ bit
 // table entries, so a warp's 32 gathers touch a few cache lines), and the
 // FP64 tensor-core tiles of dmma.cuh.  blockIdx.z selects a chunk of t: small
 // problems sum partial products afterwards (k_sum_parts).
+template <int BN_>
 struct StageAOp {
     static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
+    static constexpr int BN = BN_;
+    static constexpr int NB = BN / 8;  // B elements per thread
     const double* W;
     const double* T;
     const int* S;
@@ -367,15 +370,15 @@ struct StageAOp {
         bool ok;
     };
     struct BState {
-        i64 off[DM_ELEMS];  // aKey * Up of this thread's rows, -1 past nA
+        i64 off[NB];  // aKey * Up of this thread's rows, -1 past nA
     };
     __device__ bool begin(Block& b) const {
         const int nA = (int)cnt->nA;
-        b.n0 = blockIdx.y * DM_BN;
+        b.n0 = blockIdx.y * BN;
         if (b.n0 >= nA) return false;  // grids are sized by a bound on nA
         b.m0 = blockIdx.x * DM_BM;
         b.mvalid = min(DM_BM, nS - b.m0);
-        b.nvalid = min(DM_BN, nA - b.n0);
+        b.nvalid = min(BN, nA - b.n0);
         b.t0 = blockIdx.z * t_chunk;
         b.t1 = min(U, b.t0 + t_chunk);
         b.nk = (b.t1 - b.t0 + DM_BK - 1) / DM_BK;
@@ -398,7 +401,7 @@ struct StageAOp {
     }
     __device__ void b_init(const Block& b, BState& st) const {
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
+        for (int q = 0; q < NB; ++q) {
             const int r = dm_rowmajor_row(threadIdx.x, q);
             st.off[q] = r < b.nvalid ? (i64)aKey[b.n0 + r] * Up : -1;
         }
@@ -406,7 +409,7 @@ struct StageAOp {
     __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
         const int k = dm_rowmajor_k(threadIdx.x), t = b.t0 + kc * DM_BK + k;
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
+        for (int q = 0; q < NB; ++q) {
             const bool v = st.off[q] >= 0 && t < b.t1;
             dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), v ? W + st.off[q] + t : W, v);
         }
@@ -429,6 +432,7 @@ struct StageAOp {
 // dependent gathers do not wait on them.
 struct StageBOp {
     static constexpr bool A_KMAJOR = false, B_KMAJOR = true;
+    static constexpr int BN = DM_BN;
     const double* W;
     const double* H;
     const int* sidx;
@@ -529,6 +533,10 @@ static int split_count(i64 blocks, int U, int grain, i64 target, int* chunk) {
     return P;
 }
 
+// column-tile width of the FP64 tensor-core GEMM for n columns: 80 where it
+// needs fewer tiles than 64 (129 keys: two tiles instead of three)
+static int col_tile(i64 n) { return (n + 79) / 80 < (n + 63) / 64 ? 80 : 64; }
+
 // blocks per SM that the split aims at for the FP64 tensor-core tiles: one
 // wave (three fit on an SM by shared memory)
 constexpr int DM_SPLIT_TARGET = 3;
@@ -584,8 +592,11 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
 
 // Q[p][j] = sum_u H2[p][u] W[keyOf[j]][u] over the pairs and used keys (their
 // counts read on the device: blocks past them return at once)
+template <int BN_>
 struct ProductOp {
     static constexpr bool A_KMAJOR = false, B_KMAJOR = false;
+    static constexpr int BN = BN_;
+    static constexpr int NB = BN / 8;  // B elements per thread
     const double* H2;
     const double* W;
     const int* keyOf;
@@ -601,14 +612,14 @@ struct ProductOp {
         i64 off[DM_ELEMS];
     };
     struct BState {
-        i64 off[DM_ELEMS];
+        i64 off[NB];
     };
     __device__ bool begin(Block& b) const {
         if (!choice_runs(choice, cnt, m)) return false;
         b.m0 = blockIdx.x * DM_BM;
-        b.n0 = blockIdx.y * DM_BN;
+        b.n0 = blockIdx.y * BN;
         b.mvalid = min(DM_BM, (int)cnt->nP - b.m0);
-        b.nvalid = min(DM_BN, (int)cnt->nku - b.n0);
+        b.nvalid = min(BN, (int)cnt->nku - b.n0);
         b.nk = (U + DM_BK - 1) / DM_BK;
         return b.mvalid > 0 && b.nvalid > 0;
     }
@@ -621,7 +632,7 @@ struct ProductOp {
     }
     __device__ void b_init(const Block& b, BState& st) const {
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
+        for (int q = 0; q < NB; ++q) {
             const int r = dm_rowmajor_row(threadIdx.x, q);
             st.off[q] = r < b.nvalid ? (i64)keyOf[b.n0 + r] * Up : -1;
         }
@@ -637,7 +648,7 @@ struct ProductOp {
     __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
         const int k = dm_rowmajor_k(threadIdx.x), u = kc * DM_BK + k;
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
+        for (int q = 0; q < NB; ++q) {
             const bool ok = st.off[q] >= 0 && u < U;
             dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? W + st.off[q] + u : W, ok);
         }
@@ -1001,7 +1012,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         // small problems split the t loop so that enough blocks exist
         // (partial sums, then one summing pass)
         const unsigned mb = (unsigned)((nS + DM_BM - 1) / DM_BM);
-        const unsigned nb = (unsigned)((nA + DM_BN - 1) / DM_BN);
+        const int bn = col_tile(nA);
+        const unsigned nb = (unsigned)((nA + bn - 1) / bn);
         int t_chunk = U;
         const int P = split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
         const i64 ps = nA * (i64)nS;
@@ -1011,8 +1023,12 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             parts.alloc((i64)P * ps, s);
             dst = parts.p;
         }
-        dmma_launch(StageAOp{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst}, dim3(mb, nb, (unsigned)P),
-                    s);
+        if (bn == 80)
+            dmma_launch(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
+                        dim3(mb, nb, (unsigned)P), s);
+        else
+            dmma_launch(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
+                        dim3(mb, nb, (unsigned)P), s);
         if (P > 1) {
             k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
                                                                                                       H.p);
@@ -1094,8 +1110,12 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     const int c_prod = undecided ? 1 : 0, c_class = undecided ? 2 : 0;
     if (undecided || product_host) {
         DevBuf<double> Q(nP * nku, s);
-        dmma_launch(ProductOp{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p},
-                    dim3((unsigned)((nP + DM_BM - 1) / DM_BM), (unsigned)((nku + DM_BN - 1) / DM_BN)), s);
+        const int bn = col_tile(nku);
+        const dim3 grid((unsigned)((nP + DM_BM - 1) / DM_BM), (unsigned)((nku + bn - 1) / bn));
+        if (bn == 80)
+            dmma_launch(ProductOp<80>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
+        else
+            dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
         k_gather_q<<<cb, 256, 0, s>>>(Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
                                       a.out);
         GLI_CHECK_LAUNCH();
@@ -1170,9 +1190,11 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     // function attributes are set outside the capture
     tc_gemm_prepare();
     dgemm_prepare();
-    dmma_prepare<StageAOp>();
+    dmma_prepare<StageAOp<64>>();
+    dmma_prepare<StageAOp<80>>();
     dmma_prepare<StageBOp>();
-    dmma_prepare<ProductOp>();
+    dmma_prepare<ProductOp<64>>();
+    dmma_prepare<ProductOp<80>>();
     const long long l0 = launch_count();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;

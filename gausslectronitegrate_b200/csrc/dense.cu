@@ -240,6 +240,7 @@ struct MatView {
 template <bool AK, bool BK>
 struct StridedOp {
     static constexpr bool A_KMAJOR = AK, B_KMAJOR = BK;
+    static constexpr int BN = DM_BN;
     int M, N, K;
     MatView A, B;
     double* C;

@@ -1,12 +1,14 @@
 // FP64 tensor-core tiles: mma.sync.m8n8k4.f64 over operand tiles that the
 // caller gathers into shared memory with 8-byte cp.async copies.
 //
-// A block (4 warps) computes a 64 x 64 tile of C = A B over K in chunks of 16,
-// three chunks in flight (cp.async groups; the waits are the hardware's own
-// group waits, no flag spins).  Warp w owns the 32 x 32 quadrant
-// (w & 1, w >> 1) as 4 x 4 m8n8 accumulators (32 doubles per thread); per
-// k-step of 4 it reads 4 A and 4 B fragments (one double each) for 16 MMAs of
-// 256 FMAs, so operand traffic through shared memory is 1/16 of the FMA count.
+// A block (4 warps) computes a 64 x BN tile of C = A B (BN = 64 or 80, chosen
+// per Op) over K in chunks of 16, three chunks in flight (cp.async groups; the
+// waits are the hardware's own group waits, no flag spins).  Warp w owns the
+// 32 x BN/2 quadrant (w & 1, w >> 1) as 4 x BN/16 m8n8 accumulators; per
+// k-step of 4 it reads 4 A and BN/16 B fragments (one double each) for
+// 4 BN/16 MMAs of 256 FMAs.  BN = 80 serves 65..80 and 129..160 columns in
+// one and two column tiles (129 keys: 2 tiles instead of 3, measured 20%
+// faster on the stage A shape).
 //
 // The operand sources are arbitrary: an Op class says, per tile element, where
 // the double comes from (a strided matrix, a lattice-table gather, a gather
@@ -15,8 +17,10 @@
 // that coalesces the global reads also writes shared memory without bank
 // conflicts, and so that the fragment reads (row = lane / 4, k = lane % 4) are
 // conflict-free in both:
-//   K-major  [k][row], 68 doubles per k    (rows are the unit-stride direction)
-//   row-major [row][k], 20 doubles per row (k is the unit-stride direction)
+//   K-major  [k][row], rows + 4 doubles per k (rows are the unit-stride direction)
+//   row-major [row][k], 20 doubles per row    (k is the unit-stride direction)
+// (rows + 4 and 20 are 4 mod 16 doubles, so the 16 (row, k) pairs of a half
+// warp's fragment read fall in distinct bank pairs.)
 // Fragment layouts of m8n8k4 (PTX ISA, mma .f64 m8n8k4): A row = lane/4,
 // k = lane%4; B k = lane%4, column = lane/4; C row = lane/4, columns
 // 2 (lane%4) + {0, 1}.
@@ -30,16 +34,20 @@ namespace gli {
 
 constexpr int DM_BM = 64, DM_BN = 64, DM_BK = 16, DM_STAGES = 3, DM_THREADS = 128;
 constexpr int DM_LDK = DM_BK + 4;          // row-major tile: doubles per row
-constexpr int DM_LDR = DM_BM + 4;          // K-major tile: doubles per k
-constexpr int DM_TILE = DM_BM * DM_LDK;    // doubles per operand tile (>= DM_BK * DM_LDR)
-constexpr int DM_SMEM = DM_STAGES * 2 * DM_TILE * (int)sizeof(double);  // 61,440 bytes
-static_assert(DM_TILE >= DM_BK * DM_LDR, "operand tile too small for the K-major layout");
-static_assert(DM_BM == DM_BN, "one thread mapping serves both operands");
+constexpr int DM_LDR = DM_BM + 4;          // K-major 64-row tile: doubles per k
+constexpr int DM_TILE_A = DM_BM * DM_LDK;  // doubles of the A tile (>= DM_BK * DM_LDR)
+static_assert(DM_TILE_A >= DM_BK * DM_LDR, "operand tile too small for the K-major layout");
 
-// Thread tid's q-th element (q < 8) of a 64 x 16 operand tile:
-//   K-major:   row = tid & 63,          k = (tid >> 6) + 2 q
-//   row-major: row = (tid >> 4) + 8 q,  k = tid & 15
-constexpr int DM_ELEMS = DM_BM * DM_BK / DM_THREADS;  // 8
+// doubles of a B tile of BN rows, and the shared memory of a launch
+__host__ __device__ constexpr int dm_tile_b(int bn) { return bn * DM_LDK; }
+__host__ __device__ constexpr int dm_smem(int bn) {
+    return DM_STAGES * (DM_TILE_A + dm_tile_b(bn)) * (int)sizeof(double);
+}
+
+// Thread tid's q-th element of a rows x 16 operand tile:
+//   K-major (64 rows):  row = tid & 63,          k = (tid >> 6) + 2 q,  q < 8
+//   row-major:          row = (tid >> 4) + 8 q,  k = tid & 15,          q < rows / 8
+constexpr int DM_ELEMS = DM_BM * DM_BK / DM_THREADS;  // 8: the 64-row tiles
 
 __device__ __forceinline__ int dm_kmajor_row(int tid) { return tid & 63; }
 __device__ __forceinline__ int dm_kmajor_k(int tid, int q) { return (tid >> 6) + 2 * q; }
@@ -74,21 +82,24 @@ __device__ __forceinline__ double dm_frag(const double* s, int row0, int k0, int
 }
 
 // Op interface (all device, const):
-//   static constexpr bool A_KMAJOR, B_KMAJOR;
+//   static constexpr bool A_KMAJOR, B_KMAJOR;  static constexpr int BN (64 or 80;
+//   K-major B tiles have 64 rows)
 //   struct Block { int mvalid, nvalid, nk; ... };       the block's work item
 //   struct AState; struct BState;                       per-thread cached row data
 //   bool begin(Block&)                                  false: nothing to do (uniform)
 //   void a_init(const Block&, AState&), b_init(...)
-//   void a_issue(const Block&, AState&, int kc, double* tile)   8 cp.async of chunk kc
+//   void a_issue(const Block&, AState&, int kc, double* tile)   cp.async of chunk kc
 //   void b_issue(const Block&, BState&, int kc, double* tile)   (chunks issued in order)
 //   void store(const Block&, int m, int n, double v_n, double v_n1)   C[m][n], C[m][n+1]
+//
 // The k loop of one block; FULL: every m8n8 tile of the warp's quadrant holds
 // data, so the MMAs run unpredicated (a runtime predicate per MMA costs about
 // a fifth of the tensor-pipe throughput).
 template <class Op, bool FULL>
 __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Block& blk, typename Op::AState& as,
                                             typename Op::BState& bs, double* smem, int wm, int wn, int mt, int nt,
-                                            double (&acc)[4][4][2]) {
+                                            double (&acc)[4][Op::BN / 16][2]) {
+    constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN);
     const int lane = threadIdx.x & 31;
     const int nk = blk.nk;
     for (int kc = 0; kc < nk; ++kc) {
@@ -97,23 +108,23 @@ __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Blo
         const int nx = kc + DM_STAGES - 1;
         if (nx < nk) {
             const int st = nx % DM_STAGES;
-            op.a_issue(blk, as, nx, smem + st * 2 * DM_TILE);
-            op.b_issue(blk, bs, nx, smem + st * 2 * DM_TILE + DM_TILE);
+            op.a_issue(blk, as, nx, smem + st * STAGE);
+            op.b_issue(blk, bs, nx, smem + st * STAGE + DM_TILE_A);
         }
         dm_commit();
-        const double* a_s = smem + (kc % DM_STAGES) * 2 * DM_TILE;
-        const double* b_s = a_s + DM_TILE;
+        const double* a_s = smem + (kc % DM_STAGES) * STAGE;
+        const double* b_s = a_s + DM_TILE_A;
 #pragma unroll
         for (int k0 = 0; k0 < DM_BK; k0 += 4) {
-            double af[4], bf[4];
+            double af[4], bf[NJ];
 #pragma unroll
             for (int i = 0; i < 4; ++i) af[i] = dm_frag<Op::A_KMAJOR>(a_s, wm + 8 * i, k0, lane);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) bf[j] = dm_frag<Op::B_KMAJOR>(b_s, wn + 8 * j, k0, lane);
+            for (int j = 0; j < NJ; ++j) bf[j] = dm_frag<Op::B_KMAJOR>(b_s, wn + 8 * j, k0, lane);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
+                for (int j = 0; j < NJ; ++j)
                     if (FULL || (i < mt && j < nt)) dm_mma(acc[i][j], af[i], bf[j]);
         }
     }
@@ -121,11 +132,13 @@ __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Blo
 
 template <class Op>
 __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
+    constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN);
+    static_assert(Op::BN == 64 || (Op::BN == 80 && !Op::B_KMAJOR), "column tiles of 64, or 80 read row-major");
     extern __shared__ __align__(16) double dm_smem[];
     typename Op::Block blk;
     if (!op.begin(blk)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * (Op::BN / 2);
     typename Op::AState as;
     typename Op::BState bs;
     op.a_init(blk, as);
@@ -133,20 +146,20 @@ __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
 #pragma unroll
     for (int st = 0; st < DM_STAGES - 1; ++st) {
         if (st < blk.nk) {
-            op.a_issue(blk, as, st, dm_smem + st * 2 * DM_TILE);
-            op.b_issue(blk, bs, st, dm_smem + st * 2 * DM_TILE + DM_TILE);
+            op.a_issue(blk, as, st, dm_smem + st * STAGE);
+            op.b_issue(blk, bs, st, dm_smem + st * STAGE + DM_TILE_A);
         }
         dm_commit();
     }
     // m8 / n8 tiles of this warp's quadrant that hold rows / columns (warp-uniform)
     const int mt = min(4, max(0, (blk.mvalid - wm + 7) >> 3));
-    const int nt = min(4, max(0, (blk.nvalid - wn + 7) >> 3));
-    double acc[4][4][2];
+    const int nt = min(NJ, max(0, (blk.nvalid - wn + 7) >> 3));
+    double acc[4][NJ][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    if (mt == 4 && nt == 4)
+        for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    if (mt == 4 && nt == NJ)
         dm_mainloop<Op, true>(op, blk, as, bs, dm_smem, wm, wn, mt, nt, acc);
     else
         dm_mainloop<Op, false>(op, blk, as, bs, dm_smem, wm, wn, mt, nt, acc);
@@ -154,12 +167,12 @@ __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < NJ; ++j)
             if (i < mt && j < nt)
                 op.store(blk, wm + 8 * i + (lane >> 2), wn + 8 * j + 2 * (lane & 3), acc[i][j][0], acc[i][j][1]);
 }
 
-// (three blocks per SM: 3 x 60 KB of shared memory, at most 170 registers)
+// (three blocks per SM: 3 x 60 or 69 KB of shared memory, at most 170 registers)
 
 // shared memory above the 48 KB default: set once per device and Op type,
 // outside any graph capture (cudaFuncSetAttribute is not a stream operation)
@@ -170,7 +183,7 @@ void dmma_prepare() {
     GLI_CUDA(cudaGetDevice(&dev));
     const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
     if (bit && (done.load() & bit)) return;
-    GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, DM_SMEM));
+    GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, dm_smem(Op::BN)));
     done.fetch_or(bit);
 }
 
@@ -179,7 +192,7 @@ template <class Op>
 void dmma_launch(const Op& op, dim3 grid, cudaStream_t s) {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
     dmma_prepare<Op>();
-    k_dmma<Op><<<grid, DM_THREADS, DM_SMEM, s>>>(op);
+    k_dmma<Op><<<grid, DM_THREADS, dm_smem(Op::BN), s>>>(op);
     GLI_CHECK_LAUNCH();
 }
 

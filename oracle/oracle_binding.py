@@ -24,6 +24,10 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE, "restated"], check=True)
     if os.path.isdir("/root/reference/src"):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        # the reference's own Python module linked against the B200 library
+        # (the drop-in check), once that library is built
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "gausslectronitegrate_b200", "libgli_b200.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "dropin"], check=True)
 
 
 def _grid6(grid):
