@@ -308,10 +308,11 @@ static void ensure_streams(int device, int n) {
 }
 
 // Queues one chunk of instances (descriptors already on the device): weights,
-// field, per-instance contractions on `nstreams` forked streams, scatter.
-// Makes no call that a stream capture forbids.
+// field, per-instance contractions on `nstreams` forked streams (int8-sliced
+// tensor-core products when `sliced`, else the FP64 tensor-core GEMM),
+// scatter.  Makes no call that a stream capture forbids.
 static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_inst, const double* F, int nf, int nb,
-                          const int* coords, const double* npos, const double* ncharge, int form, int nstreams,
+                          const int* coords, const double* npos, const double* ncharge, bool sliced, int nstreams,
                           int num_sms, int* err, cudaStream_t s) {
     const int ni = (int)hosts.size();
     i64 w_total = 0, phi_total = 0, vk_total = 0;
@@ -329,7 +330,6 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
         max_rows = std::max(max_rows, (i64)h.d.U[0] * h.d.U[1]);
         max_n = std::max(max_n, h.d.N);
     }
-    const bool mixed = form == FORM_MIXED;
     DevBuf<double> W(w_total, s), Phi(phi_total, s), Vk(vk_total, s);
     k_nuc_weights<<<dim3((unsigned)((max_u + 127) / 128), (unsigned)max_nk, (unsigned)(3 * ni)), 128, 0, s>>>(
         d_inst, F, nf, nb, coords, W.p);
@@ -348,7 +348,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
     for (int k = 0; k < ni; ++k) {
         cudaStream_t st = t_ring.streams[k % nstreams];
         const NucInst& in = hosts[order[k]].d;
-        if (mixed)
+        if (sliced)
             nuc_contract_mixed(in, W.p, Phi.p, Vk.p, err, st);
         else
             nuc_contract_fp64(in, W.p, Phi.p, Vk.p, st);
@@ -365,14 +365,14 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
 
 // Captures the chunk as one CUDA graph and launches it once
 static void run_chunk_graph(const std::vector<NucHost>& hosts, const NucInst* d_inst, const double* F, int nf,
-                            int nb, const int* coords, const double* npos, const double* ncharge, int form,
+                            int nb, const int* coords, const double* npos, const double* ncharge, bool sliced,
                             int nstreams, int num_sms, int* err, cudaStream_t s) {
     tc_gemm_prepare();
     dgemm_prepare();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     try {
-        enqueue_chunk(hosts, d_inst, F, nf, nb, coords, npos, ncharge, form, nstreams, num_sms, err, s);
+        enqueue_chunk(hosts, d_inst, F, nf, nb, coords, npos, ncharge, sliced, nstreams, num_sms, err, s);
     } catch (...) {
         cudaStreamEndCapture(s, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -518,23 +518,30 @@ void nuclear_batch_device(const double* h_coeffs, i64 nb, const std::vector<Nucl
     for (size_t c = 0; c < chunks.size(); ++c) {
         const std::vector<NucHost> part(hosts.begin() + chunks[c].first, hosts.begin() + chunks[c].second);
         const NucInst* dptr = d_inst.p + chunks[c].first;
-        // streams for the per-instance contractions: chosen by timing the first
-        // chunk of a batch of this shape (cached per shape key)
+        // streams for the per-instance contractions and, in the mixed form, the
+        // contraction path: chosen by timing the first chunk of a batch of this
+        // shape (cached per shape key).  Candidate c: c % 16 streams, c >= 16
+        // the int8-sliced tensor-core contractions (mixed form only; they pay
+        // only where the GEMMs are large enough to carry the slicing passes)
         char key[160];
         snprintf(key, sizeof(key), "nuclear form=%d dev=%d inst=%zu maxN=%lld", form, ctx.device, part.size(),
                  (long long)std::max_element(part.begin(), part.end(), [](const NucHost& a, const NucHost& b) {
                      return a.d.N < b.d.N;
                  })->d.N);
-        auto run = [&](int nstreams) {
+        auto run = [&](int cand) {
+            const bool sliced = cand >= 16;
+            const int nstreams = cand % 16;
             if (graphs)
-                run_chunk_graph(part, dptr, F.p, nf, (int)nb, d_coords.p, d_npos.p, d_nq.p, form, nstreams,
+                run_chunk_graph(part, dptr, F.p, nf, (int)nb, d_coords.p, d_npos.p, d_nq.p, sliced, nstreams,
                                 ctx.num_sms, err.p, s);
             else
-                enqueue_chunk(part, dptr, F.p, nf, (int)nb, d_coords.p, d_npos.p, d_nq.p, form, nstreams, ctx.num_sms,
-                              err.p, s);
+                enqueue_chunk(part, dptr, F.p, nf, (int)nb, d_coords.p, d_npos.p, d_nq.p, sliced, nstreams,
+                              ctx.num_sms, err.p, s);
         };
-        const std::vector<int> cands = part.size() == 1 ? std::vector<int>{1} : std::vector<int>{1, 2, 4, 8};
-        const int nstreams = autotune().choose(key, cands, [&](int cand) {
+        std::vector<int> cands = part.size() == 1 ? std::vector<int>{1} : std::vector<int>{1, 2, 4, 8};
+        if (form == FORM_MIXED)
+            for (size_t k = 0, n0 = cands.size(); k < n0; ++k) cands.push_back(16 + cands[k]);
+        const int choice = autotune().choose(key, cands, [&](int cand) {
             cudaEvent_t e0, e1;
             GLI_CUDA(cudaEventCreate(&e0));
             GLI_CUDA(cudaEventCreate(&e1));
@@ -548,8 +555,8 @@ void nuclear_batch_device(const double* h_coeffs, i64 nb, const std::vector<Nucl
             cudaEventDestroy(e1);
             return (double)ms;
         });
-        stats.streams = nstreams;
-        run(nstreams);
+        stats.streams = choice % 16;
+        run(choice);
         stats.chunks += 1;
     }
     int h_err = 0;

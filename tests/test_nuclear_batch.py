@@ -52,14 +52,26 @@ def test_batch_small_instances_against_oracle(gli):
         assert_parity(outs[k], ref, what=f"batch instance {k} vs oracle")
 
 
-def test_batch_mixed_against_fp64(gli):
+@pytest.mark.parametrize("choice", ["17", "1", None])
+def test_batch_mixed_against_fp64(gli, choice, monkeypatch):
+    # the mixed form's contraction path is the autotuner's choice; "17" forces
+    # the int8-sliced tensor-core contractions (one stream), "1" the FP64 ones,
+    # None leaves the choice to the measurement
+    if choice is not None:
+        monkeypatch.setenv("GLI_B200_TUNE_NUCLEAR", choice)
     grids, pos, q = h_chain_batch(np.random.default_rng(11), 8, 4, 12, 0.5)
     fp = gli.compute_nuclear_gausslet_integrals_batch(g10(), grids, pos, q, TOL)
     mx = gli.compute_nuclear_gausslet_integrals_batch(g10(), grids, pos, q, TOL, form="mixed")
+    worst = 0.0
     for k in range(len(grids)):
         err = np.max(np.abs(mx[k] - fp[k]))
         assert np.all(np.isfinite(mx[k]))
         assert err <= 5e-9, f"instance {k}: max abs err {err:.3e}"
+        worst = max(worst, err)
+    if choice == "17":
+        assert worst > 0  # the sliced products did run
+    if choice == "1":
+        assert worst == 0  # the FP64 contractions, as in the FP64 form
 
 
 def test_batch_autotuner_decision(gli):
