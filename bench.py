@@ -534,8 +534,9 @@ def run_nuclear_batch(args):
 
 def run_surrogate(args):
     """Config: ERIDA 128^3 (odd stand-in 129^3) at 0.3 bohr with the far-field
-    surrogate: train on exact classes, evaluate with a 1% seeded audit at
-    1e-6 Ha, compare with the exact evaluation."""
+    surrogate: train on exact classes, evaluate with a 1% seeded audit against
+    the 1e-6 Ha target (shells redone above half of it), compare with the exact
+    evaluation."""
     import gausslectronitegrate_b200 as gli
     from gausslectronitegrate_b200 import _abi
     L = gli.lib()
@@ -552,7 +553,9 @@ def run_surrogate(args):
     gs = gli._grid_struct(grid)
     ex = gli.compute_sparse_erida_gausslet_integrals(g10(), grid, TOL)
     idx = ex.indices
-    shell_tol = 1e-6 * 0.3
+    # audit threshold at half the 1e-6 Ha target: an audited shell whose sample
+    # errs by more is evaluated exactly, so that its unaudited classes keep a margin
+    shell_tol = 0.5e-6 * 0.3
     vals = np.empty(idx.size)
     rep = np.zeros((256, 4))
     exact_ms, sur_ms = [], []

@@ -194,18 +194,27 @@ __global__ void k_erida_disp(GridDesc g, const int64_t* __restrict__ idx, i64 m,
     disp[3 * n + 2] = d[2];
 }
 
+// slot of a sorted displacement a >= b >= c in a dense (R+1)^3 table
+__host__ __device__ inline int disp_slot(int a, int b, int c, int R) { return (a * (R + 1) + b) * (R + 1) + c; }
+
 // predicted values of classes: 1/r + s(r) MLP (r_cut < r <= r_mlp) or 1/r (r > r_mlp);
-// classes with r <= r_cut get NaN (they are evaluated exactly)
+// classes with r <= r_cut get NaN (they are evaluated exactly).  shell[n]:
+// floor(r) beyond r_cut, -1 within it.
 __global__ void k_surrogate_values(const float* __restrict__ P, const int* __restrict__ disp, i64 m, double c0,
-                                   double c1, double c2, double r_cut, double r_mlp, double* __restrict__ out) {
+                                   double c1, double c2, double r_cut, double r_mlp, const uint8_t* __restrict__ known,
+                                   int R, double* __restrict__ out, int* __restrict__ shell) {
     const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m) return;
-    const double a = disp[3 * n], b = disp[3 * n + 1], c = disp[3 * n + 2];
+    const int ia = disp[3 * n], ib = disp[3 * n + 1], ic = disp[3 * n + 2];
+    const double a = ia, b = ib, c = ic;
     const double r = sqrt(a * a + b * b + c * c);
-    if (r <= r_cut) {
+    // within r_cut, or a displacement the network is known to miss: exact
+    if (r <= r_cut || (known && r <= r_mlp && ia <= R && known[disp_slot(ia, ib, ic, R)])) {
         out[n] = nan("");
+        shell[n] = -1;
         return;
     }
+    shell[n] = (int)floor(r);
     double v = 1.0 / r;
     if (r <= r_mlp) {
         float f[MLP_IN], h[MLP_ACT];
@@ -225,6 +234,11 @@ struct Surrogate {
     // training report
     i64 samples = 0, holdout = 0;
     double loss = 0, max_dz_train = 0, max_dz_holdout = 0, max_res_err_train = 0, max_res_err_holdout = 0;
+    // |prediction - exact| of every displacement of the network's range (the
+    // training and the hold-out ones: their exact values are known), indexed
+    // by disp_slot(a, b, c) with a >= b >= c, dense over a <= R = ceil(r_mlp)
+    int R = 0;
+    std::vector<float> fit_err;
 };
 
 // One optimisation run: full-batch Adam over `steps` steps, each step a CUDA
@@ -458,6 +472,18 @@ Surrogate* surrogate_train(const double* coeffs, i64 nb, double tol, double r_ml
         sur->max_dz_holdout = std::max(sur->max_dz_holdout, fabs((double)yh[k] - T[q]));
         sur->max_res_err_holdout = std::max(sur->max_res_err_holdout, fabs((double)yh[k] * env[q] - res[q]));
     }
+    sur->R = R;
+    sur->fit_err.assign((size_t)(R + 1) * (R + 1) * (R + 1), 0.f);
+    for (size_t k = 0; k < train.size(); ++k) {
+        const i64 q = train[k];
+        sur->fit_err[disp_slot(std::get<0>(disp[q]), std::get<1>(disp[q]), std::get<2>(disp[q]), R)] =
+            (float)fabs((double)yt[k] * env[q] - res[q]);
+    }
+    for (size_t k = 0; k < hold.size(); ++k) {
+        const i64 q = hold[k];
+        sur->fit_err[disp_slot(std::get<0>(disp[q]), std::get<1>(disp[q]), std::get<2>(disp[q]), R)] =
+            (float)fabs((double)yh[k] * env[q] - res[q]);
+    }
     sur->loss = wsum > 0 ? loss / wsum : 0;
     sur->samples = (i64)train.size();
     sur->holdout = nh;
@@ -476,76 +502,109 @@ void surrogate_erida_values(const Surrogate& sur, const double* coeffs, i64 nb, 
     if (!(audit_fraction >= 0 && audit_fraction <= 1)) fail(GLI_ERR_ARGUMENT, "audit fraction in [0, 1]");
     if (!(shell_tol >= 0)) fail(GLI_ERR_ARGUMENT, "shell tolerance must be non-negative");
     DevBuf<int64_t> di(m, s);
-    DevBuf<int> dd(3 * m, s);
+    DevBuf<int> dd(3 * m, s), dsh(m, s);
     DevBuf<double> dv(m, s);
     DevBuf<float> dP(MLP_PARAMS, s);
     GLI_CUDA(cudaMemcpyAsync(di.p, h_idx, m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     GLI_CUDA(cudaMemcpyAsync(dP.p, sur.params.data(), MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice, s));
     k_erida_disp<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(g, di.p, m, dd.p);
     GLI_CHECK_LAUNCH();
+    // displacements whose fit error (measured at training) exceeds shell_tol
+    // are evaluated exactly: the audit samples a shell, this covers the
+    // outliers it may miss
+    std::vector<uint8_t> known(sur.fit_err.size());
+    bool any = false;
+    for (size_t k = 0; k < known.size(); ++k) {
+        known[k] = sur.fit_err[k] > shell_tol ? 1 : 0;
+        any = any || known[k];
+    }
+    DevBuf<uint8_t> dknown(any ? known.size() : 0, s);
+    if (any)
+        GLI_CUDA(cudaMemcpyAsync(dknown.p, known.data(), known.size(), cudaMemcpyHostToDevice, s));
     k_surrogate_values<<<(unsigned)((m + 127) / 128), 128, 0, s>>>(dP.p, dd.p, m, sur.env[0], sur.env[1], sur.env[2],
-                                                                    sur.r_cut, sur.r_mlp, dv.p);
+                                                                    sur.r_cut, sur.r_mlp, any ? dknown.p : nullptr,
+                                                                    sur.R, dv.p, dsh.p);
     GLI_CHECK_LAUNCH();
-    std::vector<int> disp(3 * m);
+    std::vector<int> shell(m);
     GLI_CUDA(cudaMemcpyAsync(h_out, dv.p, m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GLI_CUDA(cudaMemcpyAsync(disp.data(), dd.p, 3 * m * sizeof(int), cudaMemcpyDeviceToHost, s));
+    GLI_CUDA(cudaMemcpyAsync(shell.data(), dsh.p, m * sizeof(int), cudaMemcpyDeviceToHost, s));
     GLI_CUDA(cudaStreamSynchronize(s));
-    // shells, near classes, seeded audit sample (a fraction of each far shell, at least 4 classes)
-    std::map<int, std::vector<i64>> shells;
+    // classes bucketed by shell (counting sort, class order kept within a shell)
+    int ns = 0;
+    for (i64 n = 0; n < m; ++n) ns = std::max(ns, shell[n] + 1);
+    std::vector<i64> first(ns + 1, 0);
     std::vector<i64> exact;
     for (i64 n = 0; n < m; ++n) {
-        const double a = disp[3 * n], b = disp[3 * n + 1], c = disp[3 * n + 2];
-        const double r = sqrt(a * a + b * b + c * c);
-        if (r <= sur.r_cut)
+        if (shell[n] < 0)
             exact.push_back(n);
         else
-            shells[(int)floor(r)].push_back(n);
+            ++first[shell[n] + 1];
     }
-    std::mt19937_64 rng(seed);
-    std::map<int, std::vector<i64>> audited;
-    for (auto& kv : shells) {
-        std::vector<i64> v = kv.second;
-        std::shuffle(v.begin(), v.end(), rng);
-        // audit_fraction 0: no audit (the prediction alone, for measurements)
-        const i64 k = audit_fraction > 0
-                          ? std::min<i64>((i64)v.size(), std::max<i64>(4, (i64)ceil(audit_fraction * v.size())))
-                          : 0;
-        audited[kv.first].assign(v.begin(), v.begin() + k);
-        exact.insert(exact.end(), v.begin(), v.begin() + k);
+    for (int k = 0; k < ns; ++k) first[k + 1] += first[k];
+    std::vector<i64> members(first[ns]);
+    {
+        std::vector<i64> fill(first.begin(), first.end() - 1);
+        for (i64 n = 0; n < m; ++n)
+            if (shell[n] >= 0) members[fill[shell[n]]++] = n;
+    }
+    // the audit sample of a shell: its k classes of smallest seeded hash of the
+    // class index (splitmix64 finaliser), k = audit_fraction of the shell, at
+    // least 4 (all of a smaller shell); audit_fraction 0: no audit (the
+    // prediction alone, for measurements).  The hash makes the sample a
+    // function of the seed and the class, not of the list order.
+    auto mix = [](uint64_t z) {
+        z += 0x9e3779b97f4a7c15ull;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return z ^ (z >> 31);
+    };
+    std::vector<i64> nsample(ns, 0);
+    std::vector<std::pair<uint64_t, i64>> keyed;
+    for (int k = 0; k < ns; ++k) {
+        const i64 cnt = first[k + 1] - first[k];
+        if (cnt == 0 || audit_fraction <= 0) continue;
+        const i64 want = std::min<i64>(cnt, std::max<i64>(4, (i64)ceil(audit_fraction * cnt)));
+        keyed.clear();
+        for (i64 q = first[k]; q < first[k + 1]; ++q)
+            keyed.push_back({mix(seed ^ (uint64_t)h_idx[members[q]]), members[q]});
+        if (want < cnt) std::nth_element(keyed.begin(), keyed.begin() + want, keyed.end());
+        for (i64 q = 0; q < want; ++q) exact.push_back(keyed[q].second);
+        nsample[k] = want;
     }
     std::vector<int64_t> eidx(exact.size());
     for (size_t k = 0; k < exact.size(); ++k) eidx[k] = h_idx[exact[k]];
     const std::vector<double> ev = exact_erida(coeffs, nb, g, eidx, tol, s);
-    std::vector<double> exact_val(m, nan(""));
-    for (size_t k = 0; k < exact.size(); ++k) exact_val[exact[k]] = ev[k];
-    // audit per shell; failing shells are evaluated exactly in full
+    // audit error per shell (the audited classes follow the near ones in `exact`)
+    std::vector<double> shell_err(ns, 0.0);
+    for (size_t k = 0; k < exact.size(); ++k) {
+        const i64 n = exact[k];
+        if (shell[n] >= 0) shell_err[shell[n]] = std::max(shell_err[shell[n]], fabs(h_out[n] - ev[k]));
+    }
+    for (size_t k = 0; k < exact.size(); ++k) h_out[exact[k]] = ev[k];
+    // shells whose audit exceeds the tolerance are evaluated exactly in full
+    std::vector<int64_t> ridx;
     std::vector<i64> redo;
-    std::map<int, double> shell_err;
-    for (auto& kv : audited) {
-        double e = 0;
-        for (i64 n : kv.second) e = std::max(e, fabs(h_out[n] - exact_val[n]));
-        shell_err[kv.first] = e;
-        if (!(e <= shell_tol))
-            for (i64 n : shells[kv.first])
-                if (std::isnan(exact_val[n])) redo.push_back(n);
+    for (int k = 0; k < ns; ++k) {
+        if (nsample[k] == 0 || shell_err[k] <= shell_tol) continue;
+        for (i64 q = first[k]; q < first[k + 1]; ++q) {
+            redo.push_back(members[q]);
+            ridx.push_back(h_idx[members[q]]);
+        }
     }
     if (!redo.empty()) {
-        std::vector<int64_t> ridx(redo.size());
-        for (size_t k = 0; k < redo.size(); ++k) ridx[k] = h_idx[redo[k]];
         const std::vector<double> rv = exact_erida(coeffs, nb, g, ridx, tol, s);
-        for (size_t k = 0; k < redo.size(); ++k) exact_val[redo[k]] = rv[k];
+        for (size_t k = 0; k < redo.size(); ++k) h_out[redo[k]] = rv[k];
     }
-    for (i64 n = 0; n < m; ++n)
-        if (!std::isnan(exact_val[n])) h_out[n] = exact_val[n];
     if (report && max_shells > 0) {
         for (i64 k = 0; k < 4 * max_shells; ++k) report[k] = 0;
-        for (auto& kv : shells) {
-            if (kv.first >= max_shells) continue;
-            double* rp = report + 4 * kv.first;
-            rp[0] = (double)kv.second.size();
-            rp[1] = (double)audited[kv.first].size();
-            rp[2] = shell_err[kv.first];
-            rp[3] = shell_err[kv.first] <= shell_tol ? 0.0 : 1.0;
+        for (int k = 0; k < ns && k < max_shells; ++k) {
+            const i64 cnt = first[k + 1] - first[k];
+            if (cnt == 0) continue;
+            double* rp = report + 4 * k;
+            rp[0] = (double)cnt;
+            rp[1] = (double)nsample[k];
+            rp[2] = shell_err[k];
+            rp[3] = nsample[k] > 0 && !(shell_err[k] <= shell_tol) ? 1.0 : 0.0;
         }
     }
 }

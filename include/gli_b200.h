@@ -339,9 +339,11 @@ int gli_b200_surrogate_info(const gli_b200_surrogate* s, double info[13]);
 glong gli_b200_surrogate_params(const gli_b200_surrogate* s, float* params, glong n);
 
 /* ERIDA values of a class list (host arrays) from the surrogate with a seeded
- * audit: every class with r <= 6 and an audit sample of each radial shell
- * (floor r; audit_fraction of its classes, at least 4; none when
- * audit_fraction is 0) are evaluated exactly;
+ * audit: every class with r <= 6, every class whose displacement the network
+ * missed by more than shell_tol at training (its error there is known), and
+ * an audit sample of each radial shell (floor r; audit_fraction of its
+ * classes, at least 4, those of smallest seeded hash of the class index; none
+ * when audit_fraction is 0) are evaluated exactly;
  * a shell whose largest audit error exceeds shell_tol (grid units) is
  * evaluated exactly in full.  report (optional, max_shells x 4): per shell
  * classes, audited classes, max audit error, evaluated in full (1/0). */
