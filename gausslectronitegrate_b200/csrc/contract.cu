@@ -662,21 +662,38 @@ struct ProductOp {
 };
 
 // val[n] = Q[pair(n)][kid(k3)], the class's (pair, key) found from its packed keys
-__global__ void k_gather_q(const double* __restrict__ Q, const uint64_t* __restrict__ keys, i64 m,
-                           const uint64_t* __restrict__ kid, int nk, const uint32_t* __restrict__ pairBits,
-                           const uint64_t* __restrict__ pairPre, int ldq, const PlanCounts* __restrict__ cnt,
-                           int choice, double* __restrict__ out) {
-    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m || !choice_runs(choice, cnt, m)) return;
-    const uint64_t p = keys[n];
-    if (p == BAD_KEYS) {
-        out[n] = 0.0;
-        return;
+__global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, const uint64_t* __restrict__ keys,
+                                                   i64 m, const uint64_t* __restrict__ kid, int nk,
+                                                   const uint32_t* __restrict__ pairBits,
+                                                   const uint64_t* __restrict__ pairPre, int ldq,
+                                                   const PlanCounts* __restrict__ cnt, int choice,
+                                                   double* __restrict__ out) {
+    if (!choice_runs(choice, cnt, m)) return;
+    // four classes per thread and step: each class is a chain of three
+    // dependent loads (keys, then pair id and key id, then Q); the four chains
+    // run side by side
+    constexpr int V = 4;
+    const i64 step = (i64)gridDim.x * blockDim.x;
+    for (i64 n0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; n0 < m; n0 += V * step) {
+        uint64_t p[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) p[v] = n0 + v * step < m ? keys[n0 + v * step] : BAD_KEYS;
+        i64 q[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            q[v] = -1;
+            if (p[v] != BAD_KEYS) {
+                int k[3];
+                unpack_keys(p[v], k);
+                q[v] = pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]) * ldq + (i64)kid[k[2]];
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const i64 n = n0 + v * step;
+            if (n < m) out[n] = q[v] >= 0 ? Q[q[v]] : 0.0;
+        }
     }
-    int k[3];
-    unpack_keys(p, k);
-    const i64 pair = pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]);
-    out[n] = Q[pair * ldq + (i64)kid[k[2]]];
 }
 
 // ---------------------------------------------------------------------------
@@ -1116,7 +1133,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             dmma_launch(ProductOp<80>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
         else
             dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
-        k_gather_q<<<cb, 256, 0, s>>>(Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
+        const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
+        k_gather_q<<<gq, 256, 0, s>>>(Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
                                       a.out);
         GLI_CHECK_LAUNCH();
     }
