@@ -100,7 +100,7 @@ __device__ inline double nuc_field_at(const NucInst& in, const double* __restric
         // rounds to 1 and g = 1 / r
         double g;
         if (r2 >= 4.0) {
-            g = 1.0 / sqrt(r2);
+            g = rsqrt(r2);
         } else {
             const double r = sqrt(r2);
             g = r > 0 ? erf(3.0 * r) / r : 3.3851375012865379;  // 6 / sqrt(pi)
@@ -124,21 +124,35 @@ __global__ void __launch_bounds__(128) k_nuc_field(const NucInst* __restrict__ i
     }
 }
 
+// q = j / d for 0 <= j < 2^24, d >= 1: the single-precision estimate j * (1/d)
+// is within one of the quotient, and one correction step lands on it
+__device__ __forceinline__ int div_small(int j, int d, float inv) {
+    int q = __float2int_rz((float)j * inv);
+    const int r = j - q * d;
+    if (r < 0)
+        --q;
+    else if (r >= d)
+        ++q;
+    return q;
+}
+
 // V[i][j] of every instance from its key-indexed block Vk[kx][kz * nky + ky];
-// grid (row blocks, instance): a block writes whole rows i (coalesced), and
-// the coordinates of j come from two 32-bit divisions per element (every
-// instance has at most 256^3 points)
+// grid (row blocks, instance): a block writes whole rows i (coalesced).  The
+// coordinates of j come from two estimated divisions per element (every
+// instance has at most 256^3 = 2^24 points); the kernel writes 8 bytes per
+// element and is bound by its instructions, so they count.
 __global__ void __launch_bounds__(256) k_nuc_scatter(const NucInst* __restrict__ inst, const double* __restrict__ Vk) {
     const NucInst& in = inst[blockIdx.y];
     const int ny = in.n[1], nz = in.n[2], nky = in.nk[1], nkz = in.nk[2];
     const int N = (int)in.N, nyz = ny * nz;
+    const float inv_nyz = 1.0f / (float)nyz, inv_nz = 1.0f / (float)nz;
     const double* vk = Vk + in.vk_off;
     for (int i = blockIdx.x; i < N; i += gridDim.x) {
         const int iz = i % nz, iy = (i / nz) % ny, ix = i / nyz;
         double* row = in.out + (i64)i * N;
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            const int jx = j / nyz, t = j - jx * nyz;
-            const int jy = t / nz, jz = t - jy * nz;
+            const int jx = div_small(j, nyz, inv_nyz), t = j - jx * nyz;
+            const int jy = div_small(t, nz, inv_nz), jz = t - jy * nz;
             const int ax = min(ix, jx), bx = max(ix, jx), ay = min(iy, jy), by = max(iy, jy);
             const int az = min(iz, jz), bz = max(iz, jz);
             const i64 kx = bx * (bx + 1) / 2 + ax;
