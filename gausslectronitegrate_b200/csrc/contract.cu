@@ -87,6 +87,8 @@ __device__ inline void decode_pt(const ClassDecode& d, uint32_t lin, int p[3]) {
 
 // coordinates of every grid point (ERI decoding)
 __global__ void k_point_table(ClassDecode d, short4* __restrict__ pt) {
+    pdl_wait();
+    pdl_release();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n32) return;
     int p[3];
@@ -153,6 +155,8 @@ struct PlanCounts {
 __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
                                               uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
                                               uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
+    pdl_wait();
+    pdl_release();
     extern __shared__ uint32_t sflag[];
     const int nk = (int)d.nkeys;
     const int words = (nk * nk + 31) >> 5;
@@ -221,6 +225,8 @@ static size_t mark_local_bytes(i64 nk) {
 __global__ void k_plan_keys(i64 nk, const uint32_t* __restrict__ used, const uint64_t* __restrict__ ids,
                             int* __restrict__ keyOf, int* __restrict__ aId, int* __restrict__ aKey,
                             PlanCounts* __restrict__ cnt) {
+    pdl_wait();
+    pdl_release();
     const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nku = ids[nk];  // exclusive scan at nk = number of used keys
     if (k == 0) {
@@ -267,6 +273,8 @@ __global__ void __launch_bounds__(1024) k_plan_keys_small(i64 nk, const uint32_t
                                                           uint64_t* __restrict__ ids, int* __restrict__ keyOf,
                                                           int* __restrict__ aId, int* __restrict__ aKey,
                                                           PlanCounts* __restrict__ cnt) {
+    pdl_wait();
+    pdl_release();
     __shared__ uint32_t ws[32], total, nku_s;
     const int k = threadIdx.x;  // flag k of 2 nk (<= 512)
     const uint32_t f = k < 2 * nk ? used[k] : 0u;
@@ -295,6 +303,8 @@ __global__ void __launch_bounds__(1024) k_pairs_small(i64 words, int nk, const u
                                                       const int* __restrict__ aId, uint64_t* __restrict__ pre,
                                                       int* __restrict__ pairA, int* __restrict__ pairB,
                                                       PlanCounts* __restrict__ cnt) {
+    pdl_wait();
+    pdl_release();
     __shared__ uint32_t ws[32], total;
     uint32_t carry = 0;
     for (i64 base = 0; base < words; base += 1024) {
@@ -318,12 +328,16 @@ __global__ void __launch_bounds__(1024) k_pairs_small(i64 words, int nk, const u
 
 // set bits per word of the pair bitmap (the exclusive scan of which gives pre)
 __global__ void k_word_counts(i64 words, const uint32_t* __restrict__ bits, uint32_t* __restrict__ counts) {
+    pdl_wait();
+    pdl_release();
     const i64 w = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (w < words) counts[w] = __popc(bits[w]);
 }
 
 __global__ void k_pair_lists(i64 words, int nk, const uint32_t* __restrict__ bits, const uint64_t* __restrict__ pre,
                              const int* __restrict__ aId, int* __restrict__ pairA, int* __restrict__ pairB) {
+    pdl_wait();
+    pdl_release();
     const i64 w = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= words) return;
     uint32_t b = bits[w];
@@ -514,6 +528,8 @@ struct StageBOp {
 
 // out[i] = sum_p parts[p n + i], in order of p (deterministic)
 __global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, double* __restrict__ out) {
+    pdl_wait();
+    pdl_release();
     for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
         double acc = parts[i];
         for (int p = 1; p < P; ++p) acc += parts[(i64)p * n + i];
@@ -571,6 +587,8 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
                                                   const uint64_t* __restrict__ pairPre, i64 m, int U, int Up,
                                                   const PlanCounts* __restrict__ cnt, int choice,
                                                   double* __restrict__ out) {
+    pdl_wait();
+    pdl_release();
     if (!choice_runs(choice, cnt, m)) return;
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
@@ -668,6 +686,8 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
                                                    const uint64_t* __restrict__ pairPre, int ldq,
                                                    const PlanCounts* __restrict__ cnt, int choice,
                                                    double* __restrict__ out) {
+    pdl_wait();
+    pdl_release();
     if (!choice_runs(choice, cnt, m)) return;
     // four classes per thread and step: each class is a chain of three
     // dependent loads (keys, then pair id and key id, then Q); the four chains
@@ -778,6 +798,8 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
                                                       int bn, int max_tiles, int* __restrict__ first,
                                                       int* __restrict__ tile0, int* __restrict__ tile_batch,
                                                       int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
+    pdl_wait();
+    pdl_release();
     __shared__ int warp_sums[32];
     __shared__ int carry;
     const int nP = (int)cnt->nP, nA = (int)cnt->nA;
@@ -944,8 +966,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     ClassDecode dec = a.d;
     if (dec.kind == 1) {
         pts.alloc(dec.N, s);
-        k_point_table<<<(unsigned)((dec.N + 255) / 256), 256, 0, s>>>(dec, pts.p);
-        GLI_CHECK_LAUNCH();
+        launch_pdl(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
         dec.pt = pts.p;
     }
     // packed key triple per class
@@ -953,26 +974,22 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     {
         const size_t lb = mark_local_bytes(nk);
         const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-        k_mark<<<mb, 256, lb, s>>>(dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad, lb ? 1 : 0);
-        GLI_CHECK_LAUNCH();
+        launch_pdl(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad, lb ? 1 : 0);
     }
     DevBuf<uint64_t> ids(2 * nk, s);
     DevBuf<int> keyOf(nk, s), aId(nk, s), aKey(nk, s);
     if (2 * nk <= 1024) {
-        k_plan_keys_small<<<1, 1024, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
-        GLI_CHECK_LAUNCH();
+        launch_pdl(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
     } else {
         exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
-        k_plan_keys<<<kb, 256, 0, s>>>(nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
-        GLI_CHECK_LAUNCH();
+        launch_pdl(k_plan_keys, dim3(kb), dim3(256), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
     }
     DevBuf<uint64_t> pairPre(words, s);
     const bool small_pairs = bounded && words <= 8 * 1024;
     DevBuf<uint32_t> counts;
     if (!small_pairs) {
         counts.alloc(words, s);
-        k_word_counts<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(words, pairBits.p, counts.p);
-        GLI_CHECK_LAUNCH();
+        launch_pdl(k_word_counts, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, pairBits.p, counts.p);
         exclusive_scan_u32_dev(counts.p, pairPre.p, words, &cnt->nP, s);
     }
     if (bounded) {
@@ -990,11 +1007,10 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     }
     DevBuf<int> pairA(sz.nP, s), pairB(sz.nP, s);
     if (small_pairs)
-        k_pairs_small<<<1, 1024, 0, s>>>(words, (int)nk, pairBits.p, aId.p, pairPre.p, pairA.p, pairB.p, cnt);
+        launch_pdl(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p, pairA.p, pairB.p, cnt);
     else
-        k_pair_lists<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(words, (int)nk, pairBits.p, pairPre.p, aId.p,
+        launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk, pairBits.p, pairPre.p, aId.p,
                                                                       pairA.p, pairB.p);
-    GLI_CHECK_LAUNCH();
 
     const i64 nA = sz.nA, nP = sz.nP, nku = sz.nku;
     if (nA * (i64)U * U > ((i64)1 << 31))
@@ -1047,9 +1063,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             dmma_launch(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
                         dim3(mb, nb, (unsigned)P), s);
         if (P > 1) {
-            k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
+            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0, s, parts.p, P, ps,
                                                                                                       H.p);
-            GLI_CHECK_LAUNCH();
         }
     }
     timer.mark();
@@ -1068,9 +1083,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         int* tile_batch = grp.p + 2 * nA;
         int* tile_col0 = tile_batch + max_tiles;
         int* tile_ncols = tile_col0 + max_tiles;
-        k_pair_tiles<<<1, 1024, 0, s>>>(pairA.p, cnt, BN, (int)max_tiles, first, tile0, tile_batch, tile_col0,
+        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, BN, (int)max_tiles, first, tile0, tile_batch, tile_col0,
                                         tile_ncols);
-        GLI_CHECK_LAUNCH();
         Wb.alloc(max_tiles, BN, U, MIXED_SLICES, s);
         slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, tile_col0, tile_ncols, cnt, Up, BN}, nP, U, Wb,
                     s);
@@ -1092,9 +1106,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         int* tile_batch = grp.p + 2 * nA;
         int* tile_col0 = tile_batch + max_tiles;
         int* tile_ncols = tile_col0 + max_tiles;
-        k_pair_tiles<<<1, 1024, 0, s>>>(pairA.p, cnt, DM_BM, (int)max_tiles, grp.p, grp.p + nA, tile_batch,
+        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, DM_BM, (int)max_tiles, grp.p, grp.p + nA, tile_batch,
                                         tile_col0, tile_ncols);
-        GLI_CHECK_LAUNCH();
         // the tile count is known on the device only: the split follows its bound
         const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
@@ -1110,9 +1123,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
                              dst},
                     dim3((unsigned)max_tiles, ub, (unsigned)P), s);
         if (P > 1) {
-            k_sum_parts<<<(unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16), 256, 0, s>>>(parts.p, P, ps,
+            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0, s, parts.p, P, ps,
                                                                                                       H2.p);
-            GLI_CHECK_LAUNCH();
         }
     }
     timer.mark();
@@ -1134,16 +1146,14 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         else
             dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
         const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-        k_gather_q<<<gq, 256, 0, s>>>(Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
+        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
                                       a.out);
-        GLI_CHECK_LAUNCH();
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
-        k_stage_c<<<gc, 256, 0, s>>>(t.W.p, H2.p, keys.p, (int)nk, pairBits.p, pairPre.p, m, U, Up, cnt, c_class,
+        launch_pdl(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, (int)nk, pairBits.p, pairPre.p, m, U, Up, cnt, c_class,
                                      a.out);
-        GLI_CHECK_LAUNCH();
     }
     timer.mark();
 }

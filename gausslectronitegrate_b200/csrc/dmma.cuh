@@ -135,6 +135,8 @@ __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
     constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN);
     static_assert(Op::BN == 64 || (Op::BN == 80 && !Op::B_KMAJOR), "column tiles of 64, or 80 read row-major");
     extern __shared__ __align__(16) double dm_smem[];
+    pdl_wait();  // the previous kernel's results are visible from here
+    pdl_release();
     typename Op::Block blk;
     if (!op.begin(blk)) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -192,8 +194,7 @@ template <class Op>
 void dmma_launch(const Op& op, dim3 grid, cudaStream_t s) {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
     dmma_prepare<Op>();
-    k_dmma<Op><<<grid, DM_THREADS, dm_smem(Op::BN), s>>>(op);
-    GLI_CHECK_LAUNCH();
+    launch_pdl(k_dmma<Op>, grid, dim3(DM_THREADS), dm_smem(Op::BN), s, op);
 }
 
 }  // namespace gli

@@ -11,11 +11,12 @@
 //   Phi[u][v][t] = sum_k Z_k g(|(u,v,t)/6 + origin - R_k|),
 // and the separable weights are contracted against it axis by axis:
 //   A   H[kz][u][v]     = sum_t Wz[kz][t] Phi[u][v][t]      (GEMM)
-//   B   H2[kz][ky][u]   = sum_v Wy[ky][v] H[kz][u][v]       (batched GEMM)
-//   C   Vk[kx][kz,ky]   = sum_u Wx[kx][u] H2[kz][ky][u]     (GEMM)
+//   B   H2[ky][kz][u]   = sum_v Wy[ky][v] H[kz][u][v]       (batched GEMM)
+//   C   Vk[kx][ky,kz]   = sum_u Wx[kx][u] H2[ky][kz][u]     (GEMM)
 // where an axis key is the unordered coordinate pair {i_a, j_a} (the factor
 // depends on |i_a - j_a|, the position on i_a + j_a).  A final scatter writes
-// the dense N x N matrix, V_ij = Vk[kx(i,j)][kz(i,j), ky(i,j)].
+// the dense N x N matrix, V_ij = Vk[kx(i,j)][ky(i,j), kz(i,j)] (the sliced
+// tensor-core contractions keep the (kz, ky) order of their batched stage B).
 //
 // Batches.  Any number of instances (each its own grid and nuclei, all with
 // the same coefficients and tol) run as one plan: one upload of every
@@ -136,12 +137,14 @@ __device__ __forceinline__ int div_small(int j, int d, float inv) {
     return q;
 }
 
-// V[i][j] of every instance from its key-indexed block Vk[kx][kz * nky + ky];
+// V[i][j] of every instance from its key-indexed block: Vk[kx][ky * nkz + kz]
+// (zfast: the FP64 contractions) or Vk[kx][kz * nky + ky] (the sliced ones);
 // grid (row blocks, instance): a block writes whole rows i (coalesced).  The
 // coordinates of j come from two estimated divisions per element (every
 // instance has at most 256^3 = 2^24 points); the kernel writes 8 bytes per
 // element and is bound by its instructions, so they count.
-__global__ void __launch_bounds__(256) k_nuc_scatter(const NucInst* __restrict__ inst, const double* __restrict__ Vk) {
+__global__ void __launch_bounds__(256) k_nuc_scatter(const NucInst* __restrict__ inst, const double* __restrict__ Vk,
+                                                     int zfast) {
     const NucInst& in = inst[blockIdx.y];
     const int ny = in.n[1], nz = in.n[2], nky = in.nk[1], nkz = in.nk[2];
     const int N = (int)in.N, nyz = ny * nz;
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(256) k_nuc_scatter(const NucInst* __restrict__
             const int az = min(iz, jz), bz = max(iz, jz);
             const i64 kx = bx * (bx + 1) / 2 + ax;
             const int ky = by * (by + 1) / 2 + ay, kz = bz * (bz + 1) / 2 + az;
-            row[j] = vk[kx * ((i64)nkz * nky) + kz * nky + ky];
+            row[j] = vk[kx * ((i64)nkz * nky) + (zfast ? ky * nkz + kz : kz * nky + ky)];
         }
     }
 }
@@ -201,8 +204,8 @@ struct NucHost {
     NucInst d;
 };
 
-// A: H[kz][(u v)] = sum_t Wz[kz][t] Phi[(u v)][t];  B: H2[kz][ky][u] = sum_v Wy[ky][v] H[kz][u][v];
-// C: Vk[kx][(kz ky)] = sum_u Wx[kx][u] H2[(kz ky)][u]
+// A: H[kz][(u v)] = sum_t Wz[kz][t] Phi[(u v)][t];  B: H2[ky][kz][u] = sum_v Wy[ky][v] H[kz][u][v];
+// C: Vk[kx][(ky kz)] = sum_u Wx[kx][u] H2[(ky kz)][u]
 static void nuc_contract_fp64(const NucInst& in, const double* W, const double* Phi, double* Vk, cudaStream_t s) {
     const int* U = in.U;
     const int* nk = in.nk;
@@ -213,7 +216,9 @@ static void nuc_contract_fp64(const NucInst& in, const double* W, const double* 
     DevBuf<double> H((i64)nk[2] * UxUy, s), H2(nzy * U[0], s);
     dgemm_strided(nk[2], (int)UxUy, U[2], Wz, 0, U[2], 1, Phi + in.phi_off, 0, 1, U[2], H.p, 0, UxUy, 1, 1, false,
                   s);
-    dgemm_strided(nk[1], U[0], U[1], Wy, 0, U[1], 1, H.p, UxUy, 1, U[1], H2.p, (i64)nk[1] * U[0], U[0], 1, nk[2],
+    // H2 rows ordered (ky, kz): Vk comes out as [kx][ky][kz], kz innermost (the
+    // scatter's fastest-varying key along a matrix row)
+    dgemm_strided(nk[1], U[0], U[1], Wy, 0, U[1], 1, H.p, UxUy, 1, U[1], H2.p, U[0], (i64)nk[2] * U[0], 1, nk[2],
                   false, s);
     dgemm_strided(nk[0], (int)nzy, U[0], Wx, 0, U[0], 1, H2.p, 0, 1, U[0], Vk + in.vk_off, 0, nzy, 1, 1, false, s);
 }
@@ -373,7 +378,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
     }
     // rows per instance: enough blocks for every SM even when few instances are large
     const unsigned sb = (unsigned)std::min<i64>(max_n, std::max<i64>(1, (i64)num_sms * 16));
-    k_nuc_scatter<<<dim3(sb, (unsigned)ni), 256, 0, s>>>(d_inst, Vk.p);
+    k_nuc_scatter<<<dim3(sb, (unsigned)ni), 256, 0, s>>>(d_inst, Vk.p, sliced ? 0 : 1);
     GLI_CHECK_LAUNCH();
 }
 
