@@ -1007,10 +1007,11 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     }
     DevBuf<int> pairA(sz.nP, s), pairB(sz.nP, s);
     if (small_pairs)
-        launch_pdl(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p, pairA.p, pairB.p, cnt);
+        launch_pdl(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p, pairA.p,
+                   pairB.p, cnt);
     else
-        launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk, pairBits.p, pairPre.p, aId.p,
-                                                                      pairA.p, pairB.p);
+        launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk, pairBits.p,
+                   pairPre.p, aId.p, pairA.p, pairB.p);
 
     const i64 nA = sz.nA, nP = sz.nP, nku = sz.nku;
     if (nA * (i64)U * U > ((i64)1 << 31))
@@ -1063,8 +1064,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             dmma_launch(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
                         dim3(mb, nb, (unsigned)P), s);
         if (P > 1) {
-            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0, s, parts.p, P, ps,
-                                                                                                      H.p);
+            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
+                       s, parts.p, P, ps, H.p);
         }
     }
     timer.mark();
@@ -1083,8 +1084,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         int* tile_batch = grp.p + 2 * nA;
         int* tile_col0 = tile_batch + max_tiles;
         int* tile_ncols = tile_col0 + max_tiles;
-        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, BN, (int)max_tiles, first, tile0, tile_batch, tile_col0,
-                                        tile_ncols);
+        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, BN, (int)max_tiles, first, tile0, tile_batch,
+                   tile_col0, tile_ncols);
         Wb.alloc(max_tiles, BN, U, MIXED_SLICES, s);
         slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, tile_col0, tile_ncols, cnt, Up, BN}, nP, U, Wb,
                     s);
@@ -1106,8 +1107,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         int* tile_batch = grp.p + 2 * nA;
         int* tile_col0 = tile_batch + max_tiles;
         int* tile_ncols = tile_col0 + max_tiles;
-        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, DM_BM, (int)max_tiles, grp.p, grp.p + nA, tile_batch,
-                                        tile_col0, tile_ncols);
+        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, DM_BM, (int)max_tiles, grp.p, grp.p + nA,
+                   tile_batch, tile_col0, tile_ncols);
         // the tile count is known on the device only: the split follows its bound
         const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
@@ -1123,8 +1124,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
                              dst},
                     dim3((unsigned)max_tiles, ub, (unsigned)P), s);
         if (P > 1) {
-            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0, s, parts.p, P, ps,
-                                                                                                      H2.p);
+            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
+                       s, parts.p, P, ps, H2.p);
         }
     }
     timer.mark();
@@ -1146,14 +1147,14 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         else
             dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
         const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p, (int)nku, cnt, c_prod,
-                                      a.out);
+        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p,
+                   (int)nku, cnt, c_prod, a.out);
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
-        launch_pdl(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, (int)nk, pairBits.p, pairPre.p, m, U, Up, cnt, c_class,
-                                     a.out);
+        launch_pdl(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, (int)nk, pairBits.p, pairPre.p, m, U, Up,
+                   cnt, c_class, a.out);
     }
     timer.mark();
 }
