@@ -794,15 +794,11 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
 // One block: first pair, pair count and first tile of every A key (pairs are
 // ordered by A key), and the tile list of stage B (tiles of bn pairs, each in
 // one A key); tiles past the last one get no columns.
-__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, const PlanCounts* __restrict__ cnt,
-                                                      int bn, int max_tiles, int* __restrict__ first,
-                                                      int* __restrict__ tile0, int* __restrict__ tile_batch,
-                                                      int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
-    pdl_wait();
-    pdl_release();
+__device__ void pair_tiles_block(const int* __restrict__ pairA, int nP, int nA, int bn, int max_tiles,
+                                 int* __restrict__ first, int* __restrict__ tile0, int* __restrict__ tile_batch,
+                                 int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
     __shared__ int warp_sums[32];
     __shared__ int carry;
-    const int nP = (int)cnt->nP, nA = (int)cnt->nA;
     if (threadIdx.x == 0) carry = 0;
     for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;
     // every A key has at least one pair, and pairs are sorted by A key: the
@@ -850,6 +846,97 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
         if (threadIdx.x == blockDim.x - 1) carry = t0 + nt;
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, const PlanCounts* __restrict__ cnt,
+                                                      int bn, int max_tiles, int* __restrict__ first,
+                                                      int* __restrict__ tile0, int* __restrict__ tile_batch,
+                                                      int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
+    pdl_wait();
+    pdl_release();
+    pair_tiles_block(pairA, (int)cnt->nP, (int)cnt->nA, bn, max_tiles, first, tile0, tile_batch, tile_col0,
+                     tile_ncols);
+}
+
+// the tile arrays of one stage B launch: first pair and first tile of every A
+// key, then batch (A key), first pair and pair count of every tile
+struct PairTiles {
+    DevBuf<int> buf;
+    int bn = 0;
+    i64 max_tiles = 0;
+    int *first = nullptr, *tile0 = nullptr, *batch = nullptr, *col0 = nullptr, *ncols = nullptr;
+    bool built = false;
+    void alloc(i64 nA, i64 nP, int tile_pairs, cudaStream_t s) {
+        bn = tile_pairs;
+        max_tiles = nP / bn + nA + 1;
+        buf.alloc(2 * nA + 3 * max_tiles, s);
+        first = buf.p;
+        tile0 = buf.p + nA;
+        batch = buf.p + 2 * nA;
+        col0 = batch + max_tiles;
+        ncols = col0 + max_tiles;
+    }
+};
+
+// Bounded plans with at most 512 key flags and 8,192 pair-bitmap words: the
+// key plan, the pair plan and the stage-B tiles in one single-block launch
+// (three phases separated by block barriers; the global writes of a phase
+// are visible to the next).
+__global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __restrict__ used,
+                                                     uint64_t* __restrict__ ids, int* __restrict__ keyOf,
+                                                     int* __restrict__ aId, int* __restrict__ aKey, i64 words,
+                                                     const uint32_t* __restrict__ bits, uint64_t* __restrict__ pre,
+                                                     int* __restrict__ pairA, int* __restrict__ pairB, int bn,
+                                                     int max_tiles, int* __restrict__ first, int* __restrict__ tile0,
+                                                     int* __restrict__ tile_batch, int* __restrict__ tile_col0,
+                                                     int* __restrict__ tile_ncols, PlanCounts* __restrict__ cnt) {
+    pdl_wait();
+    pdl_release();
+    __shared__ uint32_t ws[32], total, nku_s;
+    // keys: joint scan of [usedKey | usedA]
+    const int k = threadIdx.x;  // flag k of 2 nk (<= 512)
+    const uint32_t f = k < 2 * nk ? used[k] : 0u;
+    const uint32_t ex = block_scan_1024(f, ws, &total);
+    if (k < 2 * nk) ids[k] = ex;
+    if (k == nk) nku_s = ex;  // exclusive count at nk = used keys
+    __syncthreads();
+    const uint32_t nku = nk > 0 ? nku_s : 0u;
+    const int nA = (int)(total - nku);
+    if (k == 0) {
+        cnt->key_total = total;
+        cnt->nku = nku;
+        cnt->nA = nA;
+    }
+    if (k < nk && f) keyOf[ex] = k;
+    if (k >= nk && k < 2 * nk && f) {
+        const int a = (int)(ex - nku);
+        aId[k - nk] = a;
+        aKey[a] = (int)(k - nk);
+    }
+    __syncthreads();
+    // pairs: per-word exclusive counts, then every set bit placed in parallel
+    uint32_t carry = 0;
+    for (i64 base = 0; base < words; base += 1024) {
+        const i64 w = base + threadIdx.x;
+        const uint32_t b = w < words ? bits[w] : 0u;
+        const uint32_t id = carry + block_scan_1024(__popc(b), ws, &total);
+        if (w < words) pre[w] = id;
+        carry += total;
+        __syncthreads();  // total and ws are rewritten by the next tile's scan
+    }
+    const int nP = (int)carry;
+    if (threadIdx.x == 0) cnt->nP = nP;
+    const int slots = (int)(nk * nk);
+    for (int slot = threadIdx.x; slot < slots; slot += blockDim.x) {
+        const uint32_t b = bits[slot >> 5];
+        if (!((b >> (slot & 31)) & 1u)) continue;
+        const int id = (int)pre[slot >> 5] + __popc(b & ((1u << (slot & 31)) - 1u));
+        const int k2 = slot / (int)nk;
+        pairA[id] = aId[k2];
+        pairB[id] = slot - k2 * (int)nk;
+    }
+    __syncthreads();
+    if (first) pair_tiles_block(pairA, nP, nA, bn, max_tiles, first, tile0, tile_batch, tile_col0, tile_ncols);
 }
 
 // G sliced once per table set (cached with the tables); the build synchronises
@@ -940,6 +1027,14 @@ constexpr i64 BOUNDED_KEYS = 256;
 // stage A runs on the tensor cores (mixed form) from this many outputs nA nS
 constexpr i64 TC_A_OUTPUTS = 1000000;
 
+// Stage B on the tensor cores slices every row of the expanded Hf (nA U^2
+// gathered values) against an FP64 product of nP U^2 FMAs: measured at ERIDA
+// 129^3 (nP = 65 nA) the two cost the same, so the sliced form is taken only
+// when the pairs per A key are clearly more.
+static bool stage_b_sliced(bool mixed, i64 nA, i64 nP, int U) {
+    return mixed && nA * (i64)U * U >= 4000000 && nP >= 80 * nA;
+}
+
 static void read_status(EvalStatus* d_st, EvalStatus& h, cudaStream_t s) {
     GLI_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
     GLI_CUDA(cudaStreamSynchronize(s));
@@ -978,40 +1073,57 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     }
     DevBuf<uint64_t> ids(2 * nk, s);
     DevBuf<int> keyOf(nk, s), aId(nk, s), aKey(nk, s);
-    if (2 * nk <= 1024) {
-        launch_pdl(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
-    } else {
-        exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
-        launch_pdl(k_plan_keys, dim3(kb), dim3(256), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
-    }
     DevBuf<uint64_t> pairPre(words, s);
+    DevBuf<int> pairA, pairB;
+    PairTiles tiles;
     const bool small_pairs = bounded && words <= 8 * 1024;
-    DevBuf<uint32_t> counts;
-    if (!small_pairs) {
-        counts.alloc(words, s);
-        launch_pdl(k_word_counts, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, pairBits.p, counts.p);
-        exclusive_scan_u32_dev(counts.p, pairPre.p, words, &cnt->nP, s);
-    }
     if (bounded) {
         sz.nku = nk;
         sz.nA = nk;
         // pairs (A, B) have A >= B; every class has one pair
         sz.nP = std::min(nk * (nk + 1) / 2, m);
-    } else {
-        EvalStatus h;
-        read_status(st, h, s);
-        if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", t.kind ? "ERI" : "ERIDA");
-        sz.nku = h.cnt.nku;
-        sz.nA = h.cnt.nA;
-        sz.nP = (i64)h.cnt.nP;
     }
-    DevBuf<int> pairA(sz.nP, s), pairB(sz.nP, s);
-    if (small_pairs)
-        launch_pdl(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p, pairA.p,
-                   pairB.p, cnt);
-    else
-        launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk, pairBits.p,
-                   pairPre.p, aId.p, pairA.p, pairB.p);
+    if (small_pairs && 2 * nk <= 1024) {
+        // the whole plan and stage B's tiles in one launch
+        pairA.alloc(sz.nP, s);
+        pairB.alloc(sz.nP, s);
+        tiles.alloc(sz.nA, sz.nP, stage_b_sliced(a.mixed, sz.nA, sz.nP, U) ? tile_n(MIXED_SLICES) : DM_BM, s);
+        launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
+                   pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
+                   tiles.batch, tiles.col0, tiles.ncols, cnt);
+        tiles.built = true;
+    } else {
+        if (2 * nk <= 1024) {
+            launch_pdl(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
+        } else {
+            exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
+            launch_pdl(k_plan_keys, dim3(kb), dim3(256), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
+        }
+        DevBuf<uint32_t> counts;
+        if (!small_pairs) {
+            counts.alloc(words, s);
+            launch_pdl(k_word_counts, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, pairBits.p,
+                       counts.p);
+            exclusive_scan_u32_dev(counts.p, pairPre.p, words, &cnt->nP, s);
+        }
+        if (!bounded) {
+            EvalStatus h;
+            read_status(st, h, s);
+            if (h.bad)
+                fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", t.kind ? "ERI" : "ERIDA");
+            sz.nku = h.cnt.nku;
+            sz.nA = h.cnt.nA;
+            sz.nP = (i64)h.cnt.nP;
+        }
+        pairA.alloc(sz.nP, s);
+        pairB.alloc(sz.nP, s);
+        if (small_pairs)
+            launch_pdl(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p,
+                       pairA.p, pairB.p, cnt);
+        else
+            launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk,
+                       pairBits.p, pairPre.p, aId.p, pairA.p, pairB.p);
+    }
 
     const i64 nA = sz.nA, nP = sz.nP, nku = sz.nku;
     if (nA * (i64)U * U > ((i64)1 << 31))
@@ -1020,11 +1132,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     // the mixed form runs a stage on the tensor cores when it is large enough for
     // them to pay off; smaller stages (latency-bound either way) stay FP64
     const bool tc_a = a.mixed && nA * (i64)nS >= TC_A_OUTPUTS;
-    // stage B on the tensor cores slices every row of the expanded Hf (nA U^2
-    // gathered values) against an FP64 product of nP U^2 FMAs: measured at
-    // ERIDA 129^3 (nP = 65 nA) the two cost the same, so the sliced form is
-    // taken only when the pairs per A key are clearly more
-    const bool tc_b = a.mixed && nA * (i64)U * U >= 4000000 && nP >= 80 * nA;
+    const bool tc_b = stage_b_sliced(a.mixed, nA, nP, U);
     timer.mark();
     // ---- stage A
     if (tc_a) {
@@ -1077,38 +1185,34 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         TiledSlices Hs, Wb;
         Hs.alloc(nA * mb, TC_BM, U, MIXED_SLICES, s);
         slice_tiled(ExpandedHRows{H.p, t.sidx.p, cnt, nS, U, mb}, nA * U, U, Hs, s);
-        const i64 max_tiles = nP / BN + nA + 1;
-        DevBuf<int> grp(2 * nA + 3 * max_tiles, s);
-        int* first = grp.p;
-        int* tile0 = grp.p + nA;
-        int* tile_batch = grp.p + 2 * nA;
-        int* tile_col0 = tile_batch + max_tiles;
-        int* tile_ncols = tile_col0 + max_tiles;
-        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, BN, (int)max_tiles, first, tile0, tile_batch,
-                   tile_col0, tile_ncols);
+        if (!tiles.built) {
+            tiles.alloc(nA, nP, BN, s);
+            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, BN, (int)tiles.max_tiles, tiles.first,
+                       tiles.tile0, tiles.batch, tiles.col0, tiles.ncols);
+        }
+        const i64 max_tiles = tiles.max_tiles;
         Wb.alloc(max_tiles, BN, U, MIXED_SLICES, s);
-        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, first, tile0, tile_col0, tile_ncols, cnt, Up, BN}, nP, U, Wb,
-                    s);
+        slice_tiled(PairRows{t.W.p, pairA.p, pairB.p, tiles.first, tiles.tile0, tiles.col0, tiles.ncols, cnt, Up, BN},
+                    nP, U, Wb, s);
         TileWork w;
         w.a_rows = U;
         w.a_blocks = mb;
         w.a_batched = 1;
-        w.tile_batch = tile_batch;
-        w.tile_col0 = tile_col0;
-        w.tile_ncols = tile_ncols;
+        w.tile_batch = tiles.batch;
+        w.tile_col0 = tiles.col0;
+        w.tile_ncols = tiles.ncols;
         w.C = H2.p;
         w.rs = 1;
         w.cs = Up;
         tc_gemm_tiled(Hs.view(), Wb.view(), w, (int)max_tiles, &st->tc_err, s);
     } else {
         // tiles of 64 pairs of one A key, then (tile, 64 u, chunk of v) blocks
-        const i64 max_tiles = nP / DM_BM + nA + 1;
-        DevBuf<int> grp(2 * nA + 3 * max_tiles, s);
-        int* tile_batch = grp.p + 2 * nA;
-        int* tile_col0 = tile_batch + max_tiles;
-        int* tile_ncols = tile_col0 + max_tiles;
-        launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, DM_BM, (int)max_tiles, grp.p, grp.p + nA,
-                   tile_batch, tile_col0, tile_ncols);
+        if (!tiles.built) {
+            tiles.alloc(nA, nP, DM_BM, s);
+            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, DM_BM, (int)tiles.max_tiles, tiles.first,
+                       tiles.tile0, tiles.batch, tiles.col0, tiles.ncols);
+        }
+        const i64 max_tiles = tiles.max_tiles;
         // the tile count is known on the device only: the split follows its bound
         const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
@@ -1120,8 +1224,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             parts.alloc(P * ps, s);
             dst = parts.p;
         }
-        dmma_launch(StageBOp{t.W.p, H.p, t.sidx.p, pairB.p, tile_batch, tile_col0, tile_ncols, nS, U, Up, v_chunk, ps,
-                             dst},
+        dmma_launch(StageBOp{t.W.p, H.p, t.sidx.p, pairB.p, tiles.batch, tiles.col0, tiles.ncols, nS, U, Up, v_chunk,
+                             ps, dst},
                     dim3((unsigned)max_tiles, ub, (unsigned)P), s);
         if (P > 1) {
             launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
