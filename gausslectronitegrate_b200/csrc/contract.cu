@@ -76,6 +76,18 @@ __device__ inline uint64_t div_est(uint64_t u, uint64_t d, double inv) {
     return q;
 }
 
+// the same for 32-bit operands, in 32-bit arithmetic (d < 2^31): the
+// remainder of a quotient one too large wraps to at least 2^32 - d
+__device__ inline uint32_t div32_est(uint32_t u, uint32_t d, double inv) {
+    uint32_t q = (uint32_t)((double)u * inv);
+    const uint32_t r = u - q * d;
+    if (r >= 0x80000000u)
+        --q;
+    else if (r >= d)
+        ++q;
+    return q;
+}
+
 // grid point lin (x-major) -> coordinates; 32-bit arithmetic
 __device__ inline void decode_pt(const ClassDecode& d, uint32_t lin, int p[3]) {
     const uint32_t r = lin / d.n2;
@@ -110,9 +122,9 @@ __device__ inline bool class_keys(const ClassDecode& d, i64 idx, int k[3]) {
     } else {
         const uint64_t hi = d.fast ? div_est(u, d.N2, d.invN2) : u / d.N2;  // point pair (p0, p1)
         if (hi >= d.N2) return false;
-        const uint64_t lo = u - hi * d.N2;                                   // point pair (p2, p3)
-        const uint64_t i0 = div_est(hi, d.n32, d.invN), i2 = div_est(lo, d.n32, d.invN);
-        const short4 p0 = d.pt[i0], p1 = d.pt[hi - i0 * d.n32], p2 = d.pt[i2], p3 = d.pt[lo - i2 * d.n32];
+        const uint32_t h = (uint32_t)hi, lo = (uint32_t)(u - hi * d.N2);  // point pair (p2, p3); N^2 < 2^32
+        const uint32_t i0 = div32_est(h, d.n32, d.invN), i2 = div32_est(lo, d.n32, d.invN);
+        const short4 p0 = d.pt[i0], p1 = d.pt[h - i0 * d.n32], p2 = d.pt[i2], p3 = d.pt[lo - i2 * d.n32];
         const int L = (int)d.L;
         k[0] = eri_axis_key32(p0.x - p1.x, p2.x - p3.x, (p0.x + p1.x) - (p2.x + p3.x), L);
         k[1] = eri_axis_key32(p0.y - p1.y, p2.y - p3.y, (p0.y + p1.y) - (p2.y + p3.y), L);
@@ -1084,14 +1096,27 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         sz.nP = std::min(nk * (nk + 1) / 2, m);
     }
     if (small_pairs && 2 * nk <= 1024) {
-        // the whole plan and stage B's tiles in one launch
-        pairA.alloc(sz.nP, s);
-        pairB.alloc(sz.nP, s);
-        tiles.alloc(sz.nA, sz.nP, stage_b_sliced(a.mixed, sz.nA, sz.nP, U) ? tile_n(MIXED_SLICES) : DM_BM, s);
+        // the whole plan and stage B's tiles in one launch, sized by bounds
+        // (for exact plans, with their larger key spaces, the single block's
+        // pass over nk^2 pair slots measured no faster than the multi-block
+        // path: ERI 7^3 0.206 against 0.200 ms)
+        const i64 nA_b = nk, nP_b = std::min(nk * (nk + 1) / 2, m);
+        pairA.alloc(nP_b, s);
+        pairB.alloc(nP_b, s);
+        tiles.alloc(nA_b, nP_b, bounded && stage_b_sliced(a.mixed, nA_b, nP_b, U) ? tile_n(MIXED_SLICES) : DM_BM, s);
         launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
                    tiles.batch, tiles.col0, tiles.ncols, cnt);
         tiles.built = true;
+        if (!bounded) {
+            EvalStatus h;
+            read_status(st, h, s);
+            if (h.bad)
+                fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", t.kind ? "ERI" : "ERIDA");
+            sz.nku = h.cnt.nku;
+            sz.nA = h.cnt.nA;
+            sz.nP = (i64)h.cnt.nP;
+        }
     } else {
         if (2 * nk <= 1024) {
             launch_pdl(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
@@ -1179,6 +1204,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     timer.mark();
     // ---- stage B
     DevBuf<double> H2(nP * (i64)Up, s);
+    if (tiles.built && tiles.bn != (tc_b ? tile_n(MIXED_SLICES) : DM_BM)) tiles.built = false;
     if (tc_b) {
         constexpr int BN = tile_n(MIXED_SLICES);
         const int mb = (U + TC_BM - 1) / TC_BM;

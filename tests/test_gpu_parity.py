@@ -141,6 +141,17 @@ def test_eri_values_large_key_space(gli, form):
         assert np.max(np.abs(vals - ref)) <= 1e-8
 
 
+def test_eri_values_sample_7(gli):
+    # ERI on 7^3: every one of the 3,571,977 classes evaluated (364 axis keys:
+    # the plan reads its counts back), a seeded sample against the oracle
+    s = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(7), 1e-10)
+    idx, val = s.indices, s.values
+    assert idx.size == 3571977
+    pick = np.random.default_rng(5).choice(idx.size, size=300, replace=False)
+    ref = ORACLE.values("eri", g10(), sym_grid(7), idx[pick], 1e-10)
+    assert_parity(val[pick], ref, what="ERI 7^3 sample")
+
+
 def test_erida_values_sample_129(gli):
     # ERIDA on 129^3: enumeration count, sortedness and a seeded sample of
     # classes against the oracle (the full CPU reference takes minutes)
