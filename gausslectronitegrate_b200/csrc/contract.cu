@@ -1096,27 +1096,17 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         sz.nP = std::min(nk * (nk + 1) / 2, m);
     }
     if (small_pairs && 2 * nk <= 1024) {
-        // the whole plan and stage B's tiles in one launch, sized by bounds
-        // (for exact plans, with their larger key spaces, the single block's
-        // pass over nk^2 pair slots measured no faster than the multi-block
-        // path: ERI 7^3 0.206 against 0.200 ms)
-        const i64 nA_b = nk, nP_b = std::min(nk * (nk + 1) / 2, m);
-        pairA.alloc(nP_b, s);
-        pairB.alloc(nP_b, s);
-        tiles.alloc(nA_b, nP_b, bounded && stage_b_sliced(a.mixed, nA_b, nP_b, U) ? tile_n(MIXED_SLICES) : DM_BM, s);
+        // the whole plan and stage B's tiles in one launch (bounded plans; for
+        // the larger key spaces of exact plans the single block's pass over
+        // nk^2 pair slots measured no faster than the multi-block path: ERI
+        // 7^3 0.206 against 0.200 ms)
+        pairA.alloc(sz.nP, s);
+        pairB.alloc(sz.nP, s);
+        tiles.alloc(sz.nA, sz.nP, stage_b_sliced(a.mixed, sz.nA, sz.nP, U) ? tile_n(MIXED_SLICES) : DM_BM, s);
         launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
                    tiles.batch, tiles.col0, tiles.ncols, cnt);
         tiles.built = true;
-        if (!bounded) {
-            EvalStatus h;
-            read_status(st, h, s);
-            if (h.bad)
-                fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", t.kind ? "ERI" : "ERIDA");
-            sz.nku = h.cnt.nku;
-            sz.nA = h.cnt.nA;
-            sz.nP = (i64)h.cnt.nP;
-        }
     } else {
         if (2 * nk <= 1024) {
             launch_pdl(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
