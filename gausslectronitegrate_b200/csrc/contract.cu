@@ -377,7 +377,7 @@ template <int BN_>
 struct StageAOp {
     static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
     static constexpr int BN = BN_;
-    static constexpr int NB = BN / 8;  // B elements per thread
+    static constexpr int NB = BN / 16;  // B element pairs per thread (rows of W are contiguous in t)
     const double* W;
     const double* T;
     const int* S;
@@ -428,16 +428,19 @@ struct StageAOp {
     __device__ void b_init(const Block& b, BState& st) const {
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
-            const int r = dm_rowmajor_row(threadIdx.x, q);
+            const int r = dm_pair_row(threadIdx.x, q);
             st.off[q] = r < b.nvalid ? (i64)aKey[b.n0 + r] * Up : -1;
         }
     }
+    // pairs (t, t + 1), t even: W rows start at multiples of Up (a multiple of
+    // 4) and chunks at multiples of 16, so every pair is 16-byte aligned
     __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
-        const int k = dm_rowmajor_k(threadIdx.x), t = b.t0 + kc * DM_BK + k;
+        const int k = dm_pair_k(threadIdx.x), t = b.t0 + kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(t, b.t1);
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
-            const bool v = st.off[q] >= 0 && t < b.t1;
-            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), v ? W + st.off[q] + t : W, v);
+            const int n = st.off[q] >= 0 ? bytes : 0;
+            dm_cp16(tile + dm_rowmajor_at(dm_pair_row(threadIdx.x, q), k), n ? W + st.off[q] + t : W, n);
         }
     }
     __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
@@ -476,7 +479,7 @@ struct StageBOp {
         double* H2;
     };
     struct AState {
-        i64 off[DM_ELEMS];  // pairB * Up of this thread's pair rows, -1 past the tile
+        i64 off[DM_BM / 16];  // pairB * Up of this thread's pair rows, -1 past the tile
     };
     struct BState {
         int sv[DM_ELEMS];  // sidx of the next chunk's elements (-1: zero fill)
@@ -497,17 +500,19 @@ struct StageBOp {
     }
     __device__ void a_init(const Block& b, AState& st) const {
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
-            const int r = dm_rowmajor_row(threadIdx.x, q);
+        for (int q = 0; q < DM_BM / 16; ++q) {
+            const int r = dm_pair_row(threadIdx.x, q);
             st.off[q] = r < b.mvalid ? (i64)pairB[b.p0 + r] * Up : -1;
         }
     }
+    // pairs (v, v + 1), v even: 16-byte aligned in the W rows
     __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
-        const int k = dm_rowmajor_k(threadIdx.x), v = b.v0 + kc * DM_BK + k;
+        const int k = dm_pair_k(threadIdx.x), v = b.v0 + kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(v, b.v1);
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
-            const bool ok = st.off[q] >= 0 && v < b.v1;
-            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? W + st.off[q] + v : W, ok);
+        for (int q = 0; q < DM_BM / 16; ++q) {
+            const int n = st.off[q] >= 0 ? bytes : 0;
+            dm_cp16(tile + dm_rowmajor_at(dm_pair_row(threadIdx.x, q), k), n ? W + st.off[q] + v : W, n);
         }
     }
     __device__ void b_load(const Block& b, BState& st, int kc) const {
@@ -626,7 +631,7 @@ template <int BN_>
 struct ProductOp {
     static constexpr bool A_KMAJOR = false, B_KMAJOR = false;
     static constexpr int BN = BN_;
-    static constexpr int NB = BN / 8;  // B elements per thread
+    static constexpr int NB = BN / 16;  // B element pairs per thread
     const double* H2;
     const double* W;
     const int* keyOf;
@@ -639,7 +644,7 @@ struct ProductOp {
         int m0, n0;
     };
     struct AState {
-        i64 off[DM_ELEMS];
+        i64 off[DM_BM / 16];
     };
     struct BState {
         i64 off[NB];
@@ -655,32 +660,36 @@ struct ProductOp {
     }
     __device__ void a_init(const Block& b, AState& st) const {
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
-            const int r = dm_rowmajor_row(threadIdx.x, q);
+        for (int q = 0; q < DM_BM / 16; ++q) {
+            const int r = dm_pair_row(threadIdx.x, q);
             st.off[q] = r < b.mvalid ? (i64)(b.m0 + r) * Up : -1;
         }
     }
     __device__ void b_init(const Block& b, BState& st) const {
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
-            const int r = dm_rowmajor_row(threadIdx.x, q);
+            const int r = dm_pair_row(threadIdx.x, q);
             st.off[q] = r < b.nvalid ? (i64)keyOf[b.n0 + r] * Up : -1;
         }
     }
+    // pairs (u, u + 1), u even: H2 and W rows start at multiples of Up (a
+    // multiple of 4), so every pair is 16-byte aligned
     __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
-        const int k = dm_rowmajor_k(threadIdx.x), u = kc * DM_BK + k;
+        const int k = dm_pair_k(threadIdx.x), u = kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(u, U);
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
-            const bool ok = st.off[q] >= 0 && u < U;
-            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? H2 + st.off[q] + u : H2, ok);
+        for (int q = 0; q < DM_BM / 16; ++q) {
+            const int n = st.off[q] >= 0 ? bytes : 0;
+            dm_cp16(tile + dm_rowmajor_at(dm_pair_row(threadIdx.x, q), k), n ? H2 + st.off[q] + u : H2, n);
         }
     }
     __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
-        const int k = dm_rowmajor_k(threadIdx.x), u = kc * DM_BK + k;
+        const int k = dm_pair_k(threadIdx.x), u = kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(u, U);
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
-            const bool ok = st.off[q] >= 0 && u < U;
-            dm_cp8(tile + dm_rowmajor_at(dm_rowmajor_row(threadIdx.x, q), k), ok ? W + st.off[q] + u : W, ok);
+            const int n = st.off[q] >= 0 ? bytes : 0;
+            dm_cp16(tile + dm_rowmajor_at(dm_pair_row(threadIdx.x, q), k), n ? W + st.off[q] + u : W, n);
         }
     }
     __device__ void store(const Block& b, int mm, int n, double v0, double v1) const {

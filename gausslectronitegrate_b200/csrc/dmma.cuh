@@ -63,6 +63,18 @@ __device__ __forceinline__ void dm_cp8(double* dst, const double* src, bool vali
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0)
                  : "memory");
 }
+// 16-byte copy of two consecutive doubles; bytes (0, 8 or 16) are read, the
+// rest of the 16 written as zeros (src 16-byte aligned, valid even for 0)
+__device__ __forceinline__ void dm_cp16(double* dst, const double* src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+// row-major tiles whose rows are contiguous in K: thread tid's q-th pair of
+// elements (q < rows / 16) is row (tid >> 3) + 16 q, k = 2 (tid & 7) and k + 1
+__device__ __forceinline__ int dm_pair_row(int tid, int q) { return (tid >> 3) + 16 * q; }
+__device__ __forceinline__ int dm_pair_k(int tid) { return (tid & 7) * 2; }
+// bytes of the pair (k, k + 1) that lie before the end of the K range
+__device__ __forceinline__ int dm_pair_bytes(int k, int kend) { return k + 1 < kend ? 16 : (k < kend ? 8 : 0); }
 __device__ __forceinline__ void dm_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void dm_wait() {
