@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <list>
 #include <memory>
+#include <thread>
 
 #include "dmma.cuh"
 #include "tables.cuh"
@@ -1503,6 +1504,30 @@ struct HostCallBuffers {
 };
 static thread_local HostCallBuffers t_host_call;
 
+// Host copies of long class lists: a pageable <-> pinned memcpy runs at a
+// fraction of the host's memory bandwidth on one core, so copies of several MB
+// are split over a few threads.
+static void host_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kSplit = (size_t)1 << 20;  // at least 1 MB per thread
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<size_t>(std::min<size_t>(8, hw > 1 ? hw / 2 : 1), bytes / kSplit);
+    if (nt <= 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes / nt + 63) / 64 * 64;
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) {
+        const size_t b0 = std::min(bytes, k * part), b1 = std::min(bytes, (k + 1) * part);
+        if (b1 > b0) th.emplace_back([=] { memcpy((char*)dst + b0, (const char*)src + b0, b1 - b0); });
+    }
+    memcpy(dst, src, std::min(bytes, part));
+    for (auto& t : th) t.join();
+}
+
+// The evaluation from and into host arrays: the class list goes to the device
+// in chunks, each chunk's DMA overlapping the host copy of the next into the
+// pinned staging buffer; the values come back the same way in reverse.
 void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices, i64 m,
                         double tol, int form, double* h_out, cudaStream_t s) {
     if (m == 0) return;
@@ -1511,16 +1536,47 @@ void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc
     int64_t* pin_idx = (int64_t*)t_pin_idx.get((size_t)m * sizeof(int64_t));
     double* pin_val = (double*)t_pin_val.get((size_t)m * sizeof(double));
     t_host_call.ensure(ctx.device, m);
-    memcpy(pin_idx, h_indices, (size_t)m * sizeof(int64_t));
-    GLI_CUDA(cudaMemcpyAsync(t_host_call.idx->p, pin_idx, (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const i64 chunks = m >= ((i64)1 << 20) ? 2 : 1, per = (m + chunks - 1) / chunks;
+    for (i64 c = 0; c < chunks; ++c) {
+        const i64 b = c * per, n = std::min(m, b + per) - b;
+        if (n <= 0) break;
+        host_copy(pin_idx + b, h_indices + b, (size_t)n * sizeof(int64_t));
+        GLI_CUDA(cudaMemcpyAsync(t_host_call.idx->p + b, pin_idx + b, (size_t)n * sizeof(int64_t),
+                                 cudaMemcpyHostToDevice, s));
+    }
     std::shared_ptr<const LatticeTables> tp;
     StageTimer timer(t_timing, s);
     sparse_values_enqueue(kind, h_coeffs, nb, g, t_host_call.idx->p, m, tol, form, t_host_call.val->p, s, hs, tp,
                           timer);
-    GLI_CUDA(cudaMemcpyAsync(pin_val, t_host_call.val->p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GLI_CUDA(cudaStreamSynchronize(s));
+    if (chunks == 1) {
+        GLI_CUDA(cudaMemcpyAsync(pin_val, t_host_call.val->p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        check_status(kind, m, *hs, *tp, timer, nullptr);
+        host_copy(h_out, pin_val, (size_t)m * sizeof(double));
+        return;
+    }
+    cudaEvent_t ev[2];
+    for (auto& e : ev) GLI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    struct Release {
+        cudaEvent_t* e;
+        ~Release() {
+            for (int k = 0; k < 2; ++k) cudaEventDestroy(e[k]);
+        }
+    } release{ev};
+    for (i64 c = 0; c < chunks; ++c) {
+        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
+        if (n > 0)
+            GLI_CUDA(cudaMemcpyAsync(pin_val + b, t_host_call.val->p + b, (size_t)n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaEventRecord(ev[c], s));
+    }
+    GLI_CUDA(cudaEventSynchronize(ev[0]));  // the status copy came before the values
     check_status(kind, m, *hs, *tp, timer, nullptr);
-    memcpy(h_out, pin_val, (size_t)m * sizeof(double));
+    for (i64 c = 0; c < chunks; ++c) {
+        const i64 b = c * per, n = std::min(m, b + per) - b;
+        GLI_CUDA(cudaEventSynchronize(ev[c]));
+        if (n > 0) host_copy(h_out + b, pin_val + b, (size_t)n * sizeof(double));
+    }
 }
 
 }  // namespace gli
