@@ -466,7 +466,8 @@ struct StageBOp {
     const double* W;
     const double* H;
     const int* sidx;
-    const int* pairB;
+    const int* rowKey;   // weight key of each tile row
+    const int* rowPair;  // H2 row (pair id) of each tile row
     const int* tile_batch;
     const int* tile_col0;
     const int* tile_ncols;
@@ -480,7 +481,7 @@ struct StageBOp {
         double* H2;
     };
     struct AState {
-        i64 off[DM_BM / 16];  // pairB * Up of this thread's pair rows, -1 past the tile
+        i64 off[DM_BM / 16];  // weight key * Up of this thread's rows, -1 past the tile
     };
     struct BState {
         int sv[DM_ELEMS];  // sidx of the next chunk's elements (-1: zero fill)
@@ -503,7 +504,7 @@ struct StageBOp {
 #pragma unroll
         for (int q = 0; q < DM_BM / 16; ++q) {
             const int r = dm_pair_row(threadIdx.x, q);
-            st.off[q] = r < b.mvalid ? (i64)pairB[b.p0 + r] * Up : -1;
+            st.off[q] = r < b.mvalid ? (i64)rowKey[b.p0 + r] * Up : -1;
         }
     }
     // pairs (v, v + 1), v even: 16-byte aligned in the W rows
@@ -536,7 +537,7 @@ struct StageBOp {
     }
     __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
         if (m >= b.mvalid) return;
-        double* h2 = b.H2 + (i64)(b.p0 + m) * Up + b.u0 + n;
+        double* h2 = b.H2 + (i64)__ldg(&rowPair[b.p0 + m]) * Up + b.u0 + n;
         if (n + 1 < b.nvalid)
             *reinterpret_cast<double2*>(h2) = make_double2(v0, v1);  // Up, u0 and n are even
         else if (n < b.nvalid)
@@ -813,12 +814,45 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
     __device__ bool valid(i64 p) const { return p < (i64)cnt->nP; }
 };
 
+// Balanced hosts of a full pair triangle.  A pair's stage-B row is symmetric
+// in its two keys (sum_v sum_t W_b[v] W_a[t] T[u^2 + v^2 + t^2]), so either
+// key's H row can host it.  Hosting by the larger key gives key a a + 1 rows
+// (ragged tiles: 67% full at 129 keys); when every pair {a, b} of n A keys is
+// present the hosts are chosen instead so that most keys fill whole tiles:
+// keys below y = min(n, 2 bn - 1) form a regular tournament (key i hosts its
+// own pair and i + j mod y for j < reg_count(i, y): at most bn rows), and the
+// keys from y up host every pair with a key below y plus a regular tournament
+// among themselves (129 keys: 132 tiles of 64 instead of 195).
+__device__ __forceinline__ int reg_count(int i, int y) { return (y & 1) ? (y + 1) / 2 : y / 2 + (i < y / 2); }
+__device__ __forceinline__ int reg_prefix(int i, int y) {  // rows of the members below i
+    if (y & 1) return i * ((y + 1) / 2);
+    const int h = y / 2;
+    return i <= h ? i * (h + 1) : h * (h + 1) + (i - h) * h;
+}
+__device__ __forceinline__ int bal_count(int h, int n, int y) {
+    return h < y ? reg_count(h, y) : y + reg_count(h - y, n - y);
+}
+__device__ __forceinline__ int bal_offset(int h, int n, int y) {
+    return h < y ? reg_prefix(h, y) : y * (y + 1) / 2 + (h - y) * y + reg_prefix(h - y, n - y);
+}
+// the partner key of host h's j-th row
+__device__ __forceinline__ int bal_partner(int h, int j, int n, int y) {
+    if (h < y) return (h + j) % y;
+    return j < y ? j : y + (h - y + j - y) % (n - y);
+}
+
 // One block: first pair, pair count and first tile of every A key (pairs are
-// ordered by A key), and the tile list of stage B (tiles of bn pairs, each in
-// one A key); tiles past the last one get no columns.
-__device__ void pair_tiles_block(const int* __restrict__ pairA, int nP, int nA, int bn, int max_tiles,
+// ordered by A key), and the tile list of stage B (tiles of bn rows, each in
+// one host A key); tiles past the last one get no columns.  With row lists
+// (rowPair, rowKey: the H2 row and the weight key of each tile row) a full
+// pair triangle of more than bn keys gets balanced hosts; otherwise the rows
+// are the pairs in order, each hosted by its A key.
+// (pairA, pairB and aKey may have been written earlier in the same kernel:
+// plain coherent loads, no __restrict__)
+__device__ void pair_tiles_block(const int* pairA, const int* pairB, const int* aKey, int nP, int nA, int nku, int bn, int max_tiles,
                                  int* __restrict__ first, int* __restrict__ tile0, int* __restrict__ tile_batch,
-                                 int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
+                                 int* __restrict__ tile_col0, int* __restrict__ tile_ncols, int* __restrict__ rowPair,
+                                 int* __restrict__ rowKey) {
     __shared__ int warp_sums[32];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -827,13 +861,38 @@ __device__ void pair_tiles_block(const int* __restrict__ pairA, int nP, int nA, 
     // first pair of each key is where the key changes
     for (int p = threadIdx.x; p < nP; p += blockDim.x)
         if (p == 0 || pairA[p] != pairA[p - 1]) first[pairA[p]] = p;
+    const bool balanced = rowPair && nA > bn && nku == nA && (i64)nP == (i64)nA * (nA + 1) / 2;
+    const int y = min(nA, 2 * bn - 1);
+    if (rowPair) {
+        if (balanced) {
+            // host h's rows in stripes of 8 threads
+            for (int item = threadIdx.x; item < nA * 8; item += blockDim.x) {
+                const int h = item >> 3, d = bal_count(h, nA, y), o = bal_offset(h, nA, y);
+                for (int j = item & 7; j < d; j += 8) {
+                    const int g = bal_partner(h, j, nA, y), hi = max(h, g), lo = min(h, g);
+                    rowPair[o + j] = hi * (hi + 1) / 2 + lo;  // the pair id of (hi, lo) in a full triangle
+                    rowKey[o + j] = aKey[g];
+                }
+            }
+        } else {
+            for (int p = threadIdx.x; p < nP; p += blockDim.x) {
+                rowPair[p] = p;
+                rowKey[p] = pairB[p];
+            }
+        }
+    }
     __syncthreads();
     for (int base = 0; base < nA; base += blockDim.x) {
         const int a = base + threadIdx.x;
         int lo = 0, npairs = 0;
         if (a < nA) {
-            lo = first[a];
-            npairs = (a + 1 < nA ? first[a + 1] : nP) - lo;
+            if (balanced) {
+                lo = bal_offset(a, nA, y);
+                npairs = bal_count(a, nA, y);
+            } else {
+                lo = first[a];
+                npairs = (a + 1 < nA ? first[a + 1] : nP) - lo;
+            }
         }
         const int nt = (npairs + bn - 1) / bn;
         // block exclusive scan of nt
@@ -870,33 +929,39 @@ __device__ void pair_tiles_block(const int* __restrict__ pairA, int nP, int nA, 
     }
 }
 
-__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, const PlanCounts* __restrict__ cnt,
+__global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pairA, const int* __restrict__ pairB,
+                                                      const int* __restrict__ aKey, const PlanCounts* __restrict__ cnt,
                                                       int bn, int max_tiles, int* __restrict__ first,
                                                       int* __restrict__ tile0, int* __restrict__ tile_batch,
-                                                      int* __restrict__ tile_col0, int* __restrict__ tile_ncols) {
+                                                      int* __restrict__ tile_col0, int* __restrict__ tile_ncols,
+                                                      int* __restrict__ rowPair, int* __restrict__ rowKey) {
     pdl_wait();
     pdl_release();
-    pair_tiles_block(pairA, (int)cnt->nP, (int)cnt->nA, bn, max_tiles, first, tile0, tile_batch, tile_col0,
-                     tile_ncols);
+    pair_tiles_block(pairA, pairB, aKey, (int)cnt->nP, (int)cnt->nA, (int)cnt->nku, bn, max_tiles, first, tile0,
+                     tile_batch, tile_col0, tile_ncols, rowPair, rowKey);
 }
 
 // the tile arrays of one stage B launch: first pair and first tile of every A
-// key, then batch (A key), first pair and pair count of every tile
+// key, then batch (host A key), first row and row count of every tile, and
+// (FP64 stage B: `rows`) the H2 row and weight key of every tile row
 struct PairTiles {
     DevBuf<int> buf;
     int bn = 0;
     i64 max_tiles = 0;
     int *first = nullptr, *tile0 = nullptr, *batch = nullptr, *col0 = nullptr, *ncols = nullptr;
+    int *rowPair = nullptr, *rowKey = nullptr;
     bool built = false;
-    void alloc(i64 nA, i64 nP, int tile_pairs, cudaStream_t s) {
+    void alloc(i64 nA, i64 nP, int tile_pairs, bool rows, cudaStream_t s) {
         bn = tile_pairs;
         max_tiles = nP / bn + nA + 1;
-        buf.alloc(2 * nA + 3 * max_tiles, s);
+        buf.alloc(2 * nA + 3 * max_tiles + (rows ? 2 * nP : 0), s);
         first = buf.p;
         tile0 = buf.p + nA;
         batch = buf.p + 2 * nA;
         col0 = batch + max_tiles;
         ncols = col0 + max_tiles;
+        rowPair = rows ? ncols + max_tiles : nullptr;
+        rowKey = rows ? rowPair + nP : nullptr;
     }
 };
 
@@ -911,7 +976,8 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
                                                      int* __restrict__ pairA, int* __restrict__ pairB, int bn,
                                                      int max_tiles, int* __restrict__ first, int* __restrict__ tile0,
                                                      int* __restrict__ tile_batch, int* __restrict__ tile_col0,
-                                                     int* __restrict__ tile_ncols, PlanCounts* __restrict__ cnt) {
+                                                     int* __restrict__ tile_ncols, int* __restrict__ rowPair,
+                                                     int* __restrict__ rowKey, PlanCounts* __restrict__ cnt) {
     pdl_wait();
     pdl_release();
     __shared__ uint32_t ws[32], total, nku_s;
@@ -958,7 +1024,9 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
         pairB[id] = slot - k2 * (int)nk;
     }
     __syncthreads();
-    if (first) pair_tiles_block(pairA, nP, nA, bn, max_tiles, first, tile0, tile_batch, tile_col0, tile_ncols);
+    if (first)
+        pair_tiles_block(pairA, pairB, aKey, nP, nA, (int)nku, bn, max_tiles, first, tile0, tile_batch, tile_col0,
+                         tile_ncols, rowPair, rowKey);
 }
 
 // G sliced once per table set (cached with the tables); the build synchronises
@@ -1112,10 +1180,11 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         // 7^3 0.206 against 0.200 ms)
         pairA.alloc(sz.nP, s);
         pairB.alloc(sz.nP, s);
-        tiles.alloc(sz.nA, sz.nP, stage_b_sliced(a.mixed, sz.nA, sz.nP, U) ? tile_n(MIXED_SLICES) : DM_BM, s);
+        const bool sliced = stage_b_sliced(a.mixed, sz.nA, sz.nP, U);
+        tiles.alloc(sz.nA, sz.nP, sliced ? tile_n(MIXED_SLICES) : DM_BM, !sliced, s);
         launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
-                   tiles.batch, tiles.col0, tiles.ncols, cnt);
+                   tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt);
         tiles.built = true;
     } else {
         if (2 * nk <= 1024) {
@@ -1212,9 +1281,10 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         Hs.alloc(nA * mb, TC_BM, U, MIXED_SLICES, s);
         slice_tiled(ExpandedHRows{H.p, t.sidx.p, cnt, nS, U, mb}, nA * U, U, Hs, s);
         if (!tiles.built) {
-            tiles.alloc(nA, nP, BN, s);
-            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, BN, (int)tiles.max_tiles, tiles.first,
-                       tiles.tile0, tiles.batch, tiles.col0, tiles.ncols);
+            tiles.alloc(nA, nP, BN, false, s);
+            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, pairB.p, aKey.p, cnt, BN,
+                       (int)tiles.max_tiles, tiles.first, tiles.tile0, tiles.batch, tiles.col0, tiles.ncols,
+                       (int*)nullptr, (int*)nullptr);
         }
         const i64 max_tiles = tiles.max_tiles;
         Wb.alloc(max_tiles, BN, U, MIXED_SLICES, s);
@@ -1232,11 +1302,12 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         w.cs = Up;
         tc_gemm_tiled(Hs.view(), Wb.view(), w, (int)max_tiles, &st->tc_err, s);
     } else {
-        // tiles of 64 pairs of one A key, then (tile, 64 u, chunk of v) blocks
+        // tiles of 64 rows of one host A key, then (tile, 64 u, chunk of v) blocks
         if (!tiles.built) {
-            tiles.alloc(nA, nP, DM_BM, s);
-            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, cnt, DM_BM, (int)tiles.max_tiles, tiles.first,
-                       tiles.tile0, tiles.batch, tiles.col0, tiles.ncols);
+            tiles.alloc(nA, nP, DM_BM, true, s);
+            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, pairB.p, aKey.p, cnt, DM_BM,
+                       (int)tiles.max_tiles, tiles.first, tiles.tile0, tiles.batch, tiles.col0, tiles.ncols,
+                       tiles.rowPair, tiles.rowKey);
         }
         const i64 max_tiles = tiles.max_tiles;
         // the tile count is known on the device only: the split follows its bound
@@ -1250,8 +1321,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             parts.alloc(P * ps, s);
             dst = parts.p;
         }
-        dmma_launch(StageBOp{t.W.p, H.p, t.sidx.p, pairB.p, tiles.batch, tiles.col0, tiles.ncols, nS, U, Up, v_chunk,
-                             ps, dst},
+        dmma_launch(StageBOp{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch, tiles.col0, tiles.ncols,
+                             nS, U, Up, v_chunk, ps, dst},
                     dim3((unsigned)max_tiles, ub, (unsigned)P), s);
         if (P > 1) {
             launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
