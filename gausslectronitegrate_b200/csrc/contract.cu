@@ -628,7 +628,12 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
 }
 
 // Q[p][j] = sum_u H2[p][u] W[keyOf[j]][u] over the pairs and used keys (their
-// counts read on the device: blocks past them return at once)
+// counts read on the device: blocks past them return at once).  A class reads
+// Q at its pair (A key a, B key) and its largest key c >= a, and pairs are
+// ordered by A key, so the column tiles of a row tile start at the key of its
+// first A key: keys below it are never read (129 ERIDA keys: 166 blocks
+// instead of 396).  blockIdx.z selects a chunk of u; the chunks' partial
+// products go to separate slices of Q, summed by k_gather_q.
 template <int BN_>
 struct ProductOp {
     static constexpr bool A_KMAJOR = false, B_KMAJOR = false;
@@ -637,13 +642,18 @@ struct ProductOp {
     const double* H2;
     const double* W;
     const int* keyOf;
+    const int* pairA;
+    const int* aKey;
+    const uint64_t* kid;  // dense id of each used key
     const PlanCounts* cnt;
     i64 m;
-    int choice, U, Up, ldq;
+    int choice, U, Up, ldq, u_chunk;
+    i64 part_stride;
     double* Q;
     struct Block {
         int mvalid, nvalid, nk;
-        int m0, n0;
+        int m0, n0, u0, u1;
+        double* Q;
     };
     struct AState {
         i64 off[DM_BM / 16];
@@ -654,11 +664,16 @@ struct ProductOp {
     __device__ bool begin(Block& b) const {
         if (!choice_runs(choice, cnt, m)) return false;
         b.m0 = blockIdx.x * DM_BM;
-        b.n0 = blockIdx.y * BN;
         b.mvalid = min(DM_BM, (int)cnt->nP - b.m0);
+        if (b.mvalid <= 0) return false;
+        b.n0 = (int)kid[aKey[pairA[b.m0]]] + blockIdx.y * BN;
         b.nvalid = min(BN, (int)cnt->nku - b.n0);
-        b.nk = (U + DM_BK - 1) / DM_BK;
-        return b.mvalid > 0 && b.nvalid > 0;
+        if (b.nvalid <= 0) return false;
+        b.u0 = blockIdx.z * u_chunk;
+        b.u1 = min(U, b.u0 + u_chunk);
+        b.nk = (b.u1 - b.u0 + DM_BK - 1) / DM_BK;
+        b.Q = Q + (i64)blockIdx.z * part_stride;
+        return b.nk > 0;
     }
     __device__ void a_init(const Block& b, AState& st) const {
 #pragma unroll
@@ -677,8 +692,8 @@ struct ProductOp {
     // pairs (u, u + 1), u even: H2 and W rows start at multiples of Up (a
     // multiple of 4), so every pair is 16-byte aligned
     __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
-        const int k = dm_pair_k(threadIdx.x), u = kc * DM_BK + k;
-        const int bytes = dm_pair_bytes(u, U);
+        const int k = dm_pair_k(threadIdx.x), u = b.u0 + kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(u, b.u1);
 #pragma unroll
         for (int q = 0; q < DM_BM / 16; ++q) {
             const int n = st.off[q] >= 0 ? bytes : 0;
@@ -686,8 +701,8 @@ struct ProductOp {
         }
     }
     __device__ void b_issue(const Block& b, BState& st, int kc, double* tile) const {
-        const int k = dm_pair_k(threadIdx.x), u = kc * DM_BK + k;
-        const int bytes = dm_pair_bytes(u, U);
+        const int k = dm_pair_k(threadIdx.x), u = b.u0 + kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(u, b.u1);
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
             const int n = st.off[q] >= 0 ? bytes : 0;
@@ -696,15 +711,17 @@ struct ProductOp {
     }
     __device__ void store(const Block& b, int mm, int n, double v0, double v1) const {
         if (mm >= b.mvalid) return;
-        double* q = Q + (i64)(b.m0 + mm) * ldq + b.n0 + n;
+        double* q = b.Q + (i64)(b.m0 + mm) * ldq + b.n0 + n;
         if (n < b.nvalid) q[0] = v0;
         if (n + 1 < b.nvalid) q[1] = v1;
     }
 };
 
-// val[n] = Q[pair(n)][kid(k3)], the class's (pair, key) found from its packed keys
-__global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, const uint64_t* __restrict__ keys,
-                                                   i64 m, const uint64_t* __restrict__ kid, int nk,
+// val[n] = Q[pair(n)][kid(k3)], the class's (pair, key) found from its packed
+// keys, summed over the `parts` slices of Q in order (deterministic)
+__global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, int parts, i64 part_stride,
+                                                   const uint64_t* __restrict__ keys, i64 m,
+                                                   const uint64_t* __restrict__ kid, int nk,
                                                    const uint32_t* __restrict__ pairBits,
                                                    const uint64_t* __restrict__ pairPre, int ldq,
                                                    const PlanCounts* __restrict__ cnt, int choice,
@@ -734,7 +751,13 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             const i64 n = n0 + v * step;
-            if (n < m) out[n] = q[v] >= 0 ? Q[q[v]] : 0.0;
+            if (n >= m) continue;
+            double acc = 0.0;
+            if (q[v] >= 0) {
+                acc = Q[q[v]];
+                for (int z = 1; z < parts; ++z) acc += Q[z * part_stride + q[v]];
+            }
+            out[n] = acc;
         }
     }
 }
@@ -1311,6 +1334,8 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         }
         const i64 max_tiles = tiles.max_tiles;
         // the tile count is known on the device only: the split follows its bound
+        // (64 u per tile: 80-row K-major gathers measured slower, ERIDA 129^3
+        // stage B 0.32 against 0.21 ms)
         const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
         const int P = split_count(max_tiles * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
@@ -1340,14 +1365,26 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     const bool undecided = bounded && !product_host && m >= 65536;
     const int c_prod = undecided ? 1 : 0, c_class = undecided ? 2 : 0;
     if (undecided || product_host) {
-        DevBuf<double> Q(nP * nku, s);
         // 64-column tiles: the product's grid is small, and wider tiles cost it
-        // parallelism (ERIDA 129^3: 73 us with 80 columns, 66 us with 64)
-        const dim3 grid((unsigned)((nP + DM_BM - 1) / DM_BM), (unsigned)((nku + DM_BN - 1) / DM_BN));
-        dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, cnt, m, c_prod, U, Up, (int)nku, Q.p}, grid, s);
+        // parallelism (ERIDA 129^3: 73 us with 80 columns, 66 us with 64).  A
+        // grid under a wave splits u in two where the classes are few beside
+        // the product (each class then sums two slices: ERIDA 129^3 has 366,145
+        // classes and 1.08 million products; ERI 7^3's 3.57 million classes
+        // would pay more in the gather than the split saves)
+        const i64 mt = (nP + DM_BM - 1) / DM_BM, nt = (nku + DM_BN - 1) / DM_BN;
+        int u_chunk = U;
+        int P = std::min(2, split_count(mt * nt, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &u_chunk));
+        if (2 * m > nP * nku) P = 1;
+        u_chunk = ((U + P - 1) / P + DM_BK - 1) / DM_BK * DM_BK;
+        P = (U + u_chunk - 1) / u_chunk;
+        const i64 ps = nP * nku;
+        DevBuf<double> Q(P * ps, s);
+        dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up, (int)nku,
+                                  u_chunk, ps, Q.p},
+                    dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, keys.p, m, ids.p, (int)nk, pairBits.p, pairPre.p,
-                   (int)nku, cnt, c_prod, a.out);
+        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, m, ids.p, (int)nk, pairBits.p,
+                   pairPre.p, (int)nku, cnt, c_prod, a.out);
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
