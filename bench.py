@@ -600,7 +600,9 @@ def roofline(form, dom, st, plan, U, m, fp64_peak):
     it must move (int8 slices read, FP64 results written) against the measured
     HBM bandwidth.  The mixed form runs stage A on the tensor cores when
     nA nS >= 1e6, stage B when nA U^2 >= 4e6 and nP >= 80 nA (the library's
-    rule); plan = (nA, nP, used keys, stage C product flag) of the step."""
+    rule); plan = (nA, nP, used keys, stage C products) of the step: the
+    (pair, key) products the product GEMM computed, 0 when stage C ran per
+    class (one length-U dot product per class)."""
     nA, nP, nku, product = plan
     ms = st[dom]
     nS = lattice_nS(U)
@@ -609,7 +611,7 @@ def roofline(form, dom, st, plan, U, m, fp64_peak):
                                            (dom == "B" and nA * U * U >= 4000000 and nP >= 80 * nA))
     if not on_tensor_cores:
         flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U,
-                 "C": 2.0 * (nP * nku if product else m) * U}[dom]
+                 "C": 2.0 * (product if product else m) * U}[dom]
         kernel = {"A": "k_dmma<StageAOp>", "B": "k_dmma<StageBOp>",
                   "C": "k_dmma<ProductOp> + k_gather_q" if product else "k_stage_c"}[dom]
         achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None

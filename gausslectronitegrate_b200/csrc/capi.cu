@@ -244,7 +244,7 @@ int gli_b200_last_plan(glong out[4]) {
     out[0] = st.keys_a;
     out[1] = st.pairs;
     out[2] = st.keys_used;
-    out[3] = st.product;
+    out[3] = st.product ? std::max<i64>(1, st.products) : 0;
     return GLI_OK;
 }
 

@@ -650,6 +650,7 @@ struct ProductOp {
     int choice, U, Up, ldq, u_chunk;
     i64 part_stride;
     double* Q;
+    unsigned long long* products;  // count of the products computed (one add per tile)
     struct Block {
         int mvalid, nvalid, nk;
         int m0, n0, u0, u1;
@@ -673,6 +674,7 @@ struct ProductOp {
         b.u1 = min(U, b.u0 + u_chunk);
         b.nk = (b.u1 - b.u0 + DM_BK - 1) / DM_BK;
         b.Q = Q + (i64)blockIdx.z * part_stride;
+        if (threadIdx.x == 0 && blockIdx.z == 0) atomicAdd(products, (unsigned long long)b.mvalid * b.nvalid);
         return b.nk > 0;
     }
     __device__ void a_init(const Block& b, AState& st) const {
@@ -1107,8 +1109,9 @@ struct StageTimer {
 // status of one evaluation, read back by the host after the last kernel
 struct EvalStatus {
     PlanCounts cnt;
-    int bad;     // a class index outside the tensor
-    int tc_err;  // a tensor-core CTA gave up waiting
+    int bad;                      // a class index outside the tensor
+    int tc_err;                   // a tensor-core CTA gave up waiting
+    unsigned long long products;  // (pair, key) products that stage C's product GEMM computed
 };
 
 struct EvalArgs {
@@ -1380,7 +1383,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         const i64 ps = nP * nku;
         DevBuf<double> Q(P * ps, s);
         dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up, (int)nku,
-                                  u_chunk, ps, Q.p},
+                                  u_chunk, ps, Q.p, &st->products},
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
         launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, m, ids.p, (int)nk, pairBits.p,
@@ -1566,6 +1569,7 @@ static void check_status(int kind, i64 m, const EvalStatus& h, const LatticeTabl
     st.U = t.U;
     st.keys_used = h.cnt.nku;
     st.product = product_pays((double)h.cnt.nP, (double)h.cnt.nku, m) ? 1 : 0;
+    st.products = st.product ? (i64)h.products : 0;
     if (t_timing) {
         st.ms_tables = timer.between(0, 1);
         st.ms_a = timer.between(2, 3);

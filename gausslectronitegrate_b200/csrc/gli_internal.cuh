@@ -165,6 +165,7 @@ struct ContractStats {
     i64 keys_a = 0, pairs = 0, U = 0;
     i64 keys_used = 0;  // distinct axis keys of the class list
     int product = 0;    // stage C ran as the (pair, key) product GEMM
+    i64 products = 0;   // ... and computed this many (pair, key) products
     float ms_tables = 0, ms_a = 0, ms_b = 0, ms_c = 0;
 };
 

@@ -410,8 +410,9 @@ int gli_b200_kinetic_matrix_noalloc(const double* d_coeffs, glong num_coeffs,
 int gli_b200_last_stage_times(float ms[4], glong sizes[3]);
 
 /* Plan of the calling thread's last sparse evaluation: out[0] A keys, out[1]
- * (A, B) key pairs, out[2] distinct axis keys, out[3] 1 when stage C ran as
- * the (pair, key) product GEMM, 0 when per class. */
+ * (A, B) key pairs, out[2] distinct axis keys, out[3] the (pair, key) products
+ * that stage C computed as the product GEMM (at least 1 when it ran so), 0 when
+ * it ran per class. */
 int gli_b200_last_plan(glong out[4]);
 
 #ifdef __cplusplus

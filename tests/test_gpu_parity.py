@@ -164,6 +164,49 @@ def test_erida_values_sample_129(gli):
     assert_parity(val[pick], ref, what="ERIDA 129^3 sample")
 
 
+@pytest.mark.parametrize("L", [65, 101, 131])
+def test_erida_values_balanced_hosts(gli, L):
+    # full pair triangles of more than 64 A keys: stage B hosts each pair on
+    # either of its keys (65 and 101 keys: one regular tournament; 131 keys:
+    # 127 in a tournament, 4 hosting the rest); a seeded sample of classes
+    s = gli.compute_sparse_erida_gausslet_integrals(g10(), sym_grid(L), 1e-10)
+    idx, val = s.indices, s.values
+    assert idx.size == L * (L + 1) * (L + 2) // 6
+    pick = np.random.default_rng(L).choice(idx.size, size=150, replace=False)
+    ref = ORACLE.values("erida", g10(), sym_grid(L), idx[pick], 1e-10)
+    assert_parity(val[pick], ref, what=f"ERIDA {L}^3 sample")
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_erida_values_partial_triangle(gli, form):
+    # a class list whose pairs do not fill the triangle (no class whose two
+    # smallest displacement components are equal, so no pair (a, a)): stage B
+    # keeps each pair on its A key
+    import ctypes as C
+    from gausslectronitegrate_b200 import _abi
+    g = sym_grid(129)
+    N = 129 ** 3
+    full = gli.compute_sparse_erida_gausslet_integrals(g10(), g, 1e-10).indices
+    a, b = full // N, full % N
+    d = np.abs(np.stack([a // (129 * 129) - b // (129 * 129), (a // 129) % 129 - (b // 129) % 129,
+                         a % 129 - b % 129], 1))
+    ds = np.sort(d, axis=1)
+    idx = np.ascontiguousarray(full[ds[:, 0] != ds[:, 1]])
+    assert 0 < idx.size < full.size
+    vals = np.empty(idx.size)
+    gd, keep = gli._parse_coeffs(g10(), "")
+    rc = gli.lib().gli_b200_sparse_values(_abi.GLI_KIND_ERIDA, C.byref(gd), C.byref(gli._grid_struct(g)),
+                                          idx.ctypes.data_as(_abi.lptr), idx.size, 1e-10, form,
+                                          vals.ctypes.data_as(_abi.dptr))
+    assert rc == 0, gli.lib().gli_b200_last_error_message()
+    pick = np.random.default_rng(3).choice(idx.size, size=150, replace=False)
+    ref = ORACLE.values("erida", g10(), g, idx[pick], 1e-10)
+    if form == 0:
+        assert_parity(vals[pick], ref, what="ERIDA 129^3 partial triangle")
+    else:
+        assert np.max(np.abs(vals[pick] - ref)) <= 1e-8
+
+
 # --- golden fixtures of the reference test suite --------------------------------
 
 def test_fixture_eri_dense(gli):
