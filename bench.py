@@ -20,7 +20,10 @@ reported in Hartree.
 
 Timing: W >= 3 untimed warm-up steps; each timed step is bracketed by CUDA
 events on the stream the library launches on; L2 (126 MB) is flushed by
-writing a 256 MB buffer between timed steps (outside the events); the K steps
+writing a 1 GB buffer between timed steps (outside the events).  Each library
+call synchronises (it reads back the evaluation's status), so the flush, about
+160 us on the device, is also the host's lead for queueing the next step: a
+shorter flush let host latency into the timed events of small steps.  The K steps
 are bracketed by a barrier and device synchronisation, and the slowest rank's
 time counts.  N > 1 (torchrun, one process per GPU): every rank evaluates its
 own copy of the workload (weak scaling, no data-path collective).
@@ -289,7 +292,7 @@ def run_ours(args):
     enum_ms = e0.elapsed_time(e1)
     m = num.value
     out = torch.empty(m, dtype=torch.float64, device=f"cuda:{local}")
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     coeff_p = b.ctypes.data_as(_abi.dptr)
 
     def step(f):
@@ -430,7 +433,7 @@ def run_ours(args):
         "dtype": "f64" if chosen == "fp64" else "s8 tensor-core slices (int32 exact) + f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "classes": m, "form": chosen, "tol": TOL, "spacing_bohr": SPACING,
-                   "l2": "flushed between timed steps (256 MB write)",
+                   "l2": "flushed between timed steps (1 GB write)",
                    "max_abs_err_ha_mixed_vs_fp64": max_abs_err_ha,
                    "forms": {chosen: {"classes_per_s": main["value"], "ms_per_step": main["ms_per_step"]},
                              other: {"classes_per_s": side["value"], "ms_per_step": side["ms_per_step"]}},
@@ -602,13 +605,28 @@ def roofline(form, dom, st, plan, U, m, fp64_peak):
     nA nS >= 1e6, stage B when nA U^2 >= 4e6 and nP >= 80 nA (the library's
     rule); plan = (nA, nP, used keys, stage C products) of the step: the
     (pair, key) products the product GEMM computed, 0 when stage C ran per
-    class (one length-U dot product per class)."""
+    class (one length-U dot product per class).  A product-form stage C with
+    at least 8 classes per product is the class gather's HBM traffic (16 bytes
+    per class) against the measured HBM bandwidth."""
     nA, nP, nku, product = plan
     ms = st[dom]
     nS = lattice_nS(U)
     kp = (U + 63) // 64 * 64
     on_tensor_cores = form == "mixed" and ((dom == "A" and nA * nS >= 1000000) or
                                            (dom == "B" and nA * U * U >= 4000000 and nP >= 80 * nA))
+    if dom == "C" and product and m >= 8 * product:
+        # the product GEMM is small beside the class gather (ERI 7^3: 207k
+        # products for 3.57 million classes): the stage moves 8 bytes of packed
+        # keys in and 8 bytes of value out per class, the gather's HBM traffic
+        ms = st[dom]
+        bytes_ = 16.0 * m
+        achieved = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
+        peak = measured_peaks()["hbm_gbs"]
+        return {"bound": "hbm", "stage": dom, "kernel": "k_gather_q (+ k_dmma<ProductOp> in the stage time)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved and peak else None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "algorithmic_bytes_per_launch": bytes_, "products": product, "traffic": None}
     if not on_tensor_cores:
         flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U,
                  "C": 2.0 * (product if product else m) * U}[dom]
