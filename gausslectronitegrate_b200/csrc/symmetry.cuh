@@ -12,6 +12,7 @@ struct SymGrid {
     int e;   // extent: coordinates -e .. e
     int L;   // 2e + 1
     i64 N;   // L^3
+    const int* omin = nullptr;  // enumeration: smallest linear index among each point's 48 O_h images
 };
 
 __device__ inline i64 lin3(const SymGrid& G, const int q[3]) {

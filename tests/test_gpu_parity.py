@@ -35,11 +35,36 @@ def test_enumerate_erida_bit_exact(gli, L):
     assert s.num_entries == L * (L + 1) * (L + 2) // 6
 
 
+@pytest.mark.parametrize("mode", [None, "1", "live"])
 @pytest.mark.parametrize("L", [1, 3, 5])
-def test_enumerate_eri_bit_exact(gli, L):
+def test_enumerate_eri_bit_exact(gli, L, mode, monkeypatch):
+    # the one-pass enumeration over the live slots, the thread-per-slot two
+    # passes ("1") and the count and write passes over the live slots ("live")
+    if mode:
+        monkeypatch.setenv("GLI_B200_ENUM_TWO_PASS", mode)
     ref = core()[f"eri_idx_{L}"] if L in (3, 5) else ORACLE.enumerate("eri", sym_grid(L))
     s = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(L), 1e-3)
     assert np.array_equal(s.indices, ref)
+
+
+@pytest.mark.parametrize("kind,L", [("eri", 7), ("erida", 129)])
+def test_enumerate_one_pass_matches_two_pass(gli, kind, L, monkeypatch):
+    import ctypes as C
+    from gausslectronitegrate_b200 import _abi
+
+    def run():
+        gs = gli._grid_struct(sym_grid(L))
+        out = _abi.SparseIndices()
+        getattr(gli.lib(), f"enumerate_symmetry_reduced_{kind}_indices")(C.byref(gs), C.byref(out))
+        idx = np.ctypeslib.as_array(out.indices, shape=(out.num,)).copy()
+        getattr(gli.lib(), f"delete_sparse_{kind}_indices")(C.byref(out))
+        return idx
+
+    one = run()
+    for mode in ("1", "live"):
+        monkeypatch.setenv("GLI_B200_ENUM_TWO_PASS", mode)
+        two = run()
+        assert one.size == two.size and np.array_equal(one, two), mode
 
 
 def test_enumerate_eri_7_properties(gli):
