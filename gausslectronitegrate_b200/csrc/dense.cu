@@ -25,9 +25,9 @@
 // (the staged contraction computes it from exactly that), and every entry has
 // the key triple of its class.  The values are then scattered once into a
 // table indexed by the sorted key triple, and dense entries are generated by
-// key arithmetic and one table read.  The projection then generates each slab
-// of the first contraction directly as int8 slices and runs that contraction,
-// the O(N^4 M) one, on the tensor cores (FP64-level slicing).
+// key arithmetic and one table read.  The projection fills each slab of the
+// first contraction (the O(N^4 M) one) that way, in 32-bit arithmetic from a
+// point table, and contracts it on the FP64 tensor-core GEMM.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -35,7 +35,6 @@
 #include "dmma.cuh"
 #include "symmetry.cuh"
 #include "tables.cuh"
-#include "tc_gemm.cuh"
 
 namespace gli {
 
@@ -172,47 +171,33 @@ __global__ void k_fill_eri_rows_keyed(DenseGrid D, const double* __restrict__ ta
     }
 }
 
-// row r = (j k) of slab i of the sparse grid's tensor, column l (keyed lookup)
-struct KeyedSlabRows {
-    SymGrid G;
-    const double* table;
-    i64 i;
-    struct Ctx {
-        int p[3][3];  // points i, j, k of the row
-    };
-    __device__ Ctx row(i64 r) const {
-        Ctx c;
-        point_of(G, i, c.p[0]);
-        point_of(G, r / G.N, c.p[1]);
-        point_of(G, r % G.N, c.p[2]);
-        return c;
-    }
-    __device__ double at(const Ctx& c, int l) const {
-        int p[4][3];
-        for (int a = 0; a < 3; ++a) {
-            p[0][a] = c.p[0][a];
-            p[1][a] = c.p[1][a];
-            p[2][a] = c.p[2][a];
-        }
-        point_of(G, l, p[3]);
-        return table[eri_key_slot(p, G.L)];
-    }
-    __device__ bool valid(i64) const { return true; }
-    GLI_IDENTITY_ROWS
-};
+// points of a dense grid (x-major), for the slab fill
+__global__ void k_dense_points(DenseGrid D, short4* __restrict__ pt) {
+    const i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= D.N) return;
+    int p[3];
+    dense_point(D, n, p);
+    pt[n] = make_short4((short)p[0], (short)p[1], (short)p[2], 0);
+}
 
-// row s of the transpose of a row-major matrix with leading dimension ld
-struct TransposedRows {
-    const double* src;
-    i64 ld;
-    struct Ctx {
-        const double* p;
-    };
-    __device__ Ctx row(i64 r) const { return {src + r}; }
-    __device__ double at(const Ctx& c, int k) const { return c.p[(i64)k * ld]; }
-    __device__ bool valid(i64) const { return true; }
-    GLI_IDENTITY_ROWS
-};
+// slab i of the (i j k l) tensor, S[(j N + k) N + l] = V[i j k l], from the key
+// table (range L) of a complete list: 32-bit index arithmetic (N^3 < 2^32),
+// the points from a table, 32-bit axis keys, one entry per thread
+__global__ void __launch_bounds__(256) k_fill_slab_keyed(const short4* __restrict__ pt, uint32_t N, int L, short4 pi,
+                                                         const double* __restrict__ table, double* __restrict__ S) {
+    const uint32_t total = N * N * N;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const uint32_t row = e / N, l = e - row * N, j = row / N, k = row - j * N;
+        const short4 pj = pt[j], pk = pt[k], pl = pt[l];
+        int a = eri_axis_key32(pi.x - pj.x, pk.x - pl.x, (pi.x + pj.x) - (pk.x + pl.x), L);
+        int b = eri_axis_key32(pi.y - pj.y, pk.y - pl.y, (pi.y + pj.y) - (pk.y + pl.y), L);
+        int c = eri_axis_key32(pi.z - pj.z, pk.z - pl.z, (pi.z + pj.z) - (pk.z + pl.z), L);
+        if (a > b) { const int t = a; a = b; b = t; }
+        if (b > c) { const int t = b; b = c; c = t; }
+        if (a > b) { const int t = a; a = b; b = t; }
+        S[e] = table[tetra_index(a, b, c)];
+    }
+}
 
 // 48 x N permutation tables: perm[g][i] = linear index of O_h element g applied to point i
 __global__ void k_grid_perms(SymGrid G, int64_t* __restrict__ perm) {
@@ -237,10 +222,13 @@ struct MatView {
     i64 sb, r, c;
 };
 
-template <bool AK, bool BK>
+// BN_ = 32: products of at most 32 columns (B read row-major), whose 64-column
+// tiles would leave half the warps without columns
+template <bool AK, bool BK, int BN_ = DM_BN>
 struct StridedOp {
     static constexpr bool A_KMAJOR = AK, B_KMAJOR = BK;
-    static constexpr int BN = DM_BN;
+    static constexpr int BN = BN_;
+    static_assert(BN == DM_BN || (BN == 32 && !BK), "32-column tiles read B row-major");
     int M, N, K;
     MatView A, B;
     double* C;
@@ -257,9 +245,9 @@ struct StridedOp {
     struct BState {};
     __device__ bool begin(Block& b) const {
         b.m0 = blockIdx.y * DM_BM;
-        b.n0 = blockIdx.x * DM_BN;
+        b.n0 = blockIdx.x * BN;
         b.mvalid = min(DM_BM, M - b.m0);
-        b.nvalid = min(DM_BN, N - b.n0);
+        b.nvalid = min(BN, N - b.n0);
         b.nk = (K + DM_BK - 1) / DM_BK;
         b.a = A.p + (i64)blockIdx.z * A.sb + (i64)b.m0 * A.r;
         b.b = B.p + (i64)blockIdx.z * B.sb + (i64)b.n0 * B.c;
@@ -280,7 +268,7 @@ struct StridedOp {
     }
     __device__ void b_issue(const Block& b, BState&, int kc, double* tile) const {
 #pragma unroll
-        for (int q = 0; q < DM_ELEMS; ++q) {
+        for (int q = 0; q < BN * DM_BK / DM_THREADS; ++q) {
             const int r = BK ? dm_kmajor_row(threadIdx.x) : dm_rowmajor_row(threadIdx.x, q);
             const int k = BK ? dm_kmajor_k(threadIdx.x, q) : dm_rowmajor_k(threadIdx.x);
             const int kk = kc * DM_BK + k;
@@ -303,6 +291,16 @@ static void dgemm(int M, int N, int K, MatView A, MatView B, double* C, i64 csb,
     // stage an operand K-major when its row index is the unit-stride direction
     const bool ak = A.r == 1 && A.c != 1, bk = B.c == 1 && B.r != 1;
     const int acc = accumulate ? 1 : 0;
+    if (N <= 32) {
+        // one 32-column tile (the ERI projection's products onto 32 orbitals);
+        // B is small and read row-major
+        const dim3 g32(1, grid.y, batch);
+        if (ak)
+            dmma_launch(StridedOp<true, false, 32>{M, N, K, A, B, C, csb, cr, cc, acc}, g32, s);
+        else
+            dmma_launch(StridedOp<false, false, 32>{M, N, K, A, B, C, csb, cr, cc, acc}, g32, s);
+        return;
+    }
     if (ak && bk)
         dmma_launch(StridedOp<true, true>{M, N, K, A, B, C, csb, cr, cc, acc}, grid, s);
     else if (ak)
@@ -318,6 +316,8 @@ void dgemm_prepare() {
     dmma_prepare<StridedOp<true, false>>();
     dmma_prepare<StridedOp<false, true>>();
     dmma_prepare<StridedOp<false, false>>();
+    dmma_prepare<StridedOp<true, false, 32>>();
+    dmma_prepare<StridedOp<false, false, 32>>();
 }
 
 void dgemm_strided(int M, int N, int K, const double* A, i64 asb, i64 ar, i64 ac, const double* B, i64 bsb, i64 br,
@@ -498,44 +498,36 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
               M * M, 1, 1, false, s);
         return;
     }
-    // slab by slab over i: S[j][k][l] = V[i j k l]
+    // slab by slab over i: S[j][k][l] = V[i j k l], filled from the key table
+    // of a complete list (key arithmetic and one table read per entry) or by
+    // canonical lookups, then contracted on the FP64 tensor-core GEMM (ERI
+    // 7^3 onto 32 orbitals: the slab as FP64-level int8 slices on the tcgen05
+    // tensor cores took 0.44 s, dominated by writing the slices)
     const i64 per_i = N2 * N;
-    DevBuf<double> A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s);
+    DevBuf<double> A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s), S(per_i, s);
     KeyTable kt;
     build_key_table(G, g, d_idx, d_val, m, kt, s);
-    const bool tensor = kt.ok && N <= 8192 && N2 <= (i64)65535 * TC_BM;
-    DevBuf<double> S;
-    TiledSlices Ss, Bs;
-    DevBuf<int> err;
-    constexpr int BN = tile_n(FP64_SLICES);
-    if (tensor) {
-        // the basis as the B side: row s = column s of B (K = l)
-        Ss.alloc((N2 + TC_BM - 1) / TC_BM, TC_BM, (int)N, FP64_SLICES, s);
-        Bs.alloc((M + BN - 1) / BN, BN, (int)N, FP64_SLICES, s);
-        slice_tiled(TransposedRows{d_basis, M}, M, (int)N, Bs, s);
-        err.alloc(1, s);
-        err.zero();
-    } else {
-        S.alloc(per_i, s);
+    const bool slab32 = kt.ok && per_i < ((i64)1 << 32);
+    DevBuf<short4> pt;
+    std::vector<short4> hpt;
+    if (slab32) {
+        pt.alloc(N, s);
+        k_dense_points<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(D, pt.p);
+        GLI_CHECK_LAUNCH();
+        hpt.resize(N);
+        GLI_CUDA(cudaMemcpyAsync(hpt.data(), pt.p, N * sizeof(short4), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
     }
     for (i64 i = 0; i < N; ++i) {
-        // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-        if (tensor) {
-            slice_tiled(KeyedSlabRows{G, kt.t.p, i}, N2, (int)N, Ss, s);
-            TileWork w;
-            w.a_rows = (int)N2;
-            w.a_blocks = (int)((N2 + TC_BM - 1) / TC_BM);
-            w.n_total = (int)M;
-            w.C = A1.p;
-            w.rs = M;
-            w.cs = 1;
-            tc_gemm_tiled(Ss.view(), Bs.view(), w, (int)((M + BN - 1) / BN), err.p, s);
-        } else {
+        if (slab32)
+            k_fill_slab_keyed<<<grid_for(per_i), 256, 0, s>>>(pt.p, (uint32_t)N, (int)G.L, hpt[i], kt.t.p, S.p);
+        else if (kt.ok)
+            k_fill_eri_rows_keyed<<<grid_for(per_i), 256, 0, s>>>(D, kt.t.p, G.L, i * N, N, S.p);
+        else
             k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
-            GLI_CHECK_LAUNCH();
-            dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false,
-                  s);
-        }
+        GLI_CHECK_LAUNCH();
+        // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
+        dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false, s);
         // A2[j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j)
         dgemm((int)M, (int)M, (int)N, MatView{d_basis, 0, 1, M}, MatView{A1.p, N * M, M, 1}, A2.p, M * M, M, 1,
               (int)N, false, s);
@@ -546,12 +538,6 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     // E[p][(q r s)] = sum_i B[i][p] A3[i][(q r s)]
     dgemm((int)M, (int)(M * M * M), (int)N, MatView{d_basis, 0, 1, M}, MatView{A3.p, 0, M * M * M, 1}, d_out, 0,
           M * M * M, 1, 1, false, s);
-    if (tensor) {
-        int h = 0;
-        GLI_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-        GLI_CUDA(cudaStreamSynchronize(s));
-        if (h) fail(GLI_ERR_INTERNAL, "tensor-core projection: an mbarrier wait expired (code %d)", h);
-    }
 }
 
 }  // namespace gli

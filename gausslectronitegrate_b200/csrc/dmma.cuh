@@ -1,7 +1,7 @@
 // FP64 tensor-core tiles: mma.sync.m8n8k4.f64 over operand tiles that the
 // caller gathers into shared memory with 8-byte cp.async copies.
 //
-// A block (4 warps) computes a 64 x BN tile of C = A B (BN = 64 or 80, chosen
+// A block (4 warps) computes a 64 x BN tile of C = A B (BN = 32, 64 or 80, chosen
 // per Op) over K in chunks of 16, three chunks in flight (cp.async groups; the
 // waits are the hardware's own group waits, no flag spins).  Warp w owns the
 // 32 x BN/2 quadrant (w & 1, w >> 1) as 4 x BN/16 m8n8 accumulators; per
@@ -94,8 +94,8 @@ __device__ __forceinline__ double dm_frag(const double* s, int row0, int k0, int
 }
 
 // Op interface (all device, const):
-//   static constexpr bool A_KMAJOR, B_KMAJOR;  static constexpr int BN (64 or 80;
-//   K-major B tiles have 64 rows)
+//   static constexpr bool A_KMAJOR, B_KMAJOR;  static constexpr int BN (32, 64 or
+//   80; K-major B tiles have 64 rows)
 //   struct Block { int mvalid, nvalid, nk; ... };       the block's work item
 //   struct AState; struct BState;                       per-thread cached row data
 //   bool begin(Block&)                                  false: nothing to do (uniform)
@@ -145,7 +145,8 @@ __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Blo
 template <class Op>
 __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
     constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN);
-    static_assert(Op::BN == 64 || (Op::BN == 80 && !Op::B_KMAJOR), "column tiles of 64, or 80 read row-major");
+    static_assert(Op::BN == 64 || ((Op::BN == 80 || Op::BN == 32) && !Op::B_KMAJOR),
+                  "column tiles of 64, or 32 and 80 read row-major");
     extern __shared__ __align__(16) double dm_smem[];
     pdl_wait();  // the previous kernel's results are visible from here
     pdl_release();
