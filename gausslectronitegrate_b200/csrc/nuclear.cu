@@ -125,42 +125,38 @@ __global__ void __launch_bounds__(128) k_nuc_field(const NucInst* __restrict__ i
     }
 }
 
-// q = j / d for 0 <= j < 2^24, d >= 1: the single-precision estimate j * (1/d)
-// is within one of the quotient, and one correction step lands on it
-__device__ __forceinline__ int div_small(int j, int d, float inv) {
-    int q = __float2int_rz((float)j * inv);
-    const int r = j - q * d;
-    if (r < 0)
-        --q;
-    else if (r >= d)
-        ++q;
-    return q;
-}
-
 // V[i][j] of every instance from its key-indexed block: Vk[kx][ky * nkz + kz]
-// (zfast: the FP64 contractions) or Vk[kx][kz * nky + ky] (the sliced ones);
-// grid (row blocks, instance): a block writes whole rows i (coalesced).  The
-// coordinates of j come from two estimated divisions per element (every
-// instance has at most 256^3 = 2^24 points); the kernel writes 8 bytes per
-// element and is bound by its instructions, so they count.
+// (zfast: the FP64 contractions) or Vk[kx][kz * nky + ky] (the sliced ones).
+// Grid (x pairs, instance): block (ix, jx) writes the (ny nz) x (ny nz)
+// sub-block of rows ix nyz + (iy, iz) and columns jx nyz + (jy, jz), whose
+// entries all lie in the one slice kx = key(ix, jx) (nky nkz entries, read
+// from cache after the first touch; a whole row of V would read every slice,
+// more than L2 holds for a 24^3 instance).  A thread owns columns, decoded
+// once; rows run as (iy, iz) loops, so the inner loop has no division.
 __global__ void __launch_bounds__(256) k_nuc_scatter(const NucInst* __restrict__ inst, const double* __restrict__ Vk,
                                                      int zfast) {
     const NucInst& in = inst[blockIdx.y];
-    const int ny = in.n[1], nz = in.n[2], nky = in.nk[1], nkz = in.nk[2];
-    const int N = (int)in.N, nyz = ny * nz;
-    const float inv_nyz = 1.0f / (float)nyz, inv_nz = 1.0f / (float)nz;
-    const double* vk = Vk + in.vk_off;
-    for (int i = blockIdx.x; i < N; i += gridDim.x) {
-        const int iz = i % nz, iy = (i / nz) % ny, ix = i / nyz;
-        double* row = in.out + (i64)i * N;
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            const int jx = div_small(j, nyz, inv_nyz), t = j - jx * nyz;
-            const int jy = div_small(t, nz, inv_nz), jz = t - jy * nz;
-            const int ax = min(ix, jx), bx = max(ix, jx), ay = min(iy, jy), by = max(iy, jy);
-            const int az = min(iz, jz), bz = max(iz, jz);
-            const i64 kx = bx * (bx + 1) / 2 + ax;
-            const int ky = by * (by + 1) / 2 + ay, kz = bz * (bz + 1) / 2 + az;
-            row[j] = vk[kx * ((i64)nkz * nky) + (zfast ? ky * nkz + kz : kz * nky + ky)];
+    const int nx = in.n[0], ny = in.n[1], nz = in.n[2], nky = in.nk[1], nkz = in.nk[2];
+    const int nyz = ny * nz;
+    const i64 N = in.N;
+    const i64 sy = zfast ? nkz : 1, sz = zfast ? 1 : nky;  // strides of ky and kz in a slice
+    for (int pair = blockIdx.x; pair < nx * nx; pair += gridDim.x) {
+        const int ix = pair / nx, jx = pair - ix * nx;
+        const int ax = min(ix, jx), bx = max(ix, jx);
+        const double* slice = Vk + in.vk_off + (i64)(bx * (bx + 1) / 2 + ax) * ((i64)nky * nkz);
+        double* block = in.out + (i64)ix * nyz * N + (i64)jx * nyz;
+        for (int c = threadIdx.x; c < nyz; c += blockDim.x) {
+            const int jy = c / nz, jz = c - jy * nz;
+            double* col = block + c;
+            for (int iy = 0; iy < ny; ++iy) {
+                const int ay = min(iy, jy), by = max(iy, jy);
+                const double* sl = slice + (i64)(by * (by + 1) / 2 + ay) * sy;
+                double* out = col + (i64)iy * nz * N;
+                for (int iz = 0; iz < nz; ++iz) {
+                    const int az = min(iz, jz), bz = max(iz, jz);
+                    out[(i64)iz * N] = sl[(i64)(bz * (bz + 1) / 2 + az) * sz];
+                }
+            }
         }
     }
 }
@@ -336,7 +332,7 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
     const int ni = (int)hosts.size();
     i64 w_total = 0, phi_total = 0, vk_total = 0;
     int max_nk = 1, max_u = 1;
-    i64 max_rows = 1, max_n = 1;
+    i64 max_rows = 1;
     for (const NucHost& h : hosts) {
         for (int a = 0; a < 3; ++a) {
             w_total = std::max(w_total, h.d.w_off[a] + (i64)h.d.nk[a] * h.d.U[a]);
@@ -347,7 +343,6 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
         phi_total = std::max(phi_total, h.d.phi_off + cells);
         vk_total = std::max(vk_total, h.d.vk_off + (i64)h.d.nk[0] * h.d.nk[1] * h.d.nk[2]);
         max_rows = std::max(max_rows, (i64)h.d.U[0] * h.d.U[1]);
-        max_n = std::max(max_n, h.d.N);
     }
     DevBuf<double> W(w_total, s), Phi(phi_total, s), Vk(vk_total, s);
     k_nuc_weights<<<dim3((unsigned)((max_u + 127) / 128), (unsigned)max_nk, (unsigned)(3 * ni)), 128, 0, s>>>(
@@ -376,9 +371,10 @@ static void enqueue_chunk(const std::vector<NucHost>& hosts, const NucInst* d_in
         GLI_CUDA(cudaEventRecord(t_ring.events[k], t_ring.streams[k]));
         GLI_CUDA(cudaStreamWaitEvent(s, t_ring.events[k], 0));
     }
-    // rows per instance: enough blocks for every SM even when few instances are large
-    const unsigned sb = (unsigned)std::min<i64>(max_n, std::max<i64>(1, (i64)num_sms * 16));
-    k_nuc_scatter<<<dim3(sb, (unsigned)ni), 256, 0, s>>>(d_inst, Vk.p, sliced ? 0 : 1);
+    // one block per x pair (ix, jx) of the largest instance
+    i64 max_pairs = 1;
+    for (const NucHost& h : hosts) max_pairs = std::max<i64>(max_pairs, (i64)h.d.n[0] * h.d.n[0]);
+    k_nuc_scatter<<<dim3((unsigned)max_pairs, (unsigned)ni), 256, 0, s>>>(d_inst, Vk.p, sliced ? 0 : 1);
     GLI_CHECK_LAUNCH();
 }
 
