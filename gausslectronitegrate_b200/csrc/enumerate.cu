@@ -24,21 +24,25 @@
 // survivors in shared memory and sorts them (within a block ascending index is
 // the (slot, partner) order, and blocks cover increasing index ranges), then
 // appends them to a scratch buffer; a scan of the blocks' counts and a copy
-// place the runs in block order.
+// place the runs in block order.  129^3: 1.4 ms.
 //
-// ERI: at 7^3, 168,092 of the 40 million slots (i, j, k) hold a canonical
-// class, and a thread per slot leaves most lanes of a warp idle beside one
-// busy slot.  The slots that pass the filter are compacted first (k_eri_live);
-// a warp then takes each live slot's partner candidates 32 at a time in
-// ascending order, keeps the survivors (placed in order by its ballots) in
-// shared memory and appends them to a scratch buffer, and a scan of the
-// slots' counts and a copy place the runs (k_eri_slots_collect).  7^3: 25 ms
-// against 146 ms for a thread per slot in two passes.
+// ERI, live slots: at 7^3, 168,092 of the 40 million slots (i, j, k) hold a
+// canonical class, and a thread per slot leaves most lanes of a warp idle
+// beside one busy slot.  The slots that pass the filter are compacted first
+// (k_enum_live); a warp then takes each live slot's partner candidates 32 at
+// a time in ascending order, keeps the survivors (placed in order by its
+// ballots) in shared memory and appends them to a scratch buffer, and a scan
+// of the slots' counts and a copy place the runs (k_enum_slots_collect).  7^3:
+// 25 ms against 146 ms for a thread per slot in two passes.  (The same
+// scheme for ERIDA, whose live slots have only 27 cheap candidates each,
+// measured slower at 129^3: 3.6 against 1.4 ms; it serves the ERIDA tests of
+// the live-slot fallback.)
 //
-// Fallbacks, when a block's (ERIDA) or a slot's (ERI) survivors exceed its
-// shared buffer or the scratch buffer fills: two passes (count, exclusive
-// scan, write at each slot's offset), over the live slots for ERI, over every
-// slot for ERIDA.  The output is sorted by construction on every path.
+// Fallbacks, when a block's or a slot's survivors exceed its buffer or the
+// scratch buffer fills: two passes (count, scan, write), over the live slots
+// (k_enum_slots) for ERI and over every slot (k_enum_erida) for ERIDA.  The
+// thread-per-slot two passes of ERI (k_enum_eri) remain for the tests.  The
+// output is sorted by construction on every path.
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
@@ -197,14 +201,16 @@ __global__ void k_enum_eri(SymGrid G, uint32_t* __restrict__ counts, const uint6
 }
 
 // ---------------------------------------------------------------------------
-// one pass
-constexpr int ENUM_BLOCK = 128;  // slots per block
-constexpr int ENUM_CAP = 2048;   // survivors a block can hold (16 KB)
+// one pass (ERIDA: blocks of slots; ERI: live slots)
 
 struct EnumStatus {
     unsigned long long used;  // scratch entries reserved
-    int overflow;             // 1: a block's survivors exceeded ENUM_CAP; 2: the scratch buffer filled
+    int overflow;             // 1: a block's (or slot's) survivors exceeded its buffer; 2: the scratch buffer filled
 };
+
+// ERIDA in one pass: a thread per slot, survivors sorted per block
+constexpr int ENUM_BLOCK = 128;  // slots per block
+constexpr int ENUM_CAP = 2048;   // survivors a block can hold (16 KB)
 
 template <int KIND>
 __global__ void __launch_bounds__(ENUM_BLOCK) k_enum_collect(SymGrid G, i64 slots, int64_t* __restrict__ scratch,
@@ -262,8 +268,8 @@ __global__ void __launch_bounds__(ENUM_BLOCK) k_enum_collect(SymGrid G, i64 slot
     for (int k = threadIdx.x; k < cnt; k += ENUM_BLOCK) scratch[off + k] = buf[k];
 }
 
-// each block's run from the scratch buffer to its place (dest: exclusive scan
-// of the run lengths in block order); one warp per run
+// each slot's run from the scratch buffer to its place (dest: exclusive scan
+// of the run lengths in slot order); one warp per run
 __global__ void k_enum_place(const int64_t* __restrict__ scratch, const uint32_t* __restrict__ run_n,
                              const unsigned long long* __restrict__ run_off, const uint64_t* __restrict__ dest,
                              i64 runs, int64_t* __restrict__ out) {
@@ -278,10 +284,10 @@ __global__ void k_enum_place(const int64_t* __restrict__ scratch, const uint32_t
     }
 }
 
-// scratch entries for the one-pass enumeration: ERIDA lists have
-// L (L + 1) (L + 2) / 6 classes; ERI lists about N^4 / 3,900 at L = 7 (and a
-// falling fraction beyond), so N^4 / 1024 with a floor, at most 2^26 entries
-// (512 MB); a list that does not fit takes the two passes
+// scratch entries: ERIDA lists have L (L + 1) (L + 2) / 6 classes; ERI lists
+// about N^4 / 3,900 at L = 7 (and a falling fraction beyond), so N^4 / 1024
+// with a floor; at most 2^26 entries (512 MB); a list that does not fit takes
+// the two passes
 static i64 enum_scratch(int kind, const SymGrid& G) {
     const double L = G.L, N = (double)G.N;
     const double want = kind == 0 ? L * (L + 1) * (L + 2) / 6 + 1024 : N * N * N * N / 1024 + (1 << 20);
@@ -318,28 +324,30 @@ static bool enumerate_one_pass(const SymGrid& G, i64 slots, int64_t** d_out, i64
     return true;
 }
 
-// ---------------------------------------------------------------------------
-// ERI by live slots
+// can slot t hold a canonical class: the omin filter (ERIDA: i canonical;
+// ERI: also omin[j], omin[k] >= i) and for ERI the reference's x-ordering
+// (i_x <= j_x, i_x <= k_x)
+template <int KIND>
+__device__ inline bool slot_live(const SymGrid& G, i64 t) {
+    if (KIND == 0) return G.omin[t] == (int)t;
+    const i64 N = G.N;
+    const i64 i = t / (N * N), j = (t / N) % N, k = t % N;
+    if (G.omin[i] != (int)i || G.omin[j] < (int)i || G.omin[k] < (int)i) return false;
+    // x coordinate: the leading digit of the x-major linear index
+    const i64 LL = (i64)G.L * G.L;
+    const i64 xi = i / LL;
+    return xi <= j / LL && xi <= k / LL;
+}
 
-// slots (i, j, k) that can hold a canonical class: the omin filter and the
-// reference's x-ordering (i_x <= j_x, i_x <= k_x).  WRITE = false: live slots
-// per block of 256; WRITE = true: their ids at the block's offset, in order.
-template <bool WRITE>
-__global__ void __launch_bounds__(256) k_eri_live(SymGrid G, uint32_t* __restrict__ block_counts,
-                                                  const uint64_t* __restrict__ block_offsets,
-                                                  int64_t* __restrict__ slot_ids) {
+// WRITE = false: live slots per block of 256; WRITE = true: their ids at the
+// block's offset, in order
+template <int KIND, bool WRITE>
+__global__ void __launch_bounds__(256) k_enum_live(SymGrid G, i64 slots, uint32_t* __restrict__ block_counts,
+                                                   const uint64_t* __restrict__ block_offsets,
+                                                   int64_t* __restrict__ slot_ids) {
     __shared__ uint32_t wsum[8];
-    const i64 N = G.N, t = (i64)blockIdx.x * 256 + threadIdx.x;
-    bool live = false;
-    if (t < N * N * N) {
-        const i64 i = t / (N * N), j = (t / N) % N, k = t % N;
-        if (G.omin[i] == (int)i && G.omin[j] >= (int)i && G.omin[k] >= (int)i) {
-            // x coordinate: the leading digit of the x-major linear index
-            const i64 LL = (i64)G.L * G.L;
-            const i64 xi = i / LL;
-            live = xi <= j / LL && xi <= k / LL;
-        }
-    }
+    const i64 t = (i64)blockIdx.x * 256 + threadIdx.x;
+    const bool live = t < slots && slot_live<KIND>(G, t);
     const unsigned b = __ballot_sync(0xffffffffu, live);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) wsum[warp] = __popc(b);
@@ -355,6 +363,36 @@ __global__ void __launch_bounds__(256) k_eri_live(SymGrid G, uint32_t* __restric
     uint32_t before = 0;
     for (int w = 0; w < warp; ++w) before += wsum[w];
     if (live) slot_ids[block_offsets[blockIdx.x] + before + __popc(b & ((1u << lane) - 1u))] = t;
+}
+
+// The 27 partner candidates j of live ERIDA slot i (lane c = 9 tx + 3 ty + tz,
+// ascending j), emit(idx, rank) called by every lane after the ballot (idx < 0
+// for a lane without a survivor).  Returns the slot's survivors.
+template <class Emit>
+__device__ inline uint32_t erida_slot_walk(const SymGrid& G, i64 i, int lane, Emit&& emit) {
+    int p[2][3];
+    point_of(G, i, p[0]);
+    bool keep = false;
+    i64 idx = 0;
+    if (lane < 27) {
+        const int tx = lane / 9, ty = (lane / 3) % 3, tz = lane % 3;
+        p[1][0] = -p[0][0] - 1 + tx;
+        p[1][1] = -p[0][1] - 1 + ty;
+        p[1][2] = -p[0][2] - 1 + tz;
+        bool in = p[1][0] >= p[0][0];
+        for (int a = 0; a < 3; ++a) in = in && p[1][a] >= -G.e && p[1][a] <= G.e;
+        if (in) {
+            const i64 j = lin3(G, p[1]);
+            if (G.omin[j] >= (int)i) {
+                const int bias[3] = {tx - 1, ty - 1, tz - 1};
+                idx = i * G.N + j;
+                keep = canonical_pair(G, p, bias, idx);
+            }
+        }
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, keep);
+    emit(keep ? idx : (i64)-1, (uint32_t)__popc(b & ((1u << lane) - 1u)));
+    return (uint32_t)__popc(b);
 }
 
 // The partner candidates l of live slot t (ascending), 32 at a time, one per
@@ -409,17 +447,23 @@ __device__ inline uint32_t eri_slot_walk(const SymGrid& G, i64 t, int lane, Emit
     }
 }
 
+template <int KIND, class Emit>
+__device__ inline uint32_t slot_walk(const SymGrid& G, i64 t, int lane, Emit&& emit) {
+    if (KIND == 0) return erida_slot_walk(G, t, lane, emit);
+    return eri_slot_walk(G, t, lane, emit);
+}
+
 // one warp per live slot; WRITE = false: survivors per slot; WRITE = true:
 // survivors at the slot's offset, in order
-template <bool WRITE>
-__global__ void __launch_bounds__(256) k_eri_slots(SymGrid G, const int64_t* __restrict__ slot_ids, i64 nlive,
-                                                   uint32_t* __restrict__ counts,
-                                                   const uint64_t* __restrict__ offsets, int64_t* __restrict__ out) {
+template <int KIND, bool WRITE>
+__global__ void __launch_bounds__(256) k_enum_slots(SymGrid G, const int64_t* __restrict__ slot_ids, i64 nlive,
+                                                    uint32_t* __restrict__ counts,
+                                                    const uint64_t* __restrict__ offsets, int64_t* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
     for (i64 sl = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sl < nlive; sl += warps) {
         const uint64_t w = WRITE ? offsets[sl] : 0;
-        const uint32_t c = eri_slot_walk(G, slot_ids[sl], lane, [&](i64 idx, uint32_t rank) {
+        const uint32_t c = slot_walk<KIND>(G, slot_ids[sl], lane, [&](i64 idx, uint32_t rank) {
             if (WRITE && idx >= 0) out[w + rank] = idx;
         });
         if (!WRITE && lane == 0) counts[sl] = c;
@@ -432,17 +476,18 @@ __global__ void __launch_bounds__(256) k_eri_slots(SymGrid G, const int64_t* __r
 // the overflow status
 constexpr int ENUM_SLOT_CAP = 512;
 
-__global__ void __launch_bounds__(256) k_eri_slots_collect(SymGrid G, const int64_t* __restrict__ slot_ids,
-                                                           i64 nlive, int64_t* __restrict__ scratch,
-                                                           unsigned long long cap, uint32_t* __restrict__ run_n,
-                                                           unsigned long long* __restrict__ run_off,
-                                                           EnumStatus* __restrict__ st) {
+template <int KIND>
+__global__ void __launch_bounds__(256) k_enum_slots_collect(SymGrid G, const int64_t* __restrict__ slot_ids,
+                                                            i64 nlive, int64_t* __restrict__ scratch,
+                                                            unsigned long long cap, uint32_t* __restrict__ run_n,
+                                                            unsigned long long* __restrict__ run_off,
+                                                            EnumStatus* __restrict__ st) {
     __shared__ int64_t buf[8][ENUM_SLOT_CAP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
     int64_t* mine = buf[warp];
     for (i64 sl = (i64)blockIdx.x * (blockDim.x >> 5) + warp; sl < nlive; sl += warps) {
-        const uint32_t c = eri_slot_walk(G, slot_ids[sl], lane, [&](i64 idx, uint32_t rank) {
+        const uint32_t c = slot_walk<KIND>(G, slot_ids[sl], lane, [&](i64 idx, uint32_t rank) {
             if (idx >= 0 && rank < ENUM_SLOT_CAP) mine[rank] = idx;
         });
         __syncwarp();
@@ -463,12 +508,13 @@ __global__ void __launch_bounds__(256) k_eri_slots_collect(SymGrid G, const int6
 
 // collect = false: the count and write passes over the live slots (the
 // fallback of a slot with more survivors than a warp's buffer)
-static i64 enumerate_eri_live(const SymGrid& G, bool collect, int64_t** d_out, int num_sms, cudaStream_t s) {
-    const i64 slots = G.N * G.N * G.N;
+template <int KIND>
+static i64 enumerate_live(const SymGrid& G, bool collect, int64_t** d_out, int num_sms, cudaStream_t s) {
+    const i64 slots = KIND == 0 ? G.N : G.N * G.N * G.N;
     const i64 nb = (slots + 255) / 256;
     DevBuf<uint32_t> bc(nb, s);
     DevBuf<uint64_t> bo(nb, s);
-    k_eri_live<false><<<(unsigned)nb, 256, 0, s>>>(G, bc.p, nullptr, nullptr);
+    k_enum_live<KIND, false><<<(unsigned)nb, 256, 0, s>>>(G, slots, bc.p, nullptr, nullptr);
     GLI_CHECK_LAUNCH();
     const i64 nlive = exclusive_scan_u32(bc.p, bo.p, nb, s);
     int64_t* out = nullptr;
@@ -478,19 +524,19 @@ static i64 enumerate_eri_live(const SymGrid& G, bool collect, int64_t** d_out, i
         return 0;
     }
     DevBuf<int64_t> ids(nlive, s);
-    k_eri_live<true><<<(unsigned)nb, 256, 0, s>>>(G, nullptr, bo.p, ids.p);
+    k_enum_live<KIND, true><<<(unsigned)nb, 256, 0, s>>>(G, slots, nullptr, bo.p, ids.p);
     GLI_CHECK_LAUNCH();
     const unsigned grid = (unsigned)std::max<i64>(1, std::min<i64>((nlive + 7) / 8, (i64)num_sms * 16));
     if (collect) {
         // one pass: survivors kept per warp, appended to scratch, placed in slot order
-        const i64 cap = enum_scratch(1, G);
+        const i64 cap = enum_scratch(KIND, G);
         DevBuf<int64_t> scratch(cap, s);
         DevBuf<uint32_t> run_n(nlive, s);
         DevBuf<unsigned long long> run_off(nlive, s);
         DevBuf<EnumStatus> st(1, s);
         st.zero();
-        k_eri_slots_collect<<<grid, 256, 0, s>>>(G, ids.p, nlive, scratch.p, (unsigned long long)cap, run_n.p,
-                                                 run_off.p, st.p);
+        k_enum_slots_collect<KIND><<<grid, 256, 0, s>>>(G, ids.p, nlive, scratch.p, (unsigned long long)cap,
+                                                        run_n.p, run_off.p, st.p);
         GLI_CHECK_LAUNCH();
         DevBuf<uint64_t> dest(nlive, s);
         const i64 n = exclusive_scan_u32(run_n.p, dest.p, nlive, s);  // synchronises
@@ -505,14 +551,13 @@ static i64 enumerate_eri_live(const SymGrid& G, bool collect, int64_t** d_out, i
             return n;
         }
     }
-    // a slot with more survivors than a warp's buffer: count, scan, write
     DevBuf<uint32_t> counts(nlive, s);
     DevBuf<uint64_t> offsets(nlive, s);
-    k_eri_slots<false><<<grid, 256, 0, s>>>(G, ids.p, nlive, counts.p, nullptr, nullptr);
+    k_enum_slots<KIND, false><<<grid, 256, 0, s>>>(G, ids.p, nlive, counts.p, nullptr, nullptr);
     GLI_CHECK_LAUNCH();
     const i64 total = exclusive_scan_u32(counts.p, offsets.p, nlive, s);
     GLI_CUDA(cudaMallocAsync((void**)&out, (total > 0 ? total : 1) * sizeof(int64_t), s));
-    k_eri_slots<true><<<grid, 256, 0, s>>>(G, ids.p, nlive, nullptr, offsets.p, out);
+    k_enum_slots<KIND, true><<<grid, 256, 0, s>>>(G, ids.p, nlive, nullptr, offsets.p, out);
     GLI_CHECK_LAUNCH();
     *d_out = out;
     return total;
@@ -533,16 +578,17 @@ i64 enumerate_device(int kind, const GridDesc& g, int64_t** d_out, cudaStream_t 
     k_orbit_min<<<(unsigned)((G.N + 255) / 256), 256, 0, s>>>(G, omin.p);
     GLI_CHECK_LAUNCH();
     G.omin = omin.p;
-    // ERIDA in one pass, ERI by live slots in one pass.  For their tests,
-    // GLI_B200_ENUM_TWO_PASS selects the thread-per-slot two passes, and the
-    // value "live" the count and write passes over the live ERI slots.
+    // live slots in one pass.  For their tests, GLI_B200_ENUM_TWO_PASS selects
+    // the thread-per-slot two passes, and the value "live" the count and write
+    // passes over the live slots.
     const char* two = getenv("GLI_B200_ENUM_TWO_PASS");
     const bool live_two = two && strcmp(two, "live") == 0;
     if (!two || live_two) {
         const int sms = context().num_sms;
-        if (kind == 1) return enumerate_eri_live(G, !live_two, d_out, sms, s);
+        if (kind == 1) return enumerate_live<1>(G, !live_two, d_out, sms, s);
+        if (live_two) return enumerate_live<0>(G, false, d_out, sms, s);
         i64 total = 0;
-        if (!live_two && enumerate_one_pass<0>(G, slots, d_out, &total, sms, s)) return total;
+        if (enumerate_one_pass<0>(G, slots, d_out, &total, sms, s)) return total;
     }
     DevBuf<uint32_t> counts(slots, s);
     DevBuf<uint64_t> offsets(slots, s);
