@@ -199,6 +199,81 @@ __global__ void __launch_bounds__(256) k_fill_slab_keyed(const short4* __restric
     }
 }
 
+// A1[(j k)][s] = sum_l V[i j k l] B[l][s] for slab i of a complete list, the
+// slab never written out: each A element is computed from the key table as the
+// tile is staged (K-major A tiles: a thread keeps its row (j, k) and walks l),
+// B (the basis, at most 32 columns) read row-major.
+struct KeyedSlabOp {
+    static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
+    static constexpr int BN = 32;
+    const short4* pt;  // points of the grid
+    const double* table;
+    const double* basis;  // N x M row-major
+    double* C;            // N^2 x M row-major
+    short4 pi;
+    int N, L, M;
+    struct Block {
+        int mvalid, nvalid, nk;
+        int m0;
+    };
+    struct AState {
+        int d[3], s[3], k[3];  // pi - pj, pi + pj, pk per axis of this thread's row
+        bool ok;
+    };
+    struct BState {};
+    __device__ bool begin(Block& b) const {
+        b.m0 = blockIdx.x * DM_BM;
+        b.mvalid = min(DM_BM, N * N - b.m0);
+        b.nvalid = min(BN, M);
+        b.nk = (N + DM_BK - 1) / DM_BK;
+        return b.mvalid > 0;
+    }
+    __device__ void a_init(const Block& b, AState& st) const {
+        const int r = dm_kmajor_row(threadIdx.x);
+        st.ok = r < b.mvalid;
+        const int row = st.ok ? b.m0 + r : 0, j = row / N, k = row - j * N;
+        const short4 pj = pt[j], pk = pt[k];
+        st.d[0] = pi.x - pj.x, st.d[1] = pi.y - pj.y, st.d[2] = pi.z - pj.z;
+        st.s[0] = pi.x + pj.x, st.s[1] = pi.y + pj.y, st.s[2] = pi.z + pj.z;
+        st.k[0] = pk.x, st.k[1] = pk.y, st.k[2] = pk.z;
+    }
+    __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
+        const int r = dm_kmajor_row(threadIdx.x);
+#pragma unroll
+        for (int q = 0; q < DM_ELEMS; ++q) {
+            const int kq = dm_kmajor_k(threadIdx.x, q), l = kc * DM_BK + kq;
+            const bool v = st.ok && l < N;
+            const double* src = table;
+            if (v) {
+                const short4 pl = pt[l];
+                int a = eri_axis_key32(st.d[0], st.k[0] - pl.x, st.s[0] - (st.k[0] + pl.x), L);
+                int c = eri_axis_key32(st.d[1], st.k[1] - pl.y, st.s[1] - (st.k[1] + pl.y), L);
+                int e = eri_axis_key32(st.d[2], st.k[2] - pl.z, st.s[2] - (st.k[2] + pl.z), L);
+                if (a > c) { const int t = a; a = c; c = t; }
+                if (c > e) { const int t = c; c = e; e = t; }
+                if (a > c) { const int t = a; a = c; c = t; }
+                src = table + tetra_index(a, c, e);
+            }
+            dm_cp8(tile + dm_kmajor_at(r, kq), src, v);
+        }
+    }
+    __device__ void b_init(const Block&, BState&) const {}
+    __device__ void b_issue(const Block& b, BState&, int kc, double* tile) const {
+#pragma unroll
+        for (int q = 0; q < BN * DM_BK / DM_THREADS; ++q) {
+            const int n = dm_rowmajor_row(threadIdx.x, q), kq = dm_rowmajor_k(threadIdx.x), l = kc * DM_BK + kq;
+            const bool v = n < b.nvalid && l < N;
+            dm_cp8(tile + dm_rowmajor_at(n, kq), v ? basis + (i64)l * M + n : basis, v);
+        }
+    }
+    __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
+        if (m >= b.mvalid) return;
+        double* c = C + (i64)(b.m0 + m) * M + n;
+        if (n < b.nvalid) c[0] = v0;
+        if (n + 1 < b.nvalid) c[1] = v1;
+    }
+};
+
 // 48 x N permutation tables: perm[g][i] = linear index of O_h element g applied to point i
 __global__ void k_grid_perms(SymGrid G, int64_t* __restrict__ perm) {
     const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -504,10 +579,11 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     // 7^3 onto 32 orbitals: the slab as FP64-level int8 slices on the tcgen05
     // tensor cores took 0.44 s, dominated by writing the slices)
     const i64 per_i = N2 * N;
-    DevBuf<double> A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s), S(per_i, s);
+    DevBuf<double> A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s), S;
     KeyTable kt;
     build_key_table(G, g, d_idx, d_val, m, kt, s);
     const bool slab32 = kt.ok && per_i < ((i64)1 << 32);
+    if (!(slab32 && M <= 32)) S.alloc(per_i, s);
     DevBuf<short4> pt;
     std::vector<short4> hpt;
     if (slab32) {
@@ -518,16 +594,25 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
         GLI_CUDA(cudaMemcpyAsync(hpt.data(), pt.p, N * sizeof(short4), cudaMemcpyDeviceToHost, s));
         GLI_CUDA(cudaStreamSynchronize(s));
     }
+    // the first contraction with its slab computed as the GEMM stages it (at
+    // most 32 orbitals), or from a filled slab
+    const bool fused = slab32 && M <= 32;
     for (i64 i = 0; i < N; ++i) {
-        if (slab32)
-            k_fill_slab_keyed<<<grid_for(per_i), 256, 0, s>>>(pt.p, (uint32_t)N, (int)G.L, hpt[i], kt.t.p, S.p);
-        else if (kt.ok)
-            k_fill_eri_rows_keyed<<<grid_for(per_i), 256, 0, s>>>(D, kt.t.p, G.L, i * N, N, S.p);
-        else
-            k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
-        GLI_CHECK_LAUNCH();
-        // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-        dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false, s);
+        if (fused) {
+            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, d_basis, A1.p, hpt[i], (int)N, (int)G.L, (int)M},
+                        dim3((unsigned)((N2 + DM_BM - 1) / DM_BM)), s);
+        } else {
+            if (slab32)
+                k_fill_slab_keyed<<<grid_for(per_i), 256, 0, s>>>(pt.p, (uint32_t)N, (int)G.L, hpt[i], kt.t.p, S.p);
+            else if (kt.ok)
+                k_fill_eri_rows_keyed<<<grid_for(per_i), 256, 0, s>>>(D, kt.t.p, G.L, i * N, N, S.p);
+            else
+                k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
+            GLI_CHECK_LAUNCH();
+            // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
+            dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false,
+                  s);
+        }
         // A2[j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j)
         dgemm((int)M, (int)M, (int)N, MatView{d_basis, 0, 1, M}, MatView{A1.p, N * M, M, 1}, A2.p, M * M, M, 1,
               (int)N, false, s);
