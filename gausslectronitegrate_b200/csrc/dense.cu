@@ -25,9 +25,10 @@
 // (the staged contraction computes it from exactly that), and every entry has
 // the key triple of its class.  The values are then scattered once into a
 // table indexed by the sorted key triple, and dense entries are generated by
-// key arithmetic and one table read.  The projection fills each slab of the
-// first contraction (the O(N^4 M) one) that way, in 32-bit arithmetic from a
-// point table, and contracts it on the FP64 tensor-core GEMM.
+// key arithmetic and one table read.  The projection's first contraction (the
+// O(N^4 M) one) computes its slab that way inside the FP64 tensor-core GEMM
+// as it stages the operand tiles (KeyedSlabOp, at most 32 orbitals), or fills
+// the slab first (k_fill_slab_keyed) and contracts it.
 #include <algorithm>
 #include <map>
 #include <mutex>
