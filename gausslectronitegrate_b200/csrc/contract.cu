@@ -378,6 +378,7 @@ template <int BN_>
 struct StageAOp {
     static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
     static constexpr int BN = BN_;
+    static constexpr int STAGES = BN_ > 80 ? 2 : DM_STAGES;  // 144 columns: three blocks per SM
     static constexpr int NB = BN / 16;  // B element pairs per thread (rows of W are contiguous in t)
     const double* W;
     const double* T;
@@ -397,7 +398,9 @@ struct StageAOp {
         bool ok;
     };
     struct BState {
-        i64 off[NB];  // aKey * Up of this thread's rows, -1 past nA
+        // aKey * Up of this thread's rows, -1 past nA (32-bit for the 144-column
+        // tiles, whose registers are scarce: below 2^31 with at most 8,192 keys)
+        std::conditional_t<(BN_ > 80), int, i64> off[NB];
     };
     __device__ bool begin(Block& b) const {
         const int nA = (int)cnt->nA;
@@ -430,7 +433,7 @@ struct StageAOp {
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
             const int r = dm_pair_row(threadIdx.x, q);
-            st.off[q] = r < b.nvalid ? (i64)aKey[b.n0 + r] * Up : -1;
+            st.off[q] = r < b.nvalid ? aKey[b.n0 + r] * (decltype(st.off[q]))Up : -1;
         }
     }
     // pairs (t, t + 1), t even: W rows start at multiples of Up (a multiple of
@@ -1274,7 +1277,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         // small problems split the t loop so that enough blocks exist
         // (partial sums, then one summing pass)
         const unsigned mb = (unsigned)((nS + DM_BM - 1) / DM_BM);
-        const int bn = col_tile(nA);
+        const int bn = (nA > 128 && nA <= 144) ? 144 : col_tile(nA);
         const unsigned nb = (unsigned)((nA + bn - 1) / bn);
         int t_chunk = U;
         const int P = split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
@@ -1285,7 +1288,10 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             parts.alloc((i64)P * ps, s);
             dst = parts.p;
         }
-        if (bn == 80)
+        if (bn == 144)
+            dmma_launch(StageAOp<144>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
+                        dim3(mb, nb, (unsigned)P), s);
+        else if (bn == 80)
             dmma_launch(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
                         dim3(mb, nb, (unsigned)P), s);
         else
@@ -1460,6 +1466,7 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dgemm_prepare();
     dmma_prepare<StageAOp<64>>();
     dmma_prepare<StageAOp<80>>();
+    dmma_prepare<StageAOp<144>>();
     dmma_prepare<StageBOp>();
     dmma_prepare<ProductOp<64>>();
     const long long l0 = launch_count();

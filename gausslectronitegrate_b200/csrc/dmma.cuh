@@ -1,14 +1,17 @@
 // FP64 tensor-core tiles: mma.sync.m8n8k4.f64 over operand tiles that the
 // caller gathers into shared memory with 8-byte cp.async copies.
 //
-// A block (4 warps) computes a 64 x BN tile of C = A B (BN = 32, 64 or 80, chosen
-// per Op) over K in chunks of 16, three chunks in flight (cp.async groups; the
-// waits are the hardware's own group waits, no flag spins).  Warp w owns the
+// A block (4 warps) computes a 64 x BN tile of C = A B (BN = 32, 64, 80 or 144,
+// chosen per Op) over K in chunks of 16, three chunks in flight (two for an Op
+// that declares STAGES = 2: the 144-column tiles, so that three blocks still
+// fit on an SM; cp.async groups, the waits are the hardware's own group waits,
+// no flag spins).  Warp w owns the
 // 32 x BN/2 quadrant (w & 1, w >> 1) as 4 x BN/16 m8n8 accumulators; per
 // k-step of 4 it reads 4 A and BN/16 B fragments (one double each) for
 // 4 BN/16 MMAs of 256 FMAs.  BN = 80 serves 65..80 and 129..160 columns in
 // one and two column tiles (129 keys: 2 tiles instead of 3, measured 20%
-// faster on the stage A shape).
+// faster on the stage A shape); BN = 144 holds 129 keys in one tile (another
+// 1.5%: the lattice gathers are made once).
 //
 // The operand sources are arbitrary: an Op class says, per tile element, where
 // the double comes from (a strided matrix, a lattice-table gather, a gather
@@ -27,6 +30,7 @@
 #pragma once
 
 #include <atomic>
+#include <type_traits>
 
 #include "gli_internal.cuh"
 
@@ -40,9 +44,19 @@ static_assert(DM_TILE_A >= DM_BK * DM_LDR, "operand tile too small for the K-maj
 
 // doubles of a B tile of BN rows, and the shared memory of a launch
 __host__ __device__ constexpr int dm_tile_b(int bn) { return bn * DM_LDK; }
-__host__ __device__ constexpr int dm_smem(int bn) {
-    return DM_STAGES * (DM_TILE_A + dm_tile_b(bn)) * (int)sizeof(double);
+__host__ __device__ constexpr int dm_smem(int bn, int stages = DM_STAGES) {
+    return stages * (DM_TILE_A + dm_tile_b(bn)) * (int)sizeof(double);
 }
+
+// pipeline stages of an Op: Op::STAGES where it declares one, else DM_STAGES
+template <class Op, class = void>
+struct dm_stages_of {
+    static constexpr int value = DM_STAGES;
+};
+template <class Op>
+struct dm_stages_of<Op, std::void_t<decltype(Op::STAGES)>> {
+    static constexpr int value = Op::STAGES;
+};
 
 // Thread tid's q-th element of a rows x 16 operand tile:
 //   K-major (64 rows):  row = tid & 63,          k = (tid >> 6) + 2 q,  q < 8
@@ -94,8 +108,8 @@ __device__ __forceinline__ double dm_frag(const double* s, int row0, int k0, int
 }
 
 // Op interface (all device, const):
-//   static constexpr bool A_KMAJOR, B_KMAJOR;  static constexpr int BN (32, 64 or
-//   80; K-major B tiles have 64 rows)
+//   static constexpr bool A_KMAJOR, B_KMAJOR;  static constexpr int BN (32, 64,
+//   80 or 144; K-major B tiles have 64 rows); optionally STAGES (2 or 3)
 //   struct Block { int mvalid, nvalid, nk; ... };       the block's work item
 //   struct AState; struct BState;                       per-thread cached row data
 //   bool begin(Block&)                                  false: nothing to do (uniform)
@@ -111,20 +125,20 @@ template <class Op, bool FULL>
 __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Block& blk, typename Op::AState& as,
                                             typename Op::BState& bs, double* smem, int wm, int wn, int mt, int nt,
                                             double (&acc)[4][Op::BN / 16][2]) {
-    constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN);
+    constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN), NS = dm_stages_of<Op>::value;
     const int lane = threadIdx.x & 31;
     const int nk = blk.nk;
     for (int kc = 0; kc < nk; ++kc) {
-        dm_wait<DM_STAGES - 2>();  // chunk kc has landed (this thread's copies)
-        __syncthreads();           // ... everyone's; and chunk kc - 1 is consumed
-        const int nx = kc + DM_STAGES - 1;
+        dm_wait<NS - 2>();  // chunk kc has landed (this thread's copies)
+        __syncthreads();    // ... everyone's; and chunk kc - 1 is consumed
+        const int nx = kc + NS - 1;
         if (nx < nk) {
-            const int st = nx % DM_STAGES;
+            const int st = nx % NS;
             op.a_issue(blk, as, nx, smem + st * STAGE);
             op.b_issue(blk, bs, nx, smem + st * STAGE + DM_TILE_A);
         }
         dm_commit();
-        const double* a_s = smem + (kc % DM_STAGES) * STAGE;
+        const double* a_s = smem + (kc % NS) * STAGE;
         const double* b_s = a_s + DM_TILE_A;
 #pragma unroll
         for (int k0 = 0; k0 < DM_BK; k0 += 4) {
@@ -144,9 +158,10 @@ __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Blo
 
 template <class Op>
 __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
-    constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN);
-    static_assert(Op::BN == 64 || ((Op::BN == 80 || Op::BN == 32) && !Op::B_KMAJOR),
-                  "column tiles of 64, or 32 and 80 read row-major");
+    constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN), NS = dm_stages_of<Op>::value;
+    static_assert(Op::BN == 64 || ((Op::BN == 80 || Op::BN == 32 || Op::BN == 144) && !Op::B_KMAJOR),
+                  "column tiles of 64, or 32, 80 and 144 read row-major");
+    static_assert(NS >= 2 && NS <= 3, "two or three stages");
     extern __shared__ __align__(16) double dm_smem[];
     pdl_wait();  // the previous kernel's results are visible from here
     pdl_release();
@@ -159,7 +174,7 @@ __global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
     op.a_init(blk, as);
     op.b_init(blk, bs);
 #pragma unroll
-    for (int st = 0; st < DM_STAGES - 1; ++st) {
+    for (int st = 0; st < NS - 1; ++st) {
         if (st < blk.nk) {
             op.a_issue(blk, as, st, dm_smem + st * STAGE);
             op.b_issue(blk, bs, st, dm_smem + st * STAGE + DM_TILE_A);
@@ -198,7 +213,8 @@ void dmma_prepare() {
     GLI_CUDA(cudaGetDevice(&dev));
     const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
     if (bit && (done.load() & bit)) return;
-    GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, dm_smem(Op::BN)));
+    GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  dm_smem(Op::BN, dm_stages_of<Op>::value)));
     done.fetch_or(bit);
 }
 
@@ -207,7 +223,7 @@ template <class Op>
 void dmma_launch(const Op& op, dim3 grid, cudaStream_t s) {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
     dmma_prepare<Op>();
-    launch_pdl(k_dmma<Op>, grid, dim3(DM_THREADS), dm_smem(Op::BN), s, op);
+    launch_pdl(k_dmma<Op>, grid, dim3(DM_THREADS), dm_smem(Op::BN, dm_stages_of<Op>::value), s, op);
 }
 
 }  // namespace gli
