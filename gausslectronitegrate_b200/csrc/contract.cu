@@ -380,6 +380,9 @@ struct StageAOp {
     static constexpr int BN = BN_;
     static constexpr int STAGES = BN_ > 80 ? 2 : DM_STAGES;  // 144 columns: three blocks per SM
     static constexpr int NB = BN / 16;  // B element pairs per thread (rows of W are contiguous in t)
+    // W row offsets: 32-bit for the 144-column tiles, whose registers are
+    // scarce (aKey * Up < 2^31 with at most 8,192 keys)
+    using Off = std::conditional_t<(BN_ > 80), int, i64>;
     const double* W;
     const double* T;
     const int* S;
@@ -398,9 +401,7 @@ struct StageAOp {
         bool ok;
     };
     struct BState {
-        // aKey * Up of this thread's rows, -1 past nA (32-bit for the 144-column
-        // tiles, whose registers are scarce: below 2^31 with at most 8,192 keys)
-        std::conditional_t<(BN_ > 80), int, i64> off[NB];
+        Off off[NB];  // aKey * Up of this thread's rows, -1 past nA
     };
     __device__ bool begin(Block& b) const {
         const int nA = (int)cnt->nA;
@@ -433,7 +434,7 @@ struct StageAOp {
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
             const int r = dm_pair_row(threadIdx.x, q);
-            st.off[q] = r < b.nvalid ? aKey[b.n0 + r] * (decltype(st.off[q]))Up : -1;
+            st.off[q] = r < b.nvalid ? (Off)aKey[b.n0 + r] * (Off)Up : (Off)-1;
         }
     }
     // pairs (t, t + 1), t even: W rows start at multiples of Up (a multiple of
