@@ -464,9 +464,14 @@ struct StageAOp {
 // as B, gathered through sidx straight from H (no expanded copy in memory).
 // The sidx values of the next chunk are loaded one chunk ahead, so the
 // dependent gathers do not wait on them.
+// DEEP = false: two pipeline stages and four blocks per SM (at most 128
+// registers), for grids of several waves (ERIDA 129^3: 199 against 213 us);
+// small grids keep three stages (ERIDA 33^3: 20.5 against 22.5 us)
+template <bool DEEP>
 struct StageBOp {
     static constexpr bool A_KMAJOR = false, B_KMAJOR = true;
     static constexpr int BN = DM_BN;
+    static constexpr int STAGES = DEEP ? 3 : 2, MIN_BLOCKS = DEEP ? 3 : 4;
     const double* W;
     const double* H;
     const int* sidx;
@@ -1356,9 +1361,15 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
             parts.alloc(P * ps, s);
             dst = parts.p;
         }
-        dmma_launch(StageBOp{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch, tiles.col0, tiles.ncols,
-                             nS, U, Up, v_chunk, ps, dst},
-                    dim3((unsigned)max_tiles, ub, (unsigned)P), s);
+        const dim3 grid((unsigned)max_tiles, ub, (unsigned)P);
+        if ((i64)max_tiles * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
+            dmma_launch(StageBOp<false>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch, tiles.col0,
+                                        tiles.ncols, nS, U, Up, v_chunk, ps, dst},
+                        grid, s);
+        else
+            dmma_launch(StageBOp<true>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch, tiles.col0,
+                                       tiles.ncols, nS, U, Up, v_chunk, ps, dst},
+                        grid, s);
         if (P > 1) {
             launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
                        s, parts.p, P, ps, H2.p);
@@ -1468,7 +1479,8 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<64>>();
     dmma_prepare<StageAOp<80>>();
     dmma_prepare<StageAOp<144>>();
-    dmma_prepare<StageBOp>();
+    dmma_prepare<StageBOp<true>>();
+    dmma_prepare<StageBOp<false>>();
     dmma_prepare<ProductOp<64>>();
     const long long l0 = launch_count();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));

@@ -156,8 +156,18 @@ __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Blo
     }
 }
 
+// blocks per SM a launch is compiled for: Op::MIN_BLOCKS where declared, else 3
+template <class Op, class = void>
+struct dm_blocks_of {
+    static constexpr int value = 3;
+};
 template <class Op>
-__global__ void __launch_bounds__(DM_THREADS, 3) k_dmma(const Op op) {
+struct dm_blocks_of<Op, std::void_t<decltype(Op::MIN_BLOCKS)>> {
+    static constexpr int value = Op::MIN_BLOCKS;
+};
+
+template <class Op>
+__global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(const Op op) {
     constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN), NS = dm_stages_of<Op>::value;
     static_assert(Op::BN == 64 || ((Op::BN == 80 || Op::BN == 32 || Op::BN == 144) && !Op::B_KMAJOR),
                   "column tiles of 64, or 32, 80 and 144 read row-major");
