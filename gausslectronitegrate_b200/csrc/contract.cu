@@ -647,6 +647,7 @@ template <int BN_>
 struct ProductOp {
     static constexpr bool A_KMAJOR = false, B_KMAJOR = false;
     static constexpr int BN = BN_;
+    static constexpr int STAGES = 2, MIN_BLOCKS = 4;  // four blocks per SM: a grid under a wave splits u in three
     static constexpr int NB = BN / 16;  // B element pairs per thread
     const double* H2;
     const double* W;
@@ -1388,13 +1389,15 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     if (undecided || product_host) {
         // 64-column tiles: the product's grid is small, and wider tiles cost it
         // parallelism (ERIDA 129^3: 73 us with 80 columns, 66 us with 64).  A
-        // grid under a wave splits u in two where the classes are few beside
-        // the product (each class then sums two slices: ERIDA 129^3 has 366,145
-        // classes and 1.08 million products; ERI 7^3's 3.57 million classes
-        // would pay more in the gather than the split saves)
+        // grid under a wave (four blocks per SM; about half the column tiles
+        // are active after the A-key shift) splits u in up to three where the
+        // classes are few beside the product (each class then sums the slices:
+        // ERIDA 129^3 has 366,145 classes and 1.08 million products, 45 us
+        // against 47 with two slices; ERI 7^3's 3.57 million classes would pay
+        // more in the gather than the split saves)
         const i64 mt = (nP + DM_BM - 1) / DM_BM, nt = (nku + DM_BN - 1) / DM_BN;
         int u_chunk = U;
-        int P = std::min(2, split_count(mt * nt, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &u_chunk));
+        int P = std::min(3, split_count(mt * ((nt + 1) / 2), U, DM_BK, 4 * (i64)a.num_sms, &u_chunk));
         if (2 * m > nP * nku) P = 1;
         u_chunk = ((U + P - 1) / P + DM_BK - 1) / DM_BK * DM_BK;
         P = (U + u_chunk - 1) / u_chunk;
