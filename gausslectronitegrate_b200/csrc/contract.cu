@@ -884,7 +884,7 @@ __device__ __forceinline__ int bal_partner(int h, int j, int n, int y) {
 // are the pairs in order, each hosted by its A key.
 // (pairA, pairB and aKey may have been written earlier in the same kernel:
 // plain coherent loads, no __restrict__)
-__device__ void pair_tiles_block(const int* pairA, const int* pairB, const int* aKey, int nP, int nA, int nku, int bn, int max_tiles,
+__device__ void pair_tiles_block(bool first_ready, const int* pairA, const int* pairB, const int* aKey, int nP, int nA, int nku, int bn, int max_tiles,
                                  int* __restrict__ first, int* __restrict__ tile0, int* __restrict__ tile_batch,
                                  int* __restrict__ tile_col0, int* __restrict__ tile_ncols, int* __restrict__ rowPair,
                                  int* __restrict__ rowKey) {
@@ -893,9 +893,11 @@ __device__ void pair_tiles_block(const int* pairA, const int* pairB, const int* 
     if (threadIdx.x == 0) carry = 0;
     for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;
     // every A key has at least one pair, and pairs are sorted by A key: the
-    // first pair of each key is where the key changes
-    for (int p = threadIdx.x; p < nP; p += blockDim.x)
-        if (p == 0 || pairA[p] != pairA[p - 1]) first[pairA[p]] = p;
+    // first pair of each key is where the key changes (unless the caller
+    // filled first[] already)
+    if (!first_ready)
+        for (int p = threadIdx.x; p < nP; p += blockDim.x)
+            if (p == 0 || pairA[p] != pairA[p - 1]) first[pairA[p]] = p;
     const bool balanced = rowPair && nA > bn && nku == nA && (i64)nP == (i64)nA * (nA + 1) / 2;
     const int y = min(nA, 2 * bn - 1);
     if (rowPair) {
@@ -972,8 +974,8 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
                                                       int* __restrict__ rowPair, int* __restrict__ rowKey) {
     pdl_wait();
     pdl_release();
-    pair_tiles_block(pairA, pairB, aKey, (int)cnt->nP, (int)cnt->nA, (int)cnt->nku, bn, max_tiles, first, tile0,
-                     tile_batch, tile_col0, tile_ncols, rowPair, rowKey);
+    pair_tiles_block(false, pairA, pairB, aKey, (int)cnt->nP, (int)cnt->nA, (int)cnt->nku, bn, max_tiles, first,
+                     tile0, tile_batch, tile_col0, tile_ncols, rowPair, rowKey);
 }
 
 // the tile arrays of one stage B launch: first pair and first tile of every A
@@ -1000,10 +1002,13 @@ struct PairTiles {
     }
 };
 
-// Bounded plans with at most 512 key flags and 8,192 pair-bitmap words: the
-// key plan, the pair plan and the stage-B tiles in one single-block launch
+// Bounded plans (at most 256 keys: 512 key flags, 2,048 pair-bitmap words):
+// the key plan, the pair plan and the stage-B tiles in one single-block launch
 // (three phases separated by block barriers; the global writes of a phase
-// are visible to the next).
+// are visible to the next).  The pair bitmap, its word prefixes and the A ids
+// stay in shared memory for the pair placement (a thread per slot) and for the
+// first pair of each A key (the count of set bits before its row).
+constexpr int PLAN_SMALL_KEYS = 256, PLAN_SMALL_WORDS = PLAN_SMALL_KEYS * PLAN_SMALL_KEYS / 32;
 __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __restrict__ used,
                                                      uint64_t* __restrict__ ids, int* __restrict__ keyOf,
                                                      int* __restrict__ aId, int* __restrict__ aKey, i64 words,
@@ -1016,6 +1021,8 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
     pdl_wait();
     pdl_release();
     __shared__ uint32_t ws[32], total, nku_s;
+    __shared__ uint32_t s_bits[PLAN_SMALL_WORDS], s_pre[PLAN_SMALL_WORDS];
+    __shared__ int s_aId[PLAN_SMALL_KEYS], s_aKey[PLAN_SMALL_KEYS];
     // keys: joint scan of [usedKey | usedA]
     const int k = threadIdx.x;  // flag k of 2 nk (<= 512)
     const uint32_t f = k < 2 * nk ? used[k] : 0u;
@@ -1035,6 +1042,8 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
         const int a = (int)(ex - nku);
         aId[k - nk] = a;
         aKey[a] = (int)(k - nk);
+        s_aId[k - nk] = a;
+        s_aKey[a] = (int)(k - nk);
     }
     __syncthreads();
     // pairs: per-word exclusive counts, then every set bit placed in parallel
@@ -1043,7 +1052,11 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
         const i64 w = base + threadIdx.x;
         const uint32_t b = w < words ? bits[w] : 0u;
         const uint32_t id = carry + block_scan_1024(__popc(b), ws, &total);
-        if (w < words) pre[w] = id;
+        if (w < words) {
+            pre[w] = id;
+            s_bits[w] = b;
+            s_pre[w] = id;
+        }
         carry += total;
         __syncthreads();  // total and ws are rewritten by the next tile's scan
     }
@@ -1051,17 +1064,23 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
     if (threadIdx.x == 0) cnt->nP = nP;
     const int slots = (int)(nk * nk);
     for (int slot = threadIdx.x; slot < slots; slot += blockDim.x) {
-        const uint32_t b = bits[slot >> 5];
+        const uint32_t b = s_bits[slot >> 5];
         if (!((b >> (slot & 31)) & 1u)) continue;
-        const int id = (int)pre[slot >> 5] + __popc(b & ((1u << (slot & 31)) - 1u));
+        const int id = (int)s_pre[slot >> 5] + __popc(b & ((1u << (slot & 31)) - 1u));
         const int k2 = slot / (int)nk;
-        pairA[id] = aId[k2];
+        pairA[id] = s_aId[k2];
         pairB[id] = slot - k2 * (int)nk;
     }
+    // the first pair of A key a: the set bits before row aKey[a]
+    if (first)
+        for (int a = threadIdx.x; a < nA; a += blockDim.x) {
+            const int slot = s_aKey[a] * (int)nk, w = slot >> 5;
+            first[a] = (int)s_pre[w] + __popc(s_bits[w] & ((1u << (slot & 31)) - 1u));
+        }
     __syncthreads();
     if (first)
-        pair_tiles_block(pairA, pairB, aKey, nP, nA, (int)nku, bn, max_tiles, first, tile0, tile_batch, tile_col0,
-                         tile_ncols, rowPair, rowKey);
+        pair_tiles_block(true, pairA, pairB, aKey, nP, nA, (int)nku, bn, max_tiles, first, tile0, tile_batch,
+                         tile_col0, tile_ncols, rowPair, rowKey);
 }
 
 // G sliced once per table set (cached with the tables); the build synchronises
@@ -1209,7 +1228,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         // pairs (A, B) have A >= B; every class has one pair
         sz.nP = std::min(nk * (nk + 1) / 2, m);
     }
-    if (small_pairs && 2 * nk <= 1024) {
+    if (small_pairs && nk <= PLAN_SMALL_KEYS) {
         // the whole plan and stage B's tiles in one launch (bounded plans; for
         // the larger key spaces of exact plans the single block's pass over
         // nk^2 pair slots measured no faster than the multi-block path: ERI
