@@ -1,20 +1,22 @@
 """Benchmark of the integral hot path on B200.
 
-Workload (the metric's configuration): ERIDA classes of a "32^3" grid at
-spacing 0.5 bohr -- the reference's symmetry-reduced path needs the odd
-rotationally symmetric grid, so the 33^3 grid (-16, 33)^3 with its 6,545
-symmetry-reduced classes stands in for it; G10 gausslet coefficients, tol
-1e-16, values scaled by 1/spacing = 2 to Hartree.  Synthetic: the inputs are
-the coefficients and the grid.
+Workload (the metric's configuration, "ERI classes/sec ... mixed vs FP64
+form"): ERI classes of the 6x6x6 configuration at spacing 0.7 bohr.  The
+reference's symmetry-reduced path needs the odd rotationally symmetric grid, so
+the 7^3 grid (-3, 7)^3 with its 3,571,977 symmetry-reduced classes stands in for
+it; G10 gausslet coefficients, tol 1e-16, values scaled by 1/spacing to
+Hartree.  Synthetic: the inputs are the coefficients and the grid.
 
 One step = one evaluation of every class value from the class list already
-resident in HBM (tables, staged contraction, write-back), i.e. one
-gli_b200_sparse_values_dev call.  The class enumeration is measured apart.
-The metric compares the two forms: `value` is the chosen form (--form, default
-mixed: the bulk lattice stages as int8-sliced products on the tensor cores);
-the other form is timed the same way beside it, and the mixed form's max abs
-error against the FP64 form (and both against the reference C core) is
-reported in Hartree.
+resident in HBM (plan, staged contraction, write-back), i.e. one
+gli_b200_sparse_values_dev call with the lattice tables cached.  The class
+enumeration is measured apart, and so is a cold step (caches dropped: tables,
+plan and graph built again inside the timed call).  The metric compares the
+two forms: `value` is the chosen form (--form, default mixed); the other form
+is timed the same way beside it, and the mixed form's max abs error against
+the FP64 form (and both against the reference C core on a seeded sample) is
+reported in Hartree.  `dtype` names the arithmetic that ran, per stage, as the
+library reports it (gli_b200_last_paths).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64] [--impl ours|reference]
 
@@ -22,21 +24,23 @@ Timing: W >= 3 untimed warm-up steps; each timed step is bracketed by CUDA
 events on the stream the library launches on; L2 (126 MB) is flushed by
 writing a 1 GB buffer between timed steps (outside the events).  Each library
 call synchronises (it reads back the evaluation's status), so the flush, about
-160 us on the device, is also the host's lead for queueing the next step: a
-shorter flush let host latency into the timed events of small steps.  The K steps
-are bracketed by a barrier and device synchronisation, and the slowest rank's
-time counts.  N > 1 (torchrun, one process per GPU): every rank evaluates its
-own copy of the workload (weak scaling, no data-path collective).
+160 us on the device, is also the host's lead for queueing the next step.  The K
+steps are bracketed by a barrier and device synchronisation, and the slowest
+rank's time counts.  N > 1 (torchrun, one process per GPU): every rank
+evaluates its own copy of the workload (weak scaling, no data-path
+collective); --shard splits one class list into contiguous ranges over the
+ranks and gathers the values (strong scaling, NCCL all-gather).
 
-Other hot-path configurations (--workload): erida129 (ERIDA 128^3, odd
-stand-in 129^3, spacing 0.3), eri7 (ERI on the 6x6x6 configuration's odd
-stand-in 7^3, 3,571,977 classes, spacing 0.7), nuclear-batch (256 H_n chains)
-and erida129-surrogate (MLP far field); --profile-only K runs K untimed
+Other hot-path configurations (--workload): erida33 (ERIDA 32^3, odd stand-in
+33^3, spacing 0.5), erida129 (ERIDA 128^3, odd stand-in 129^3, spacing 0.3),
+nuclear-batch (256 H_n chains), kinetic24 (24^3 kinetic matrix) and
+erida129-surrogate (MLP far field); --profile-only K runs K untimed
 evaluations for profilers.
 
 --impl reference times the reference's own CPU implementation (the reference C
-core compiled under oracle/_ref, OpenMP on all host cores) on the same
-workload and prints the same JSON line with "impl": "reference".
+core compiled under oracle/_ref, OpenMP on all host cores; the repository's C
+restatement of it when that build is absent) on a seeded sample of the same
+class list and prints the same JSON line with "impl": "reference".
 """
 import argparse
 import ctypes as C
@@ -62,21 +66,18 @@ def log(msg):
 
 
 METRIC = "ERI classes/sec on 1 B200, mixed vs FP64 form at <=1e-8 Ha max abs err"
-L_GRID = 33          # odd symmetric stand-in for 32^3
-SPACING = 0.5        # bohr
 TOL = 1e-16
-WORKLOAD = "ERIDA 32^3 grid (odd stand-in 33^3, 6545 classes), spacing 0.5 bohr, G10, tol 1e-16"
 
-KIND = "erida"       # class type of the workload: "erida" (two-index) or "eri" (four-index)
-
-# the other hot-path configurations (--workload); the default line is the metric's
+# the hot-path configurations (--workload); the default line is the metric's (eri7)
 WORKLOADS = {
-    "erida33": (33, 0.5, WORKLOAD, "erida"),
-    "erida129": (129, 0.3, "ERIDA 128^3 grid (odd stand-in 129^3, 366145 classes), spacing 0.3 bohr, G10, "
-                           "tol 1e-16", "erida"),
     "eri7": (7, 0.7, "ERI 6x6x6 grid (odd stand-in 7^3, 3571977 classes), spacing 0.7 bohr, G10, tol 1e-16",
              "eri"),
+    "erida33": (33, 0.5, "ERIDA 32^3 grid (odd stand-in 33^3, 6545 classes), spacing 0.5 bohr, G10, tol 1e-16",
+                "erida"),
+    "erida129": (129, 0.3, "ERIDA 128^3 grid (odd stand-in 129^3, 366145 classes), spacing 0.3 bohr, G10, "
+                           "tol 1e-16", "erida"),
 }
+L_GRID, SPACING, WORKLOAD, KIND = WORKLOADS["eri7"]
 
 
 def g10():
@@ -101,26 +102,6 @@ def weak_scaling_value(my_ms, classes_per_rank, steps, world_size, device):
         dist.barrier()
     total_ms = float(t.item())
     return world_size * classes_per_rank * steps / (total_ms * 1e-3), total_ms
-
-
-def h_chain_batch(rng, count, edge_lo, edge_hi, spacing):
-    """Synthetic batch of linear H_n chains (the batched-nuclear workload):
-    n uniform in 2..8, bond lengths uniform in 1.0-3.0 bohr, every nucleus
-    jittered by N(0, 0.1) bohr, chain along x centred on the origin; grid edge
-    uniform in edge_lo..edge_hi points, centred, at `spacing` bohr.  Positions
-    are returned in grid units (bohr / spacing)."""
-    grids, positions, charges = [], [], []
-    for _ in range(count):
-        n = int(rng.integers(2, 9))
-        bonds = rng.uniform(1.0, 3.0, size=n - 1)
-        x = np.concatenate([[0.0], np.cumsum(bonds)])
-        x -= x.mean()
-        pos = np.stack([x, np.zeros(n), np.zeros(n)], axis=1) + rng.normal(0.0, 0.1, size=(n, 3))
-        edge = int(rng.integers(edge_lo, edge_hi + 1))
-        grids.append([(-(edge // 2), edge)] * 3)
-        positions.append(pos / spacing)
-        charges.append([1] * n)
-    return grids, positions, charges
 
 
 def dist_env():
@@ -365,6 +346,32 @@ def run_ours(args):
     main = timed(chosen, args.steps, True)
     side = timed(other, args.steps, False)
 
+    # arithmetic that ran in each form (the library's report of its last evaluation)
+    paths = {}
+    for name, f in FORMS.items():
+        step(f)
+        stream.synchronize()
+        p3 = (C.c_int * 3)()
+        L.gli_b200_last_paths(p3)
+        paths[name] = tuple(int(x) for x in p3)
+
+    log("cold step (tables, plan and graph built inside the timed call)")
+    cold = {}
+    for name, f in FORMS.items():
+        L.gli_b200_clear_caches()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            c0.record(stream)
+        step(f)
+        with torch.cuda.stream(stream):
+            c1.record(stream)
+        stream.synchronize()
+        cold[name] = {"device_ms": c0.elapsed_time(c1), "wall_ms": 1e3 * (time.perf_counter() - t0)}
+
     log("stage timing and FP64 peak probe")
     # per-stage device times of one step (library events on the same stream;
     # the first timed call warms the stream-ordered pool for the untimed path)
@@ -425,12 +432,12 @@ def run_ours(args):
                    "sample": f"unavailable: {ex}"}
     st = stage[chosen]
     dom = max(("A", "B", "C"), key=lambda k: st[k])
-    roof = roofline(chosen, dom, st, st["plan"], U, m, peak.value)
+    roof = roofline(paths[chosen], dom, st, st["plan"], U, m, peak.value)
     line = {
         "metric": METRIC, "value": main["value"], "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": main["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if chosen == "fp64" else "s8 tensor-core slices (int32 exact) + f64",
+        "dtype": dtype_label(paths[chosen]),
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "classes": m, "form": chosen, "tol": TOL, "spacing_bohr": SPACING,
                    "l2": "flushed between timed steps (1 GB write)",
@@ -440,6 +447,11 @@ def run_ours(args):
                    "mixed_over_fp64": (main["value"] / side["value"]) if chosen == "mixed" else
                    (side["value"] / main["value"]),
                    "enumeration_ms": enum_ms,
+                   "cold_step_ms": cold,
+                   "stage_paths": {k: {"A": "s8 tcgen05" if v[0] else "f64 dmma",
+                                       "B": "s8 tcgen05" if v[1] else "f64 dmma",
+                                       "C": "f64 product gemm + gather" if v[2] else "f64 per-class dots"}
+                                   for k, v in paths.items()},
                    "stage_ms": {k: {s_: v[s_] for s_ in ("tables", "A", "B", "C")} for k, v in stage.items()},
                    "stage_sizes": {"keys_A": nA, "key_pairs": nP, "lattice_U": U},
                    "wall_s_timed_region": main["wall_s"]},
@@ -467,7 +479,8 @@ def run_nuclear_batch(args):
     from gausslectronitegrate_b200 import _abi
     L = gli.lib()
     count = args.instances
-    grids, pos, q = h_chain_batch(np.random.default_rng(2024), count, 8, 24, 0.5)
+    from gausslectronitegrate_b200 import workloads
+    grids, pos, q = workloads.nuclear_batch_config(count)
     n = len(grids)
     specs = [gli._parse_grid(g, "") for g in grids]
     gstructs = (_abi.Grid * n)(*[gli._grid_struct(sp) for sp in specs])
@@ -588,22 +601,30 @@ def run_surrogate(args):
     return 0
 
 
+def dtype_label(paths):
+    """The arithmetic of an evaluation from the library's per-stage report:
+    f64 unless a stage ran as int8-sliced products on the tensor cores."""
+    tc = [st for st, on in zip("AB", paths[:2]) if on]
+    if not tc:
+        return "f64"
+    return f"s8 tensor-core slices (int32 exact) in stage{'s' if len(tc) > 1 else ''} {'+'.join(tc)}, f64 elsewhere"
+
+
 def lattice_nS(U):
     """number of distinct u^2 + v^2 with 0 <= u, v < U (rows of stage A)"""
     u = np.arange(U, dtype=np.int64)
     return int(np.unique((u[:, None] ** 2 + u[None, :] ** 2).ravel()).size)
 
 
-def roofline(form, dom, st, plan, U, m, fp64_peak):
+def roofline(paths, dom, st, plan, U, m, fp64_peak):
     """Roofline entry of the dominant stage (from the library's stage events).
     FP64 stages (the FP64 tensor-core GEMM k_dmma, or the per-class dots of
     stage C): the stage's algorithmic FP64 FLOPs against the measured FP64 peak
     (gli_b200_measure_fp64_peak: the faster of the FMA and m8n8k4 MMA probes).
     Tensor-core stages of the mixed form: the sliced work is bound by the bytes
     it must move (int8 slices read, FP64 results written) against the measured
-    HBM bandwidth.  The mixed form runs stage A on the tensor cores when
-    nA nS >= 1e6, stage B when nA U^2 >= 4e6 and nP >= 80 nA (the library's
-    rule); plan = (nA, nP, used keys, stage C products) of the step: the
+    HBM bandwidth.  paths = the library's per-stage report of the step
+    (gli_b200_last_paths); plan = (nA, nP, used keys, stage C products): the
     (pair, key) products the product GEMM computed, 0 when stage C ran per
     class (one length-U dot product per class).  A product-form stage C with
     at least 8 classes per product is the class gather's HBM traffic (16 bytes
@@ -612,8 +633,7 @@ def roofline(form, dom, st, plan, U, m, fp64_peak):
     ms = st[dom]
     nS = lattice_nS(U)
     kp = (U + 63) // 64 * 64
-    on_tensor_cores = form == "mixed" and ((dom == "A" and nA * nS >= 1000000) or
-                                           (dom == "B" and nA * U * U >= 4000000 and nP >= 80 * nA))
+    on_tensor_cores = bool((dom == "A" and paths[0]) or (dom == "B" and paths[1]))
     if dom == "C" and product and m >= 8 * product:
         # the product GEMM is small beside the class gather (ERI 7^3: 207k
         # products for 3.57 million classes): the stage moves 8 bytes of packed
@@ -672,7 +692,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-json", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["erida33", "erida129", "eri7", "nuclear-batch", "erida129-surrogate"],
-                    default="erida33", help="erida33 is the metric's configuration (the default line)")
+                    default="eri7", help="eri7 is the metric's configuration (the default line)")
     ap.add_argument("--profile-only", type=int, default=0, metavar="K",
                     help="run K untimed evaluations of --form and print nothing (for profilers)")
     ap.add_argument("--instances", type=int, default=256, help="nuclear-batch: number of H_n chains")

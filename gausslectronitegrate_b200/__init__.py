@@ -571,8 +571,81 @@ def compute_sparse_erida_gausslet_integrals(gausslet_coeffs, grid, tol, form="fp
 
 
 def load_sparse_eri_gausslet_integrals(filename):
-    """Load a sparse ERI tensor written by the reference CLI (HDF5).  Reading
-    HDF5 needs libhdf5, which this build does not link; the call fails like the
-    reference's does when H5Fopen fails (python/pymodule.c:1199-1205)."""
+    """Load a sparse ERI tensor from the HDF5 file that the reference CLI
+    writes (cli/gli_eri_integrals.c:106-163): attributes grid_length and tol,
+    datasets gausslet_coeffs, integral_values and four_indices.  Mirrors
+    python/pymodule.c:1181-1331 (same checks, messages and exception types),
+    reading the file with the library's own HDF5 reader (no libhdf5).
+    Returns a SparseERI."""
     syntax = "load_sparse_eri_gausslet_integrals(filename)"
-    raise RuntimeError(f"'H5Fopen' failed for file '{filename}' (HDF5 support is not built in); syntax: {syntax}")
+    if not isinstance(filename, str):
+        raise SyntaxError(f"error parsing input; syntax: {syntax}")
+    L = lib()
+    f = L.gli_b200_h5_fopen(filename.encode(), 0, 0)
+    if f < 0:
+        raise RuntimeError(f"'H5Fopen' failed for file '{filename}'; syntax: {syntax}")
+    try:
+        gl = np.zeros(1, dtype=np.int64)
+        if L.read_hdf5_attribute(f, b"grid_length", _abi.H5T_NATIVE_LLONG, gl.ctypes.data) < 0:
+            raise RuntimeError(f"reading 'grid_length' attribute from HDF5 file '{filename}' failed")
+        grid_length = int(gl[0])
+        if grid_length <= 0:
+            raise ValueError(f"read invalid negative 'grid_length' attribute from HDF5 file '{filename}'")
+        tol = np.zeros(1)
+        if L.read_hdf5_attribute(f, b"tol", _abi.H5T_NATIVE_DOUBLE, tol.ctypes.data) < 0:
+            raise RuntimeError(f"reading 'tol' attribute from HDF5 file '{filename}' failed")
+        dim = np.zeros(1, dtype=np.uint64)
+        if L.get_hdf5_dataset_dims(f, b"gausslet_coeffs", dim.ctypes.data) < 0:
+            raise RuntimeError(f"obtaining dimensions of Gausslet coefficients from HDF5 file '{filename}' failed")
+        if int(dim[0]) % 2 != 1:
+            raise RuntimeError(f"expecting an odd number of Gausslet coefficients in HDF5 file '{filename}'")
+        coeffs = np.empty(int(dim[0]))
+        if L.read_hdf5_dataset(f, b"gausslet_coeffs", _abi.H5T_NATIVE_DOUBLE, coeffs.ctypes.data) < 0:
+            raise RuntimeError(f"reading Gausslet coefficients from HDF5 file '{filename}' failed")
+        if L.get_hdf5_dataset_dims(f, b"integral_values", dim.ctypes.data) < 0:
+            raise RuntimeError(f"obtaining dimensions of integral values from HDF5 file '{filename}' failed")
+        values = np.empty(int(dim[0]))
+        if L.read_hdf5_dataset(f, b"integral_values", _abi.H5T_NATIVE_DOUBLE, values.ctypes.data) < 0:
+            raise RuntimeError(f"reading integral values from HDF5 file '{filename}' failed")
+        indices = np.empty(int(dim[0]), dtype=np.int64)
+        if L.read_hdf5_dataset(f, b"four_indices", _abi.H5T_NATIVE_LLONG, indices.ctypes.data) < 0:
+            raise RuntimeError(f"reading four-indices from HDF5 file '{filename}' failed")
+    finally:
+        L.gli_b200_h5_fclose(f)
+    e = -(grid_length - 1) // 2
+    return SparseERI._make(coeffs, [(e, grid_length)] * 3, indices, values, float(tol[0]))
+
+
+def save_sparse_eri_gausslet_integrals(eri, filename):
+    """Write a SparseERI in the reference CLI's HDF5 layout
+    (cli/gli_eri_integrals.c:106-163), so that the reference's loader, this
+    module's loader and libhdf5 read it.  Extension: the reference module has
+    no writer (its CLI writes the files).  The grid must be the rotationally
+    symmetric cube that the file's single grid_length describes."""
+    syntax = "save_sparse_eri_gausslet_integrals(eri, filename)"
+    if not isinstance(eri, SparseERI) or not isinstance(filename, str):
+        raise SyntaxError(f"error parsing input; syntax: {syntax}")
+    spec = eri.grid
+    n = spec[0][1]
+    if any(tuple(a) != (-(n - 1) // 2, n) for a in spec):
+        raise ValueError(f"the file format describes rotationally symmetric cubic grids only; syntax: {syntax}")
+    L = lib()
+    f = L.gli_b200_h5_fcreate(filename.encode(), 2, 0, 0)
+    if f < 0:
+        raise RuntimeError(f"'H5Fcreate' failed for '{filename}'")
+    gl = np.array([n], dtype=np.int64)
+    tol = np.array([eri.tol], dtype=np.float64)
+    coeffs = np.ascontiguousarray(eri.gausslet_coeffs, dtype=np.float64)
+    values = np.ascontiguousarray(eri.values, dtype=np.float64)
+    indices = np.ascontiguousarray(eri.indices, dtype=np.int64)
+    ok = (L.write_hdf5_scalar_attribute(f, b"grid_length", _abi.H5T_STD_I64LE, _abi.H5T_NATIVE_LLONG,
+                                        gl.ctypes.data) >= 0 and
+          L.write_hdf5_scalar_attribute(f, b"tol", _abi.H5T_IEEE_F64LE, _abi.H5T_NATIVE_DOUBLE, tol.ctypes.data) >= 0)
+    for name, arr, store, mem in ((b"gausslet_coeffs", coeffs, _abi.H5T_IEEE_F64LE, _abi.H5T_NATIVE_DOUBLE),
+                                  (b"integral_values", values, _abi.H5T_IEEE_F64LE, _abi.H5T_NATIVE_DOUBLE),
+                                  (b"four_indices", indices, _abi.H5T_STD_I64LE, _abi.H5T_NATIVE_LLONG)):
+        dims = np.array([arr.size], dtype=np.uint64)
+        ok = ok and L.write_hdf5_dataset(f, name, 1, dims.ctypes.data, store, mem, arr.ctypes.data) >= 0
+    closed = L.gli_b200_h5_fclose(f) >= 0
+    if not (ok and closed):
+        raise RuntimeError(f"writing sparse ERI file '{filename}' failed")

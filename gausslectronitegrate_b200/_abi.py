@@ -76,13 +76,25 @@ EXPORTS = [
     "gli_b200_last_error", "gli_b200_last_error_message", "gli_b200_device_count", "gli_b200_set_device",
     "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
     "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_last_plan",
-    "gli_b200_measure_fp64_peak",
+    "gli_b200_last_paths", "gli_b200_clear_caches", "gli_b200_measure_fp64_peak",
     "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
     "gli_b200_nuclear_batch_dev", "gli_b200_nuclear_batch", "gli_b200_last_nuclear_batch", "gli_b200_autotune_report",
     "gli_b200_autotune_selftest", "gli_b200_surrogate_train", "gli_b200_surrogate_free", "gli_b200_surrogate_info",
     "gli_b200_surrogate_params", "gli_b200_erida_surrogate_values", "gli_b200_mlp_loss_grad",
     "gli_b200_mlp_param_count",
+    # HDF5 subset (include/hdf5.h, include/hdf5_util.h)
+    "gli_b200_h5_fopen", "gli_b200_h5_fcreate", "gli_b200_h5_fclose", "get_hdf5_dataset_ndims",
+    "get_hdf5_dataset_dims", "read_hdf5_dataset", "write_hdf5_dataset", "get_hdf5_attribute_dims",
+    "read_hdf5_attribute", "write_hdf5_scalar_attribute", "write_hdf5_vector_attribute",
 ]
+
+# element type ids of include/hdf5.h
+H5T_NATIVE_DOUBLE = 0x7f000001
+H5T_NATIVE_LLONG = 0x7f000002
+H5T_NATIVE_INT = 0x7f000003
+H5T_IEEE_F64LE = 0x7f000011
+H5T_STD_I64LE = 0x7f000012
+H5T_STD_I32LE = 0x7f000013
 
 
 def load(path=LIB_PATH):
@@ -131,6 +143,21 @@ def load(path=LIB_PATH):
     L.gli_b200_set_timing.argtypes = [C.c_int]
     L.gli_b200_last_stage_times.argtypes = [P(C.c_float), P(glong)]
     L.gli_b200_last_plan.argtypes = [P(glong)]
+    L.gli_b200_last_paths.argtypes = [P(C.c_int)]
+    hid = C.c_int64
+    L.gli_b200_h5_fopen.argtypes = [C.c_char_p, C.c_uint, hid]
+    L.gli_b200_h5_fopen.restype = hid
+    L.gli_b200_h5_fcreate.argtypes = [C.c_char_p, C.c_uint, hid, hid]
+    L.gli_b200_h5_fcreate.restype = hid
+    L.gli_b200_h5_fclose.argtypes = [hid]
+    L.get_hdf5_dataset_ndims.argtypes = [hid, C.c_char_p, C.c_void_p]
+    for fn in ("get_hdf5_dataset_dims", "get_hdf5_attribute_dims"):
+        getattr(L, fn).argtypes = [hid, C.c_char_p, C.c_void_p]
+    for fn in ("read_hdf5_dataset", "read_hdf5_attribute"):
+        getattr(L, fn).argtypes = [hid, C.c_char_p, hid, C.c_void_p]
+    L.write_hdf5_dataset.argtypes = [hid, C.c_char_p, C.c_int, C.c_void_p, hid, hid, C.c_void_p]
+    L.write_hdf5_scalar_attribute.argtypes = [hid, C.c_char_p, hid, hid, C.c_void_p]
+    L.write_hdf5_vector_attribute.argtypes = [hid, C.c_char_p, hid, hid, glong, C.c_void_p]
     L.gli_b200_measure_fp64_peak.argtypes = [P(C.c_double)]
     L.gli_b200_kinetic_matrix_noalloc.argtypes = [C.c_void_p, glong, P(Grid), C.c_void_p, C.c_void_p]
     L.gli_b200_kinetic_matrix_noalloc.restype = C.c_int

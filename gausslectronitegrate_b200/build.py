@@ -20,7 +20,7 @@ LIB = os.path.join(PKG, "libgli_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["runtime.cu", "tables.cu", "enumerate.cu", "contract.cu", "kinetic.cu", "nuclear.cu", "dense.cu",
-           "tc_gemm.cu", "autotune.cu", "surrogate.cu", "capi.cu"]
+           "tc_gemm.cu", "autotune.cu", "surrogate.cu", "capi.cu", "h5file.cu"]
 
 
 def _flags(debug):
@@ -37,7 +37,7 @@ def _stale(obj, src):
         return True
     t = os.path.getmtime(obj)
     deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
-    deps.append(os.path.join(REPO, "include", "gli_b200.h"))
+    deps += [os.path.join(REPO, "include", h) for h in ("gli_b200.h", "hdf5.h", "hdf5_util.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
@@ -68,7 +68,8 @@ def build(debug=False, verbose=False):
         vs = os.path.join(BUILD, "exports.map")
         with open(vs, "w") as f:
             f.write("{ global: compute_*; delete_*; enumerate_*; fill_dense_*; apply_sparse_*; project_sparse_*;"
-                    " sparse_*; minimum_octahedral_*; evaluate_octahedral_*; gli_b200_*; local: *; };\n")
+                    " sparse_*; minimum_octahedral_*; evaluate_octahedral_*; gli_b200_*; get_hdf5_*; read_hdf5_*;"
+                    " write_hdf5_*; get_time_ticks; get_tick_resolution; local: *; };\n")
         run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
             ["-Xlinker", "--version-script=" + vs, "-ccbin", "/usr/bin/g++"])
     return LIB

@@ -248,6 +248,24 @@ int gli_b200_last_plan(glong out[4]) {
     return GLI_OK;
 }
 
+int gli_b200_last_paths(int out[3]) {
+    const gli::ContractStats& st = gli::last_stats();
+    out[0] = st.tc_a;
+    out[1] = st.tc_b;
+    out[2] = st.product ? 1 : 0;
+    return GLI_OK;
+}
+
+int gli_b200_clear_caches(void) {
+    gli::clear_error();
+    try {
+        gli::clear_eval_caches();
+        gli::clear_table_cache();
+    } catch (const gli::Failure&) {
+    }
+    return gli::last_error();
+}
+
 // ---------------------------------------------------------------------------
 // kinetic (reference src/kinetic_integrals.c)
 void compute_kinetic_gausslet_integrals(const struct gausslet_data* gdata, const struct cartesian_grid_3d* grid,

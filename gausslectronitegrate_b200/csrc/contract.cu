@@ -51,6 +51,10 @@ struct ClassDecode {
     double invN, invN2;
     int fast;
     const short4* pt;
+    // ERI point pairs (p, q), index p N + q: per axis |x_p - x_q| and
+    // x_p + x_q - 2 istart, 8 bits each (axes of at most 128 points), so that a
+    // class decodes with one quotient and two loads; null: point table route
+    const uint2* pd;
     void finish() {
         n32 = (uint32_t)N;
         n1 = (uint32_t)num[1];
@@ -109,6 +113,43 @@ __global__ void k_point_table(ClassDecode d, short4* __restrict__ pt) {
     pt[i] = make_short4((short)p[0], (short)p[1], (short)p[2], 0);
 }
 
+// Axis field of one ERI pair descriptor word: bits 0-7 |x_p - x_q|, 8-15
+// x_p + x_q - 2 istart of axis 2a (word .x: axes 0, 1; word .y: axis 2).
+__device__ __forceinline__ uint32_t pd_field(int dax, int sax) {
+    return (uint32_t)abs(dax) | ((uint32_t)sax << 8);
+}
+
+// descriptor of every point pair h = p N + q (N^2 entries)
+__global__ void k_pair_desc(ClassDecode d, uint2* __restrict__ pd) {
+    pdl_wait();
+    pdl_release();
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((uint64_t)h >= d.N2) return;
+    const uint32_t p = h / d.n32, q = h - p * d.n32;
+    int a[3], b[3];
+    decode_pt(d, p, a);
+    decode_pt(d, q, b);
+    uint32_t f[3];
+    for (int x = 0; x < 3; ++x) f[x] = pd_field(a[x] - b[x], a[x] + b[x] - 2 * d.is[x]);
+    pd[h] = make_uint2(f[0] | (f[1] << 16), f[2]);
+}
+
+// key of one axis from the two pair fields (|d01| | s01 << 8, |d23| | s23 << 8):
+// the unordered shift pair and |(i+j) - (k+l)| of that axis, as eri_axis_key32
+__device__ __forceinline__ int pd_axis_key(uint32_t f01, uint32_t f23, int L2m1) {
+    const int d01 = (int)(f01 & 0xffu), d23 = (int)(f23 & 0xffu);
+    const int c = abs((int)(f01 >> 8) - (int)(f23 >> 8));
+    const int a = min(d01, d23), b = max(d01, d23);
+    return ((b * (b + 1) >> 1) + a) * L2m1 + c;
+}
+
+// The pair-descriptor decode covers ERI grids whose axes have at most 128
+// points, whose N^2 descriptors take at most 32 MB, and whose class indices
+// lie below 2^53 (the quotient estimate is exact there).
+inline bool pair_desc_applies(const ClassDecode& d) {
+    return d.kind == 1 && d.fast && d.L <= 128 && d.N2 <= ((uint64_t)1 << 22);
+}
+
 // sorted axis keys of class idx; false for an index outside the tensor
 __device__ inline bool class_keys(const ClassDecode& d, i64 idx, int k[3]) {
     if (idx < 0) return false;
@@ -120,6 +161,16 @@ __device__ inline bool class_keys(const ClassDecode& d, i64 idx, int k[3]) {
         decode_pt(d, (uint32_t)pi, a);
         decode_pt(d, (uint32_t)(u - pi * d.n32), b);
         for (int x = 0; x < 3; ++x) k[x] = abs(a[x] - b[x]);
+    } else if (d.pd) {
+        // (d.pd is set only where N^4 < 2^53: the quotient estimate is exact)
+        const uint64_t hi = div_est(u, d.N2, d.invN2);  // point pair (p0, p1)
+        if (hi >= d.N2) return false;
+        const uint32_t lo = (uint32_t)u - (uint32_t)hi * (uint32_t)d.N2;  // (p2, p3): the remainder is below 2^32
+        const uint2 a = __ldg(&d.pd[hi]), b = __ldg(&d.pd[lo]);
+        const int L2m1 = 2 * (int)d.L - 1;
+        k[0] = pd_axis_key(a.x & 0xffffu, b.x & 0xffffu, L2m1);
+        k[1] = pd_axis_key(a.x >> 16, b.x >> 16, L2m1);
+        k[2] = pd_axis_key(a.y, b.y, L2m1);
     } else {
         const uint64_t hi = d.fast ? div_est(u, d.N2, d.invN2) : u / d.N2;  // point pair (p0, p1)
         if (hi >= d.N2) return false;
@@ -156,6 +207,10 @@ struct PlanCounts {
     uint64_t key_total;  // used keys + used A keys (joint scan total)
     uint64_t nP;         // distinct (A, B) key pairs
     int64_t nku, nA;     // used keys, used A keys
+    // an evaluation queued with the sizes of an earlier one found more keys or
+    // pairs than those sizes hold: the counts are zeroed (every later pass
+    // then has nothing to do) and the host evaluates again with exact sizes
+    int64_t overflow;
 };
 
 // Decodes every class once (its packed keys are kept for the later passes)
@@ -164,7 +219,9 @@ struct PlanCounts {
 // classes share a few hundred keys and a few thousand pairs, so writes of the
 // same flag from every block would queue on a few cache lines: with `local`
 // set each block collects its key flags and pair bits in shared memory and
-// merges them once.  used = [usedKey | usedA], 2 nk flags.
+// merges them once.  used = [usedKey | usedA], 2 nk flags.  keys may be null:
+// the later passes then decode the classes again (the pair-descriptor decode
+// costs less than writing and re-reading 8 bytes per class).
 __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
                                               uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
                                               uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
@@ -196,11 +253,11 @@ __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __re
             if (n >= m) break;
             int k[3];
             if (!class_keys(d, cls[v], k)) {
-                keys[n] = BAD_KEYS;
+                if (keys) keys[n] = BAD_KEYS;
                 atomicOr(bad, 1);
                 continue;
             }
-            keys[n] = pack_keys(k);
+            if (keys) keys[n] = pack_keys(k);
             flags[k[0]] = 1;
             flags[k[1]] = 1;
             flags[k[2]] = 1;
@@ -219,6 +276,15 @@ __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __re
         for (int w = threadIdx.x; w < words; w += blockDim.x)
             if (sbits[w]) atomicOr(&pairBits[w], sbits[w]);
     }
+}
+
+// packed keys of class n: from the keys buffer, or decoded from the class
+// index when the evaluation keeps none
+__device__ __forceinline__ uint64_t class_packed(const uint64_t* __restrict__ keys, const ClassDecode& d,
+                                                 const int64_t* __restrict__ idx, i64 n) {
+    if (keys) return keys[n];
+    int k[3];
+    return class_keys(d, __ldg(&idx[n]), k) ? pack_keys(k) : BAD_KEYS;
 }
 
 // id of the pair in bit `slot` of the pair bitmap: the set bits before it
@@ -610,18 +676,19 @@ __device__ inline bool choice_runs(int choice, const PlanCounts* c, i64 m) {
 // per class: one warp per class (its pair and C key found from the packed
 // keys), lanes stride over u, shuffle reduction
 __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, const double* __restrict__ H2,
-                                                  const uint64_t* __restrict__ keys, int nk,
+                                                  const uint64_t* __restrict__ keys, ClassDecode dec,
+                                                  const int64_t* __restrict__ idx, int nk,
                                                   const uint32_t* __restrict__ pairBits,
                                                   const uint64_t* __restrict__ pairPre, i64 m, int U, int Up,
                                                   const PlanCounts* __restrict__ cnt, int choice,
                                                   double* __restrict__ out) {
     pdl_wait();
     pdl_release();
-    if (!choice_runs(choice, cnt, m)) return;
+    if (cnt->overflow || !choice_runs(choice, cnt, m)) return;
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
     for (i64 n = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); n < m; n += warps) {
-        const uint64_t p = keys[n];
+        const uint64_t p = class_packed(keys, dec, idx, n);
         double acc = 0;
         if (p != BAD_KEYS) {
             int k[3];
@@ -732,7 +799,8 @@ struct ProductOp {
 // val[n] = Q[pair(n)][kid(k3)], the class's (pair, key) found from its packed
 // keys, summed over the `parts` slices of Q in order (deterministic)
 __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, int parts, i64 part_stride,
-                                                   const uint64_t* __restrict__ keys, i64 m,
+                                                   const uint64_t* __restrict__ keys, ClassDecode dec,
+                                                   const int64_t* __restrict__ idx, i64 m,
                                                    const uint64_t* __restrict__ kid, int nk,
                                                    const uint32_t* __restrict__ pairBits,
                                                    const uint64_t* __restrict__ pairPre, int ldq,
@@ -740,7 +808,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
                                                    double* __restrict__ out) {
     pdl_wait();
     pdl_release();
-    if (!choice_runs(choice, cnt, m)) return;
+    if (cnt->overflow || !choice_runs(choice, cnt, m)) return;
     // four classes per thread and step: each class is a chain of three
     // dependent loads (keys, then pair id and key id, then Q); the four chains
     // run side by side
@@ -749,7 +817,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
     for (i64 n0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; n0 < m; n0 += V * step) {
         uint64_t p[V];
 #pragma unroll
-        for (int v = 0; v < V; ++v) p[v] = n0 + v * step < m ? keys[n0 + v * step] : BAD_KEYS;
+        for (int v = 0; v < V; ++v) p[v] = n0 + v * step < m ? class_packed(keys, dec, idx, n0 + v * step) : BAD_KEYS;
         i64 q[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -1008,8 +1076,13 @@ struct PairTiles {
 // are visible to the next).  The pair bitmap, its word prefixes and the A ids
 // stay in shared memory for the pair placement (a thread per slot) and for the
 // first pair of each A key (the count of set bits before its row).
-constexpr int PLAN_SMALL_KEYS = 256, PLAN_SMALL_WORDS = PLAN_SMALL_KEYS * PLAN_SMALL_KEYS / 32;
-__global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __restrict__ used,
+//
+// capA, capP: the A keys and pairs the buffers hold.  Bounded plans pass
+// bounds that cannot be exceeded; plans sized by an earlier evaluation of the
+// same list pass its counts, and a list that needs more sets the overflow
+// flag and zeroes the counts before anything is written past the buffers.
+constexpr int PLAN_SMALL_KEYS = 384, PLAN_SMALL_WORDS = PLAN_SMALL_KEYS * PLAN_SMALL_KEYS / 32;
+__global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP, const uint32_t* __restrict__ used,
                                                      uint64_t* __restrict__ ids, int* __restrict__ keyOf,
                                                      int* __restrict__ aId, int* __restrict__ aKey, i64 words,
                                                      const uint32_t* __restrict__ bits, uint64_t* __restrict__ pre,
@@ -1031,12 +1104,8 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
     if (k == nk) nku_s = ex;  // exclusive count at nk = used keys
     __syncthreads();
     const uint32_t nku = nk > 0 ? nku_s : 0u;
-    const int nA = (int)(total - nku);
-    if (k == 0) {
-        cnt->key_total = total;
-        cnt->nku = nku;
-        cnt->nA = nA;
-    }
+    const uint32_t key_total = total;  // (total is reused by the pair scan below)
+    const int nA = (int)(key_total - nku);
     if (k < nk && f) keyOf[ex] = k;
     if (k >= nk && k < 2 * nk && f) {
         const int a = (int)(ex - nku);
@@ -1061,7 +1130,17 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, const uint32_t* __r
         __syncthreads();  // total and ws are rewritten by the next tile's scan
     }
     const int nP = (int)carry;
-    if (threadIdx.x == 0) cnt->nP = nP;
+    const bool over = nA > capA || (i64)nP > capP;  // the same on every thread
+    if (over && tile_ncols)
+        for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;  // stage B: no tiles
+    if (threadIdx.x == 0) {
+        cnt->key_total = over ? 0 : key_total;
+        cnt->nku = over ? 0 : nku;
+        cnt->nA = over ? 0 : nA;
+        cnt->nP = over ? 0 : nP;
+        cnt->overflow = over ? 1 : 0;
+    }
+    if (over) return;
     const int slots = (int)(nk * nk);
     for (int slot = threadIdx.x; slot < slots; slot += blockDim.x) {
         const uint32_t b = s_bits[slot >> 5];
@@ -1105,6 +1184,7 @@ void dgemm_prepare();  // dense.cu: attributes of the strided FP64 GEMM
 
 static thread_local bool t_timing = false;
 static thread_local ContractStats t_last;
+static thread_local int t_paths = 0;  // tensor-core stages of the evaluation being completed
 
 void set_timing(bool on) { t_timing = on; }
 const ContractStats& last_stats() { return t_last; }
@@ -1170,7 +1250,19 @@ struct EvalSizes {
 constexpr i64 BOUNDED_KEYS = 256;
 
 // stage A runs on the tensor cores (mixed form) from this many outputs nA nS
+// (GLI_B200_TC_A_OUTPUTS overrides it, for measurements)
 constexpr i64 TC_A_OUTPUTS = 1000000;
+static i64 tc_a_outputs() {
+    static const i64 v = [] {
+        const char* e = getenv("GLI_B200_TC_A_OUTPUTS");
+        return e && *e ? (i64)atoll(e) : TC_A_OUTPUTS;
+    }();
+    return v;
+}
+
+// the tensor-core stages of the last evaluation queued by this thread (bit 0:
+// stage A, bit 1: stage B)
+static thread_local int t_enq_paths = 0;
 
 // Stage B on the tensor cores slices every row of the expanded Hf (nA U^2
 // gathered values) against an FP64 product of nP U^2 FMAs: measured at ERIDA
@@ -1185,10 +1277,25 @@ static void read_status(EvalStatus* d_st, EvalStatus& h, cudaStream_t s) {
     GLI_CUDA(cudaStreamSynchronize(s));
 }
 
+// How the host sizes an evaluation's buffers and grids:
+//   PLAN_BOUNDED  bounds derived from the key space (small key spaces);
+//   PLAN_EXACT    the exact counts, read back once after the plan (a host
+//                 round trip in the middle of the evaluation);
+//   PLAN_SIZED    the counts of an earlier evaluation of the same list, passed
+//                 in `sz`: nothing is read back; the plan kernel checks the
+//                 list against these sizes and flags an overflow instead of
+//                 writing past them (the host then evaluates again, exactly).
+enum PlanMode { PLAN_BOUNDED = 0, PLAN_EXACT = 1, PLAN_SIZED = 2 };
+
+// key spaces that the sized plan's single-block plan kernel holds
+static bool sized_plan_fits(i64 nk) { return nk <= PLAN_SMALL_KEYS && (nk * nk + 31) / 32 <= 8 * 1024; }
+
 // Queues one evaluation on stream s.  Kernels read the counts from st->cnt;
-// the host sizes buffers and grids by `sz`.
-static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
+// the host sizes buffers and grids by `sz` (an input for PLAN_SIZED, an output
+// otherwise).
+static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
                          cudaStream_t s) {
+    const bool bounded = mode == PLAN_BOUNDED;
     const LatticeTables& t = *a.t;
     const i64 nk = t.nkeys, m = a.m;
     const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
@@ -1203,14 +1310,22 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     const unsigned cb = (unsigned)((m + 255) / 256);
     const unsigned kb = (unsigned)((nk + 255) / 256);
     DevBuf<short4> pts;
+    DevBuf<uint2> pdesc;
     ClassDecode dec = a.d;
-    if (dec.kind == 1) {
+    dec.pd = nullptr;
+    if (dec.kind == 1 && pair_desc_applies(dec)) {
+        // the pair-descriptor decode: every pass decodes the classes again
+        // instead of keeping 8 bytes of packed keys per class
+        pdesc.alloc(dec.N2, s);
+        launch_pdl(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p);
+        dec.pd = pdesc.p;
+    } else if (dec.kind == 1) {
         pts.alloc(dec.N, s);
         launch_pdl(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
         dec.pt = pts.p;
     }
-    // packed key triple per class
-    DevBuf<uint64_t> keys(m, s);
+    // packed key triple per class (none with the pair-descriptor decode)
+    DevBuf<uint64_t> keys(dec.pd ? 0 : m, s);
     {
         const size_t lb = mark_local_bytes(nk);
         const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
@@ -1221,7 +1336,9 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     DevBuf<uint64_t> pairPre(words, s);
     DevBuf<int> pairA, pairB;
     PairTiles tiles;
-    const bool small_pairs = bounded && words <= 8 * 1024;
+    const bool small_pairs = (bounded || mode == PLAN_SIZED) && words <= 8 * 1024;
+    if (mode == PLAN_SIZED && !(small_pairs && nk <= PLAN_SMALL_KEYS))
+        fail(GLI_ERR_INTERNAL, "sized plan for a key space of %lld keys", (long long)nk);
     if (bounded) {
         sz.nku = nk;
         sz.nA = nk;
@@ -1229,15 +1346,15 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         sz.nP = std::min(nk * (nk + 1) / 2, m);
     }
     if (small_pairs && nk <= PLAN_SMALL_KEYS) {
-        // the whole plan and stage B's tiles in one launch (bounded plans; for
-        // the larger key spaces of exact plans the single block's pass over
-        // nk^2 pair slots measured no faster than the multi-block path: ERI
-        // 7^3 0.206 against 0.200 ms)
+        // the whole plan and stage B's tiles in one launch (bounded and sized
+        // plans; for exact plans, whose counts are read back half way, the
+        // single block's pass over nk^2 pair slots measured no faster than the
+        // multi-block path: ERI 7^3 0.206 against 0.200 ms)
         pairA.alloc(sz.nP, s);
         pairB.alloc(sz.nP, s);
         const bool sliced = stage_b_sliced(a.mixed, sz.nA, sz.nP, U);
         tiles.alloc(sz.nA, sz.nP, sliced ? tile_n(MIXED_SLICES) : DM_BM, !sliced, s);
-        launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
+        launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
                    tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt);
         tiles.built = true;
@@ -1255,7 +1372,7 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
                        counts.p);
             exclusive_scan_u32_dev(counts.p, pairPre.p, words, &cnt->nP, s);
         }
-        if (!bounded) {
+        if (mode == PLAN_EXACT) {
             EvalStatus h;
             read_status(st, h, s);
             if (h.bad)
@@ -1280,8 +1397,9 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
     DevBuf<double> H(nA * (i64)nS, s);
     // the mixed form runs a stage on the tensor cores when it is large enough for
     // them to pay off; smaller stages (latency-bound either way) stay FP64
-    const bool tc_a = a.mixed && nA * (i64)nS >= TC_A_OUTPUTS;
+    const bool tc_a = a.mixed && nA * (i64)nS >= tc_a_outputs();
     const bool tc_b = stage_b_sliced(a.mixed, nA, nP, U);
+    t_enq_paths = (tc_a ? 1 : 0) | (tc_b ? 2 : 0);
     timer.mark();
     // ---- stage A
     if (tc_a) {
@@ -1308,24 +1426,25 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         int t_chunk = U;
         const int P = split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
         const i64 ps = nA * (i64)nS;
-        DevBuf<double> parts;
-        double* dst = H.p;
-        if (P > 1) {
-            parts.alloc((i64)P * ps, s);
-            dst = parts.p;
-        }
-        if (bn == 144)
-            dmma_launch(StageAOp<144>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
-                        dim3(mb, nb, (unsigned)P), s);
-        else if (bn == 80)
-            dmma_launch(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
-                        dim3(mb, nb, (unsigned)P), s);
-        else
-            dmma_launch(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst},
-                        dim3(mb, nb, (unsigned)P), s);
-        if (P > 1) {
-            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
-                       s, parts.p, P, ps, H.p);
+        const dim3 grid(mb, nb, (unsigned)P);
+        if (bn == 144) {
+            // (no split: 129..144 A keys fill the GPU; the split partial sums of
+            // 144-column tiles would not fit the operand ring for the cluster sum)
+            DevBuf<double> parts;
+            double* dst = H.p;
+            if (P > 1) {
+                parts.alloc((i64)P * ps, s);
+                dst = parts.p;
+            }
+            dmma_launch(StageAOp<144>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst}, grid, s);
+            if (P > 1)
+                launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)),
+                           dim3(256), 0, s, parts.p, P, ps, H.p);
+        } else if (bn == 80) {
+            // a split sums its parts inside a cluster of the P blocks of a tile
+            dmma_launch_cluster(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}, grid, s);
+        } else {
+            dmma_launch_cluster(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}, grid, s);
         }
     }
     timer.mark();
@@ -1374,26 +1493,16 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
         const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
         const int P = split_count(max_tiles * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
-        const i64 ps = nP * (i64)Up;
-        DevBuf<double> parts;
-        double* dst = H2.p;
-        if (P > 1) {
-            parts.alloc(P * ps, s);
-            dst = parts.p;
-        }
+        // a split sums its parts inside a cluster of the P blocks of a tile
         const dim3 grid((unsigned)max_tiles, ub, (unsigned)P);
         if ((i64)max_tiles * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
-            dmma_launch(StageBOp<false>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch, tiles.col0,
-                                        tiles.ncols, nS, U, Up, v_chunk, ps, dst},
-                        grid, s);
+            dmma_launch_cluster(StageBOp<false>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch,
+                                                tiles.col0, tiles.ncols, nS, U, Up, v_chunk, 0, H2.p},
+                                grid, s);
         else
-            dmma_launch(StageBOp<true>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch, tiles.col0,
-                                       tiles.ncols, nS, U, Up, v_chunk, ps, dst},
-                        grid, s);
-        if (P > 1) {
-            launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)), dim3(256), 0,
-                       s, parts.p, P, ps, H2.p);
-        }
+            dmma_launch_cluster(StageBOp<true>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch,
+                                               tiles.col0, tiles.ncols, nS, U, Up, v_chunk, 0, H2.p},
+                                grid, s);
     }
     timer.mark();
     // ---- stage C: the product form computes every (pair, key) dot product --
@@ -1426,26 +1535,29 @@ static void enqueue_eval(const EvalArgs& a, bool bounded, EvalStatus* st, StageT
                                   u_chunk, ps, Q.p, &st->products},
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, m, ids.p, (int)nk, pairBits.p,
+        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk, pairBits.p,
                    pairPre.p, (int)nku, cnt, c_prod, a.out);
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
-        launch_pdl(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, (int)nk, pairBits.p, pairPre.p, m, U, Up,
+        launch_pdl(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, dec, a.idx, (int)nk, pairBits.p, pairPre.p, m, U, Up,
                    cnt, c_class, a.out);
     }
     timer.mark();
 }
 
 // ---------------------------------------------------------------------------
-// CUDA graphs of bounded evaluations.  A bounded evaluation issues no host
+// CUDA graphs of evaluations.  A bounded or sized evaluation issues no host
 // synchronisation, so the whole launch sequence (allocations, memsets and about
 // 15 kernels) is captured once and replayed: every replay recomputes everything
 // from the class list in device memory; only the launch overhead is saved.
 // A graph is keyed by what fixes its launch sequence and its pointers: the
 // table set (kept alive by the entry), the grid, the class-list pointer and
-// length, the output pointer and the form.
+// length, the output pointer and the form.  A sized graph also carries the
+// counts of the exact evaluation that sized it; a list that needs more (the
+// caller rewrote the list in place) is flagged by the plan, and the host drops
+// the graph and evaluates exactly.
 struct GraphEntry {
     const LatticeTables* tables = nullptr;
     std::shared_ptr<const LatticeTables> keep;
@@ -1456,6 +1568,9 @@ struct GraphEntry {
     i64 istart[3] = {}, num[3] = {};
     cudaGraphExec_t exec = nullptr;
     long long launches = 0;  // kernels in the graph
+    PlanMode mode = PLAN_BOUNDED;
+    EvalSizes sz;            // the sizes a PLAN_SIZED graph was captured with
+    int paths = 0;           // tensor-core stages of the captured evaluation
     DevMem<EvalStatus> status;
     ~GraphEntry() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -1480,9 +1595,21 @@ static GraphEntry* find_graph(const EvalArgs& a, int device) {
     return nullptr;
 }
 
+void clear_eval_caches() { t_graphs.clear(); }
+
+static void drop_graph(const GraphEntry* e) {
+    for (auto it = t_graphs.begin(); it != t_graphs.end(); ++it)
+        if (it->get() == e) {
+            t_graphs.erase(it);
+            return;
+        }
+}
+
 static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const LatticeTables>& tp, int device,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, PlanMode mode, const EvalSizes& sized) {
     auto e = std::make_unique<GraphEntry>();
+    e->mode = mode;
+    e->sz = sized;
     e->tables = a.t;
     e->keep = tp;
     e->device = device;
@@ -1504,13 +1631,17 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageBOp<true>>();
     dmma_prepare<StageBOp<false>>();
     dmma_prepare<ProductOp<64>>();
+    dmma_prepare<StageAOp<64>, true>();
+    dmma_prepare<StageAOp<80>, true>();
+    dmma_prepare<StageBOp<true>, true>();
+    dmma_prepare<StageBOp<false>, true>();
     const long long l0 = launch_count();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     try {
         StageTimer timer(false, s);
-        EvalSizes sz;
-        enqueue_eval(a, true, e->status.p, timer, sz, s);
+        EvalSizes sz = sized;
+        enqueue_eval(a, mode, e->status.p, timer, sz, s);
     } catch (...) {
         cudaStreamEndCapture(s, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -1519,6 +1650,7 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     }
     GLI_CUDA(cudaStreamEndCapture(s, &graph));
     e->launches = launch_count() - l0;
+    e->paths = t_enq_paths;
     const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
     cudaGraphDestroy(graph);
     GLI_CUDA(ie);
@@ -1548,9 +1680,14 @@ struct PinnedBuf {
 
 // Queues one evaluation on stream s and an asynchronous copy of its status
 // block into h_status (pinned); the caller synchronises and checks it.
+// *sized receives the sized graph that was replayed (null otherwise): when its
+// status reports an overflow, the caller drops it and calls again, which
+// evaluates exactly.
 static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
                                   const int64_t* d_indices, i64 m, double tol, int form, double* d_out, cudaStream_t s,
-                                  EvalStatus* h_status, std::shared_ptr<const LatticeTables>& tp, StageTimer& timer) {
+                                  EvalStatus* h_status, std::shared_ptr<const LatticeTables>& tp, StageTimer& timer,
+                                  const GraphEntry** sized) {
+    *sized = nullptr;
     if (form != FORM_FP64 && form != FORM_MIXED)
         fail(GLI_ERR_ARGUMENT, "form %d is not a sparse evaluation form (0 = FP64, 1 = mixed)", form);
     if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
@@ -1563,7 +1700,7 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     a.t = &t;
     // the G slices exist for stage A on the tensor cores, which needs at least
     // 1e6 stage-A outputs (nA <= nkeys A keys); built once per table set
-    if (a.mixed && t.nkeys * t.nS >= TC_A_OUTPUTS) a.G = lattice_g_slices(t, s);
+    if (a.mixed && t.nkeys * t.nS >= tc_a_outputs()) a.G = lattice_g_slices(t, s);
     timer.mark();
     a.d.kind = kind;
     a.d.N = g.points();
@@ -1586,18 +1723,24 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     a.out = d_out;
     a.num_sms = ctx.num_sms;
     const bool bounded = t.nkeys <= BOUNDED_KEYS;
-    if (bounded && !t_timing && g_graphs_enabled) {
-        GraphEntry* e = find_graph(a, ctx.device);
-        if (!e) e = capture_graph(a, tp, ctx.device, s);
+    const bool graphs = !t_timing && g_graphs_enabled;
+    GraphEntry* e = graphs && (bounded || sized_plan_fits(t.nkeys)) ? find_graph(a, ctx.device) : nullptr;
+    if (!e && graphs && bounded) e = capture_graph(a, tp, ctx.device, s, PLAN_BOUNDED, EvalSizes{});
+    if (e) {
         GLI_CUDA(cudaGraphLaunch(e->exec, s));
         add_launches(e->launches);
+        t_paths = e->paths;
         GLI_CUDA(cudaMemcpyAsync(h_status, e->status.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
-    } else {
-        DevBuf<EvalStatus> st(1, s);
-        EvalSizes sz;
-        enqueue_eval(a, bounded, st.p, timer, sz, s);
-        GLI_CUDA(cudaMemcpyAsync(h_status, st.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
+        if (e->mode == PLAN_SIZED) *sized = e;
+        return;
     }
+    DevBuf<EvalStatus> st(1, s);
+    EvalSizes sz;
+    enqueue_eval(a, bounded ? PLAN_BOUNDED : PLAN_EXACT, st.p, timer, sz, s);
+    t_paths = t_enq_paths;
+    GLI_CUDA(cudaMemcpyAsync(h_status, st.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
+    // the exact counts of this list size the graph that its next evaluations replay
+    if (graphs && !bounded && sized_plan_fits(t.nkeys)) capture_graph(a, tp, ctx.device, s, PLAN_SIZED, sz);
 }
 
 // after the stream synchronised: errors of the evaluation, and the statistics
@@ -1612,6 +1755,8 @@ static void check_status(int kind, i64 m, const EvalStatus& h, const LatticeTabl
     st.keys_used = h.cnt.nku;
     st.product = product_pays((double)h.cnt.nP, (double)h.cnt.nku, m) ? 1 : 0;
     st.products = st.product ? (i64)h.products : 0;
+    st.tc_a = t_paths & 1;
+    st.tc_b = (t_paths >> 1) & 1;
     if (t_timing) {
         st.ms_tables = timer.between(0, 1);
         st.ms_a = timer.between(2, 3);
@@ -1630,8 +1775,14 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
     EvalStatus* h = (EvalStatus*)t_pin_status.get(sizeof(EvalStatus));
     std::shared_ptr<const LatticeTables> tp;
     StageTimer timer(t_timing, s);
-    sparse_values_enqueue(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, h, tp, timer);
+    const GraphEntry* sized = nullptr;
+    sparse_values_enqueue(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, h, tp, timer, &sized);
     GLI_CUDA(cudaStreamSynchronize(s));
+    if (h->cnt.overflow) {  // the list outgrew the sizes of its graph: evaluate exactly
+        drop_graph(sized);
+        sparse_values_enqueue(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, h, tp, timer, &sized);
+        GLI_CUDA(cudaStreamSynchronize(s));
+    }
     check_status(kind, m, *h, *tp, timer, stats);
 }
 
@@ -1700,11 +1851,27 @@ void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc
     }
     std::shared_ptr<const LatticeTables> tp;
     StageTimer timer(t_timing, s);
+    const GraphEntry* sized = nullptr;
     sparse_values_enqueue(kind, h_coeffs, nb, g, t_host_call.idx->p, m, tol, form, t_host_call.val->p, s, hs, tp,
-                          timer);
+                          timer, &sized);
+    // a replayed sized graph whose list outgrew its sizes (status read back
+    // with or before the values): evaluate exactly and copy the values again
+    auto redo_if_overflow = [&]() {
+        if (!hs->cnt.overflow) return false;
+        GLI_CUDA(cudaStreamSynchronize(s));
+        drop_graph(sized);
+        sparse_values_enqueue(kind, h_coeffs, nb, g, t_host_call.idx->p, m, tol, form, t_host_call.val->p, s, hs, tp,
+                              timer, &sized);
+        GLI_CUDA(cudaMemcpyAsync(pin_val, t_host_call.val->p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        check_status(kind, m, *hs, *tp, timer, nullptr);
+        host_copy(h_out, pin_val, (size_t)m * sizeof(double));
+        return true;
+    };
     if (chunks == 1) {
         GLI_CUDA(cudaMemcpyAsync(pin_val, t_host_call.val->p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
         GLI_CUDA(cudaStreamSynchronize(s));
+        if (redo_if_overflow()) return;
         check_status(kind, m, *hs, *tp, timer, nullptr);
         host_copy(h_out, pin_val, (size_t)m * sizeof(double));
         return;
@@ -1725,6 +1892,7 @@ void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc
         GLI_CUDA(cudaEventRecord(ev[c], s));
     }
     GLI_CUDA(cudaEventSynchronize(ev[0]));  // the status copy came before the values
+    if (redo_if_overflow()) return;
     check_status(kind, m, *hs, *tp, timer, nullptr);
     for (i64 c = 0; c < chunks; ++c) {
         const i64 b = c * per, n = std::min(m, b + per) - b;

@@ -29,6 +29,8 @@
 // 2 (lane%4) + {0, 1}.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include <atomic>
 #include <type_traits>
 
@@ -166,17 +168,74 @@ struct dm_blocks_of<Op, std::void_t<decltype(Op::MIN_BLOCKS)>> {
     static constexpr int value = Op::MIN_BLOCKS;
 };
 
-template <class Op>
+// Split K inside a thread-block cluster (CLUSTER = true): the launch's
+// gridDim.z chunks of K form one cluster of gridDim.z (<= 8) blocks; each
+// block leaves its partial tile in its own shared memory, and after a cluster
+// barrier every block sums its share of the tile's rows over the cluster's
+// blocks through distributed shared memory, in the order of their ranks (the
+// same order on every run), and stores it.  The Op then writes every part to
+// the same destination (part stride 0).  Every block of a cluster reaches both
+// cluster barriers: a block without work contributes zeros.
+constexpr int DM_RED_LD = 2;  // doubles of padding per reduction-tile row
+
+template <class Op, bool CLUSTER>
+__device__ __forceinline__ void dm_cluster_reduce(const Op& op, const typename Op::Block& blk, bool active,
+                                                  double* smem, int wm, int wn, int mt, int nt,
+                                                  const double (&acc)[4][Op::BN / 16][2]) {
+    constexpr int NJ = Op::BN / 16, LD = Op::BN + DM_RED_LD;
+    namespace cg = cooperative_groups;
+    const int lane = threadIdx.x & 31;
+    __syncthreads();  // every warp is done with the operand tiles
+    // this block's partial tile, zeros where it has none
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const bool has = active && i < mt && j < nt;
+            double* d = smem + (wm + 8 * i + (lane >> 2)) * LD + wn + 8 * j + 2 * (lane & 3);
+            d[0] = has ? acc[i][j][0] : 0.0;
+            d[1] = has ? acc[i][j][1] : 0.0;
+        }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    const int P = (int)cl.num_blocks(), r = (int)cl.block_rank();
+    if (active) {
+        // rows r, r + P, ...; column pairs spread over the threads
+        constexpr int PAIRS = Op::BN / 2;
+        for (int e = threadIdx.x; e < DM_BM * PAIRS; e += blockDim.x) {
+            const int row = e / PAIRS, c = 2 * (e % PAIRS);
+            if (row % P != r) continue;
+            double v0 = 0.0, v1 = 0.0;
+            for (int q = 0; q < P; ++q) {
+                const double* src = cl.map_shared_rank(smem + row * LD + c, q);
+                v0 += src[0];
+                v1 += src[1];
+            }
+            op.store(blk, row, c, v0, v1);
+        }
+    }
+    cl.sync();  // no block leaves while another still reads its tile
+}
+
+template <class Op, bool CLUSTER = false>
 __global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(const Op op) {
     constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN), NS = dm_stages_of<Op>::value;
     static_assert(Op::BN == 64 || ((Op::BN == 80 || Op::BN == 32 || Op::BN == 144) && !Op::B_KMAJOR),
                   "column tiles of 64, or 32, 80 and 144 read row-major");
     static_assert(NS >= 2 && NS <= 3, "two or three stages");
+    static_assert(!CLUSTER || DM_BM * (Op::BN + DM_RED_LD) <= NS * STAGE, "reduction tile exceeds the operand ring");
     extern __shared__ __align__(16) double dm_smem[];
     pdl_wait();  // the previous kernel's results are visible from here
     pdl_release();
     typename Op::Block blk;
-    if (!op.begin(blk)) return;
+    const bool active = op.begin(blk);
+    if (!active) {
+        if constexpr (CLUSTER) {
+            double none[4][NJ][2];
+            dm_cluster_reduce<Op, CLUSTER>(op, blk, false, dm_smem, 0, 0, 0, 0, none);
+        }
+        return;
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = (warp & 1) * 32, wn = (warp >> 1) * (Op::BN / 2);
     typename Op::AState as;
@@ -204,6 +263,10 @@ __global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(co
     else
         dm_mainloop<Op, false>(op, blk, as, bs, dm_smem, wm, wn, mt, nt, acc);
     dm_wait<0>();
+    if constexpr (CLUSTER) {
+        dm_cluster_reduce<Op, CLUSTER>(op, blk, true, dm_smem, wm, wn, mt, nt, acc);
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -216,14 +279,14 @@ __global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(co
 
 // shared memory above the 48 KB default: set once per device and Op type,
 // outside any graph capture (cudaFuncSetAttribute is not a stream operation)
-template <class Op>
+template <class Op, bool CLUSTER = false>
 void dmma_prepare() {
     static std::atomic<uint64_t> done{0};
     int dev = 0;
     GLI_CUDA(cudaGetDevice(&dev));
     const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
     if (bit && (done.load() & bit)) return;
-    GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op, CLUSTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   dm_smem(Op::BN, dm_stages_of<Op>::value)));
     done.fetch_or(bit);
 }
@@ -234,6 +297,32 @@ void dmma_launch(const Op& op, dim3 grid, cudaStream_t s) {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
     dmma_prepare<Op>();
     launch_pdl(k_dmma<Op>, grid, dim3(DM_THREADS), dm_smem(Op::BN, dm_stages_of<Op>::value), s, op);
+}
+
+// the same with K split over grid.z (2..8) blocks that sum their partial tiles
+// in a cluster (the Op's part stride must be 0)
+template <class Op>
+void dmma_launch_cluster(const Op& op, dim3 grid, cudaStream_t s) {
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
+    if (grid.z == 1) return dmma_launch(op, grid, s);
+    if (grid.z > 8) fail(GLI_ERR_INTERNAL, "cluster split of %u parts", grid.z);
+    dmma_prepare<Op, true>();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(DM_THREADS);
+    cfg.dynamicSmemBytes = dm_smem(Op::BN, dm_stages_of<Op>::value);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = 1;
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = grid.z;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    GLI_CUDA(cudaLaunchKernelEx(&cfg, k_dmma<Op, true>, op));
+    count_launch();
 }
 
 }  // namespace gli

@@ -166,8 +166,14 @@ struct ContractStats {
     i64 keys_used = 0;  // distinct axis keys of the class list
     int product = 0;    // stage C ran as the (pair, key) product GEMM
     i64 products = 0;   // ... and computed this many (pair, key) products
+    int tc_a = 0, tc_b = 0;  // stage A / B ran as int8-sliced products on the tcgen05 tensor cores
     float ms_tables = 0, ms_a = 0, ms_b = 0, ms_c = 0;
 };
+
+// drops the calling thread's captured evaluations and every cached table set
+// (the next evaluation builds its tables again)
+void clear_eval_caches();
+void clear_table_cache();
 
 // kind: 0 = ERIDA (two-index classes), 1 = ERI (four-index classes)
 void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,

@@ -2,13 +2,18 @@
 // and :73-121 (dense K x I x I + I x K x I + I x I x K).
 //
 // The 1-D table is one block reduction per shift.  The dense matrix is a pure
-// HBM write (8 bytes per entry, almost all zero): one block row per grid point
-// i, threads stride over j with coalesced stores; the table sits in shared
-// memory.
+// HBM write (8 bytes per entry, almost all zero).  Row i = (ax, ay, az) has
+// its nonzeros on three lines through i: the x line (columns bx P + c, P =
+// ny nz, c = ay nz + az), the y line and the z line inside the x block bx = ax.
+// A block writes whole rows with 16-byte stores; each thread walks its columns
+// with the x block and the in-block offset updated incrementally (no division
+// per entry), and only the x block of the row itself decodes (y, z).
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "gli_internal.cuh"
 
@@ -36,25 +41,56 @@ __global__ void k_kinetic_1d(const double* __restrict__ b, int nb, double* __res
     }
 }
 
+// value of column (bx, q) of row (ax, c = ay nz + az)
+__device__ __forceinline__ double kinetic_entry(const double* __restrict__ k1, int ax, int ay, int az, int c, int nz,
+                                                int bx, int q) {
+    double v = q == c ? k1[abs(ax - bx)] : 0.0;  // the x line
+    if (bx == ax) {                               // the y and z lines (and the diagonal)
+        const int by = q / nz, bz = q - by * nz;
+        if (by == ay) v += k1[abs(az - bz)];
+        if (bz == az) v += k1[abs(ay - by)];
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(256) k_kinetic_matrix(const double* __restrict__ k1g, int L, int nx, int ny, int nz,
                                                         double* __restrict__ out) {
     __shared__ double k1[1024];
     for (int s = threadIdx.x; s < L && s < 1024; s += blockDim.x) k1[s] = k1g[s];
     __syncthreads();
-    const i64 N = (i64)nx * ny * nz;
-    const i64 row = blockIdx.y + (i64)blockIdx.z * gridDim.y;
-    if (row >= N) return;
-    const int az = (int)(row % nz), ay = (int)((row / nz) % ny), ax = (int)(row / ((i64)nz * ny));
-    double* r = out + row * N;
-    for (i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += (i64)gridDim.x * blockDim.x) {
-        const int bz = (int)(j % nz), by = (int)((j / nz) % ny), bx = (int)(j / ((i64)nz * ny));
-        const int dx = ax - bx, dy = ay - by, dz = az - bz;
-        double v = 0;
-        if (dy == 0 && dz == 0) v += k1[dx < 0 ? -dx : dx];
-        if (dx == 0 && dz == 0) v += k1[dy < 0 ? -dy : dy];
-        if (dx == 0 && dy == 0) v += k1[dz < 0 ? -dz : dz];
-        r[j] = v;
+    const int P = ny * nz, N = nx * P;
+    const int step = 2 * blockDim.x;
+    for (int row = blockIdx.x; row < N; row += gridDim.x) {
+        const int ax = row / P, c = row - ax * P, ay = c / nz, az = c - ay * nz;
+        double* r = out + (i64)row * N;
+        // a row starting on an odd double writes its first entry alone, so
+        // that the pairs stored as double2 sit on 16-byte boundaries
+        const int j0 = (int)(((i64)row * N) & 1);
+        if (j0 && threadIdx.x == 0) r[0] = kinetic_entry(k1, ax, ay, az, c, nz, 0, 0);
+        int j = j0 + 2 * threadIdx.x;
+        int bx = j / P, q = j - bx * P;
+        for (; j + 1 < N; j += step) {
+            const double v0 = kinetic_entry(k1, ax, ay, az, c, nz, bx, q);
+            const int q1 = q + 1 < P ? q + 1 : 0, bx1 = q + 1 < P ? bx : bx + 1;
+            const double v1 = kinetic_entry(k1, ax, ay, az, c, nz, bx1, q1);
+            *reinterpret_cast<double2*>(r + j) = make_double2(v0, v1);
+            q += step;
+            while (q >= P) {
+                q -= P;
+                ++bx;
+            }
+        }
+        if (j < N) r[j] = kinetic_entry(k1, ax, ay, az, c, nz, bx, q);  // an unpaired last entry
     }
+}
+
+// blocks of the matrix kernel: rows spread over a few waves of the current
+// device's SMs (an attribute query: no context state of the library is made)
+static unsigned kinetic_blocks(i64 N) {
+    int dev = 0, sms = 148;
+    GLI_CUDA(cudaGetDevice(&dev));
+    GLI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return (unsigned)std::min<i64>(N, (i64)sms * 8);
 }
 
 void kinetic_table_device(const double* h_coeffs, i64 nb, i64 L, double* d_k1, cudaStream_t s) {
@@ -70,11 +106,9 @@ void kinetic_matrix_device(const double* h_coeffs, i64 nb, const GridDesc& g, do
     DevBuf<double> k1(L, s);
     kinetic_table_device(h_coeffs, nb, L, k1.p, s);
     const i64 N = g.points();
-    const i64 yrows = N < 65535 ? N : 65535;
-    const i64 zrows = (N + yrows - 1) / yrows;
-    const i64 xblocks = (N + 255) / 256 < 8 ? (N + 255) / 256 : 8;
-    k_kinetic_matrix<<<dim3((unsigned)xblocks, (unsigned)yrows, (unsigned)zrows), 256, 0, s>>>(
-        k1.p, (int)L, (int)g.num[0], (int)g.num[1], (int)g.num[2], d_out);
+    if (N >= ((i64)1 << 31)) fail(GLI_ERR_LIMIT, "kinetic matrix of %lld points exceeds the row index range", (long long)N);
+    k_kinetic_matrix<<<kinetic_blocks(N), 256, 0, s>>>(k1.p, (int)L, (int)g.num[0], (int)g.num[1], (int)g.num[2],
+                                                       d_out);
     GLI_CHECK_LAUNCH();
 }
 
@@ -101,42 +135,98 @@ constexpr int kNoAllocMaxAxis = 1024;
 static __device__ __align__(256) double g_noalloc_kinetic_table[kNoAllocMaxAxis];
 
 // Host code may not use g_noalloc_kinetic_table directly: on the host that name
-// is a host-side stand-in, not a device address.  The device address is looked
-// up once per device (with that device current) and remembered.
+// is a host-side stand-in, not a device address.  The device address belongs to
+// the module loaded in the current context, so it is looked up, with the
+// device current, on every call made outside a stream capture (cheap once the
+// module is loaded; it follows a context made current by the caller and the
+// new module after a device reset) and remembered per context.  A call made
+// while its stream is being captured uses the address remembered for the
+// current context: the first call in a context must come before any capture.
 static std::mutex g_noalloc_mu;
-static double* g_noalloc_table_ptr[64] = {};
+struct NoallocAddress {
+    void* ctx;
+    double* table;
+};
+static std::vector<NoallocAddress> g_noalloc_addr;
 
-static double* noalloc_table_address() {
+// the current driver context (cuCtxGetCurrent through the runtime's entry
+// point lookup, so that the library needs no link to the driver library)
+static void* current_context() {
+    using Fn = int (*)(void**);
+    static const Fn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (Fn) nullptr;
+        return (Fn)f;
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0 || !ctx) fail(GLI_ERR_CUDA, "no current CUDA context for the no-alloc kinetic table");
+    return ctx;
+}
+
+static double* noalloc_table_address(cudaStream_t s) {
     int device = 0;
     GLI_CUDA(cudaGetDevice(&device));
-    if (device < 0 || device >= 64) fail(GLI_ERR_LIMIT, "device ordinal %d out of range for the no-alloc table", device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GLI_CUDA(cudaStreamIsCapturing(s, &cap));
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_table_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_kinetic_table);
-        if (e != cudaSuccess || p == nullptr)
-            fail(GLI_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc kinetic table failed: %s", cudaGetErrorString(e));
-        g_noalloc_table_ptr[device] = static_cast<double*>(p);
+    auto it = std::find_if(g_noalloc_addr.begin(), g_noalloc_addr.end(),
+                           [&](const NoallocAddress& a) { return a.ctx == ctx; });
+    if (cap != cudaStreamCaptureStatusNone) {
+        if (it == g_noalloc_addr.end())
+            fail(GLI_ERR_ARGUMENT, "the first allocation-free kinetic call on device %d must come before stream capture",
+                 device);
+        return it->table;
     }
-    return g_noalloc_table_ptr[device];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_kinetic_table);
+    if (e != cudaSuccess || p == nullptr)
+        fail(GLI_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc kinetic table failed: %s", cudaGetErrorString(e));
+    if (it == g_noalloc_addr.end())
+        g_noalloc_addr.push_back({ctx, static_cast<double*>(p)});
+    else
+        it->table = static_cast<double*>(p);
+    return static_cast<double*>(p);
+}
+
+// device (or managed) memory, checked outside a capture: a host pointer handed
+// to the kernels would fault the GPU instead of failing the call
+static void check_device_pointer(const void* p, const char* what, cudaStream_t s) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GLI_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return;
+    cudaPointerAttributes a = {};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(GLI_ERR_ARGUMENT, "%s pointer is not CUDA memory", what);
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+        fail(GLI_ERR_ARGUMENT, "%s pointer must be device memory (got %s memory)", what,
+             a.type == cudaMemoryTypeHost ? "pinned host" : "unregistered host");
 }
 
 static void kinetic_matrix_noalloc(const double* d_coeffs, i64 nb, const GridDesc& g, double* d_out, cudaStream_t s) {
     if (!d_coeffs || !d_out) fail(GLI_ERR_ARGUMENT, "coefficient and matrix pointers must be device memory, not NULL");
     if (nb <= 0 || nb % 2 != 1) fail(GLI_ERR_ARGUMENT, "gausslet coefficient count must be odd, got %lld", (long long)nb);
+    if (nb > 46340) fail(GLI_ERR_LIMIT, "gausslet coefficient count %lld too large (nb^2 must fit 32 bits)", (long long)nb);
     const i64 L = g.max_range();
     if (L > kNoAllocMaxAxis)
         fail(GLI_ERR_LIMIT, "the allocation-free kinetic matrix supports axes up to %d points (got %lld)", kNoAllocMaxAxis,
              (long long)L);
-    double* table = noalloc_table_address();
+    if (g.points() >= ((i64)1 << 31))
+        fail(GLI_ERR_LIMIT, "kinetic matrix of %lld points exceeds the row index range", (long long)g.points());
+    check_device_pointer(d_coeffs, "coefficient", s);
+    check_device_pointer(d_out, "matrix", s);
+    double* table = noalloc_table_address(s);
     k_kinetic_1d<<<(unsigned)L, 256, 0, s>>>(d_coeffs, (int)nb, table);
     GLI_CHECK_LAUNCH();
     const i64 N = g.points();
-    const i64 yrows = N < 65535 ? N : 65535;
-    const i64 zrows = (N + yrows - 1) / yrows;
-    const i64 xblocks = (N + 255) / 256 < 8 ? (N + 255) / 256 : 8;
-    k_kinetic_matrix<<<dim3((unsigned)xblocks, (unsigned)yrows, (unsigned)zrows), 256, 0, s>>>(
-        table, (int)L, (int)g.num[0], (int)g.num[1], (int)g.num[2], d_out);
+    k_kinetic_matrix<<<kinetic_blocks(N), 256, 0, s>>>(table, (int)L, (int)g.num[0], (int)g.num[1], (int)g.num[2],
+                                                       d_out);
     GLI_CHECK_LAUNCH();
 }
 

@@ -230,6 +230,11 @@ std::list<CacheEntry> g_cache;
 constexpr size_t kCacheEntries = 8;
 }  // namespace
 
+void clear_table_cache() {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_cache.clear();
+}
+
 std::shared_ptr<const LatticeTables> lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol,
                                                     cudaStream_t s) {
     if (nb <= 0 || nb % 2 != 1) fail(GLI_ERR_ARGUMENT, "gausslet coefficient count must be odd, got %lld", (long long)nb);

@@ -401,8 +401,12 @@ int gli_b200_dgemm_sliced_dev(const double* d_A, glong lda, const double* d_B, g
  * static device array inside the library, so the grid's largest axis may have
  * at most 1024 points (larger grids fail with GLI_ERR_LIMIT).  The array is
  * shared by every call on a device, so calls whose kernels overlap on the GPU
- * race; calls ordered on one stream do not.  The first call on each device
- * looks the array's device address up (make it before any stream capture).
+ * race; calls ordered on one stream do not.  Every call made outside a stream
+ * capture looks the array's device address up in the current context; a call
+ * made while its stream is being captured reuses the address of an earlier
+ * call in the same context, so the first call in a context must come before
+ * any capture.  Outside a capture both pointers are checked to be device (or
+ * managed) memory, and host pointers fail with GLI_ERR_ARGUMENT.
  * stream is a cudaStream_t (NULL = the legacy default stream); the call returns
  * once the work is queued.  Returns a gli_b200_status. */
 int gli_b200_kinetic_matrix_noalloc(const double* d_coeffs, glong num_coeffs,
@@ -414,6 +418,18 @@ int gli_b200_last_stage_times(float ms[4], glong sizes[3]);
  * that stage C computed as the product GEMM (at least 1 when it ran so), 0 when
  * it ran per class. */
 int gli_b200_last_plan(glong out[4]);
+
+/* Arithmetic of the calling thread's last sparse evaluation, per stage:
+ * out[0] stage A, out[1] stage B: 1 when the stage ran as int8-sliced products
+ * on the tcgen05 tensor cores, 0 when it ran on the FP64 tensor-core GEMM;
+ * out[2] stage C: 1 for the (pair, key) product GEMM plus the class gather, 0
+ * for the per-class FP64 dot products.  No reference counterpart. */
+int gli_b200_last_paths(int out[3]);
+
+/* Drops the calling thread's captured evaluation graphs and every cached
+ * lattice-table set, so that the next evaluation builds its tables and plans
+ * from scratch (used to time cold evaluations).  No reference counterpart. */
+int gli_b200_clear_caches(void);
 
 #ifdef __cplusplus
 }

@@ -19,15 +19,16 @@ _ip = C.POINTER(C.c_int)
 
 
 def build():
-    """Compile the restatement (and, where the reference tree exists, the
-    reference core) with the committed Makefile."""
+    """Compile the restatement (and, where GLI_REFERENCE_DIR names a checkout
+    of the reference, the reference core) with the committed Makefile."""
     subprocess.run(["make", "-s", "-C", HERE, "restated"], check=True)
-    if os.path.isdir("/root/reference/src"):
+    ref = os.environ.get("GLI_REFERENCE_DIR", "")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
-        # the reference's own Python module linked against the B200 library
-        # (the drop-in check), once that library is built
+        # the reference's own Python module and CLI drivers linked against the
+        # B200 library (the drop-in checks), once that library is built
         if os.path.exists(os.path.join(os.path.dirname(HERE), "gausslectronitegrate_b200", "libgli_b200.so")):
-            subprocess.run(["make", "-s", "-C", HERE, "dropin"], check=True)
+            subprocess.run(["make", "-s", "-C", HERE, "dropin", "cli"], check=True)
 
 
 def _grid6(grid):

@@ -15,7 +15,7 @@ Three sources, each pinned to the reference:
 3. The notebook known answers (examples/*.ipynb outputs) are read from the
    notebooks' JSON.
 
-Usage:  python tests/golden/make_golden.py
+Usage:  GLI_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
 """
 import json
 import os
@@ -24,7 +24,7 @@ import types
 
 import numpy as np
 
-REF = "/root/reference"
+REF = os.environ.get("GLI_REFERENCE_DIR", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 
@@ -102,6 +102,8 @@ def _notebook_outputs(path):
 
 
 def main():
+    if not os.path.isdir(os.path.join(REF, "test")):
+        raise SystemExit("set GLI_REFERENCE_DIR to a checkout of the reference")
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     cap = _run_generators()
     from gausslets import get_gausslet_g10_coeffs  # the reference's coefficient source

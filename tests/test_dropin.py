@@ -20,7 +20,10 @@ needs_dropin = pytest.mark.skipif(not HAVE, reason="drop-in module not built (ma
 
 
 def _run(code):
-    env = dict(os.environ, PYTHONPATH=DROPIN_DIR)
+    # the module directory goes in front of whatever the caller's PYTHONPATH holds
+    # (a replaced path would hide the caller's own import hooks from the child)
+    prev = os.environ.get("PYTHONPATH", "")
+    env = dict(os.environ, PYTHONPATH=DROPIN_DIR + (os.pathsep + prev if prev else ""))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, f"drop-in run failed:\n{r.stdout}\n{r.stderr}"
     return r.stdout
@@ -64,3 +67,27 @@ assert np.linalg.norm(p - ref) < 1e-12
 print('dropin ok')
 """
     assert "dropin ok" in _run(code)
+
+
+@needs_dropin
+@pytest.mark.gpu
+def test_dropin_loads_the_cli_result_file():
+    # load_sparse_eri_gausslet_integrals of the reference module (its HDF5
+    # calls resolved by include/hdf5.h and include/hdf5_util.h of this
+    # library; the loader also builds the O_h grid permutations, a GPU kernel)
+    code = f"""
+import numpy as np, gausslectronitegrate_pymodule as gli
+eri = gli.load_sparse_eri_gausslet_integrals({os.path.join(GOLDEN, 'hdf5', 'eri_3x3x3.hdf5')!r})
+c = np.load({os.path.join(GOLDEN, 'reference_core.npz')!r})
+assert eri.num_entries == 1027 and eri.tol == 1e-16
+assert eri.grid == ((-1, 3), (-1, 3), (-1, 3)) or list(map(tuple, eri.grid)) == [(-1, 3)] * 3
+ref = c['eri_val_3_1e-16']
+idx = c['eri_idx_3']
+def lin(p):
+    return ((p[0] + 1) * 3 + (p[1] + 1)) * 3 + (p[2] + 1)
+v = eri.integral_value(([0, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]))
+k = int(np.searchsorted(idx, lin([0, 0, 0]) * (27 ** 3 + 27 ** 2 + 27 + 1)))
+assert abs(v - ref[k]) <= 1e-15 * abs(ref[k])
+print('load ok')
+"""
+    assert "load ok" in _run(code)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from _common import assert_parity, g10
-from bench import h_chain_batch
+from gausslectronitegrate_b200.workloads import h_chain_batch
 from oracle_binding import Oracle
 
 pytestmark = pytest.mark.gpu

@@ -68,3 +68,31 @@ def test_kinetic_noalloc_rejects_axes_beyond_its_table():
                                              C.c_void_p(d_out.data_ptr()), None)
     assert rc == 5  # GLI_ERR_LIMIT, before any kernel runs
     assert "1024" in lib.gli_b200_last_error_message().decode()
+
+
+def test_kinetic_noalloc_rejects_host_pointers_before_launching():
+    # a host array handed over as "device" memory would be written by the
+    # kernels; the entry point checks both pointers and fails with
+    # GLI_ERR_ARGUMENT before anything is queued
+    import torch
+
+    import gausslectronitegrate_b200 as gli
+
+    lib = gli.lib()
+    if lib.gli_b200_device_count() == 0:
+        pytest.fail("no CUDA device: the gpu tests need a B200")
+    b = np.ascontiguousarray(g10())
+    d_coeffs = torch.tensor(b, dtype=torch.float64, device="cuda")
+    grid = [(-1, 3), (-1, 3), (-1, 3)]
+    pageable = np.zeros((27, 27))
+    pinned = torch.zeros((27, 27), dtype=torch.float64).pin_memory()
+    for what, coeffs, out in (("pageable matrix", d_coeffs.data_ptr(), pageable.ctypes.data),
+                              ("pinned matrix", d_coeffs.data_ptr(), pinned.data_ptr()),
+                              ("pageable coefficients", b.ctypes.data, None)):
+        d_out = torch.empty((27, 27), dtype=torch.float64, device="cuda") if out is None else None
+        launches = lib.gli_b200_launch_count()
+        rc = lib.gli_b200_kinetic_matrix_noalloc(C.c_void_p(coeffs), b.size, C.byref(gli._grid_struct(grid)),
+                                                 C.c_void_p(out if out is not None else d_out.data_ptr()), None)
+        assert rc == 2, f"{what}: {lib.gli_b200_last_error_message().decode()}"  # GLI_ERR_ARGUMENT
+        assert lib.gli_b200_launch_count() == launches, f"{what}: a kernel was launched"
+    assert np.all(pageable == 0)
