@@ -467,6 +467,141 @@ def run_ours(args):
     return 0
 
 
+def run_sharded(args):
+    """Strong scaling over one class list: every rank evaluates its contiguous
+    range of the sorted list from device memory (gausslectronitegrate_b200.
+    sharded) and one NCCL all-gather assembles the values on every rank; a step
+    is both, timed on the device with CUDA events and taken as the slowest
+    rank's.  value = classes of the whole list per second."""
+    import torch
+    import torch.distributed as dist
+
+    from gausslectronitegrate_b200 import _abi
+    from gausslectronitegrate_b200.sharded import class_ranges, evaluate_sharded, library_evaluator
+    ws, rank, local = dist_env()
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import gausslectronitegrate_b200 as gli
+    L = gli.lib()
+    L.gli_b200_set_device(local)
+    spec = grid_spec()
+    gs = gli._grid_struct(spec)
+    stream = torch.cuda.current_stream()
+    # the class list (enumerated through the C API; setup, not timed) on this rank's GPU
+    idx_s = _abi.SparseIndices()
+    getattr(L, f"enumerate_symmetry_reduced_{KIND}_indices")(C.byref(gs), C.byref(idx_s))
+    idx = torch.from_numpy(np.ctypeslib.as_array(idx_s.indices, shape=(idx_s.num,)).copy()).to(f"cuda:{local}")
+    getattr(L, f"delete_sparse_{KIND}_indices")(C.byref(idx_s))
+    m = int(idx.numel())
+    evaluate = library_evaluator(KIND, g10(), spec, TOL, args.form, stream)
+    flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(max(args.warmup, 3)):
+        evaluate_sharded(idx, evaluate, rank, ws)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        vals, _ = evaluate_sharded(idx, evaluate, rank, ws)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        dist.destroy_process_group()
+    total_ms = float(t.item())
+    if rank == 0:
+        lo, hi = class_ranges(m, ws)[0]
+        print(json.dumps({"metric": METRIC, "value": m * args.steps / (total_ms * 1e-3), "unit": "classes/s",
+                          "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3),
+                          "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                          "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "see the unsharded line",
+                          "data": "synthetic",
+                          "config": {"workload": WORKLOAD, "classes": m, "form": args.form,
+                                     "partition": f"contiguous class ranges, {hi - lo} classes on rank 0, "
+                                                  "values all-gathered (NCCL)",
+                                     "l2": "flushed between timed steps (1 GB write)"}}), flush=True)
+    return 0
+
+
+def run_kinetic(args):
+    """Config: the kinetic matrix of a 24^3 grid (13,824 points: a 13,824^2
+    FP64 matrix, 1.53 GB) at spacing 0.5 bohr.  A step is one matrix written
+    into device memory (the 1-D table and the dense matrix kernel, through the
+    allocation-free entry point, whose caller owns the output); the metric is
+    matrix bytes written per second against the measured HBM bandwidth.  e2e:
+    compute_kinetic_gausslet_integrals into host memory."""
+    import torch
+    import gausslectronitegrate_b200 as gli
+    L = gli.lib()
+    edge = 24
+    grid = [(-(edge // 2), edge)] * 3
+    N = edge ** 3
+    b = np.ascontiguousarray(g10())
+    d_b = torch.tensor(b, dtype=torch.float64, device="cuda")
+    out = torch.empty((N, N), dtype=torch.float64, device="cuda")
+    gs = gli._grid_struct(grid)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        rc = L.gli_b200_kinetic_matrix_noalloc(C.c_void_p(d_b.data_ptr()), b.size, C.byref(gs),
+                                               C.c_void_p(out.data_ptr()), C.c_void_p(stream.cuda_stream))
+        if rc:
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+
+    if args.profile_only:
+        for _ in range(args.profile_only):
+            step()
+        torch.cuda.synchronize()
+        return 0
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    t_end = time.perf_counter() + 1.0
+    while time.perf_counter() < t_end:
+        step()
+        torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    # parity of a sample against the allocating entry point's host matrix (e2e)
+    t0 = time.perf_counter()
+    host = gli.compute_kinetic_gausslet_integrals(b, grid)
+    e2e_s = time.perf_counter() - t0
+    rows = np.random.default_rng(0).integers(0, N, size=64)
+    assert np.array_equal(out[torch.from_numpy(rows).cuda()].cpu().numpy(), host[rows])
+    bytes_ = 8.0 * N * N
+    mean_ms = sum(ms) / len(ms)
+    gbs = bytes_ / (mean_ms * 1e-3) / 1e9
+    peak = measured_peaks()
+    print(json.dumps({
+        "metric": "kinetic matrix bytes written per second on 1 B200 (24^3 grid, 13,824^2 FP64)", "value": gbs,
+        "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": mean_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "kinetic matrix, 24^3 grid at 0.5 bohr, G10", "matrix_bytes": bytes_,
+                   "l2": "inputs larger than L2 (1.53 GB written per step)"},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak["hbm_gbs"], "unit": "GB/s",
+                     "frac": gbs / peak["hbm_gbs"], "kernel": "k_kinetic_matrix",
+                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {peak['source']})", "traffic": None},
+        "e2e": {"value": bytes_ / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 8 * b.size,
+                "d2h_bytes_per_step": bytes_},
+        "clocks": clk}), flush=True)
+    return 0
+
+
 def run_nuclear_batch(args):
     """Config: 256 linear H_n chains (n uniform in 2..8, bonds 1.0-3.0 bohr,
     jitter N(0, 0.1) bohr), each on its own centred grid of 8^3..24^3 points at
@@ -690,8 +825,11 @@ def main():
     ap.add_argument("--form", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: split one class list over the ranks and all-gather the values (strong scaling)")
     ap.add_argument("--cpu-baseline-json", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["erida33", "erida129", "eri7", "nuclear-batch", "erida129-surrogate"],
+    ap.add_argument("--workload", choices=["eri7", "erida33", "erida129", "nuclear-batch", "kinetic24",
+                                           "erida129-surrogate"],
                     default="eri7", help="eri7 is the metric's configuration (the default line)")
     ap.add_argument("--profile-only", type=int, default=0, metavar="K",
                     help="run K untimed evaluations of --form and print nothing (for profilers)")
@@ -705,10 +843,14 @@ def main():
         return cpu_baseline_main(args.cpu_baseline_json)
     if args.workload == "nuclear-batch":
         return run_nuclear_batch(args)
+    if args.workload == "kinetic24":
+        return run_kinetic(args)
     if args.workload == "erida129-surrogate":
         return run_surrogate(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.shard:
+        return run_sharded(args)
     return run_ours(args)
 
 

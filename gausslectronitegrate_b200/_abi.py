@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgli_b200.so")
+# GLI_B200_LIBRARY selects another build of the library (the debug build
+# libgli_b200_debug.so with its device bounds checks); default the release build
+LIB_PATH = os.environ.get("GLI_B200_LIBRARY") or os.path.join(HERE, "libgli_b200.so")
 
 glong = C.c_int64
 dptr = C.POINTER(C.c_double)

@@ -17,6 +17,10 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(REPO, "_build", "gli_b200")
 LIB = os.path.join(PKG, "libgli_b200.so")
+# the debug build (device bounds checks, -DGLI_B200_DEBUG) goes to its own
+# objects and library; GLI_B200_LIBRARY=<path> makes the package load it
+BUILD_DEBUG = os.path.join(REPO, "_build", "gli_b200_debug")
+LIB_DEBUG = os.path.join(PKG, "libgli_b200_debug.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["runtime.cu", "tables.cu", "enumerate.cu", "contract.cu", "kinetic.cu", "nuclear.cu", "dense.cu",
@@ -42,13 +46,14 @@ def _stale(obj, src):
 
 
 def build(debug=False, verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+    bdir, lib = (BUILD_DEBUG, LIB_DEBUG) if debug else (BUILD, LIB)
+    os.makedirs(bdir, exist_ok=True)
     flags = _flags(debug)
     jobs = []
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(bdir, src.replace(".cu", ".o"))
         objs.append(o)
         if _stale(o, s):
             jobs.append([NVCC] + flags + ["-c", s, "-o", o])
@@ -62,17 +67,17 @@ def build(debug=False, verbose=False):
 
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         list(ex.map(run, jobs))
-    if jobs or not os.path.exists(LIB):
+    if jobs or not os.path.exists(lib):
         # the version script exports the C entry points and keeps every
         # internal (C++) symbol local to the library
-        vs = os.path.join(BUILD, "exports.map")
+        vs = os.path.join(bdir, "exports.map")
         with open(vs, "w") as f:
             f.write("{ global: compute_*; delete_*; enumerate_*; fill_dense_*; apply_sparse_*; project_sparse_*;"
                     " sparse_*; minimum_octahedral_*; evaluate_octahedral_*; gli_b200_*; get_hdf5_*; read_hdf5_*;"
                     " write_hdf5_*; get_time_ticks; get_tick_resolution; local: *; };\n")
-        run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
+        run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", lib] + objs +
             ["-Xlinker", "--version-script=" + vs, "-ccbin", "/usr/bin/g++"])
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -34,6 +34,28 @@
 namespace gli {
 
 // ---------------------------------------------------------------------------
+// Device bounds checks of the debug build (built with -DGLI_B200_DEBUG, python
+// -m gausslectronitegrate_b200.build --debug: libgli_b200_debug.so).  A failed
+// check records its site and the offending index in a device word (the first
+// failure wins) and the access it guards is skipped, so that nothing is read
+// or written out of bounds and the GPU does not fault; the host reads the word
+// after every evaluation and fails the call with GLI_ERR_INTERNAL naming the
+// site.  Release builds compile the checks away.
+//   site 1: a decoded axis key outside the key space      (k_mark)
+//   site 2: an s index outside the distinct-s list        (stage B gathers)
+//   site 3: a (pair, key) product outside Q               (k_gather_q)
+//   site 4: a pair row or key outside H2 / W              (k_stage_c)
+#ifdef GLI_B200_DEBUG
+static __device__ unsigned long long g_debug_fault;
+__device__ __forceinline__ bool dcheck(bool cond, int site, long long index) {
+    if (!cond) atomicCAS(&g_debug_fault, 0ull, ((unsigned long long)site << 56) | ((unsigned long long)index & ((1ull << 56) - 1)));
+    return cond;
+}
+#else
+__device__ __forceinline__ constexpr bool dcheck(bool, int, long long) { return true; }
+#endif
+
+// ---------------------------------------------------------------------------
 // class decoding
 struct ClassDecode {
     int kind;
@@ -257,6 +279,7 @@ __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __re
                 atomicOr(bad, 1);
                 continue;
             }
+            if (!dcheck(k[0] >= 0 && k[2] < nk, 1, k[0] < 0 ? k[0] : k[2])) continue;
             if (keys) keys[n] = pack_keys(k);
             flags[k[0]] = 1;
             flags[k[1]] = 1;
@@ -598,6 +621,7 @@ struct StageBOp {
         for (int q = 0; q < DM_ELEMS; ++q) {
             const int v = b.v0 + kc * DM_BK + dm_kmajor_k(threadIdx.x, q);
             st.sv[q] = (n < b.nvalid && v < b.v1) ? __ldg(&sidx[v * U + u]) : -1;
+            if (!dcheck(st.sv[q] < nS, 2, st.sv[q])) st.sv[q] = -1;
         }
     }
     __device__ void b_init(const Block& b, BState& st) const { b_load(b, st, 0); }
@@ -693,9 +717,11 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
         if (p != BAD_KEYS) {
             int k[3];
             unpack_keys(p, k);
+            const i64 pid = pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]);
             const double* w = W + (i64)k[2] * Up;
-            const double* h = H2 + pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]) * Up;
-            for (int u = lane; u < U; u += 32) acc = fma(w[u], h[u], acc);
+            const double* h = H2 + pid * Up;
+            if (dcheck(pid < (i64)cnt->nP && k[2] < nk, 4, pid))
+                for (int u = lane; u < U; u += 32) acc = fma(w[u], h[u], acc);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -833,7 +859,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
             const i64 n = n0 + v * step;
             if (n >= m) continue;
             double acc = 0.0;
-            if (q[v] >= 0) {
+            if (q[v] >= 0 && dcheck(q[v] < part_stride, 3, q[v])) {
                 acc = Q[q[v]];
                 for (int z = 1; z < parts; ++z) acc += Q[z * part_stride + q[v]];
             }
@@ -1268,8 +1294,16 @@ static thread_local int t_enq_paths = 0;
 // gathered values) against an FP64 product of nP U^2 FMAs: measured at ERIDA
 // 129^3 (nP = 65 nA) the two cost the same, so the sliced form is taken only
 // when the pairs per A key are clearly more.
+// (GLI_B200_TC_B_PAIRS_PER_KEY and GLI_B200_TC_B_OUTPUTS override the two
+// thresholds, for measurements)
+static i64 env_i64(const char* name, i64 dflt) {
+    const char* e = getenv(name);
+    return e && *e ? (i64)atoll(e) : dflt;
+}
 static bool stage_b_sliced(bool mixed, i64 nA, i64 nP, int U) {
-    return mixed && nA * (i64)U * U >= 4000000 && nP >= 80 * nA;
+    static const i64 per_key = env_i64("GLI_B200_TC_B_PAIRS_PER_KEY", 80);
+    static const i64 outputs = env_i64("GLI_B200_TC_B_OUTPUTS", 4000000);
+    return mixed && nA * (i64)U * U >= outputs && nP >= per_key * nA;
 }
 
 static void read_status(EvalStatus* d_st, EvalStatus& h, cudaStream_t s) {
@@ -1743,9 +1777,24 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     if (graphs && !bounded && sized_plan_fits(t.nkeys)) capture_graph(a, tp, ctx.device, s, PLAN_SIZED, sz);
 }
 
+// debug builds: a device bounds check that failed during the evaluation
+static void check_debug_fault() {
+#ifdef GLI_B200_DEBUG
+    unsigned long long f = 0;
+    GLI_CUDA(cudaMemcpyFromSymbol(&f, g_debug_fault, sizeof(f)));
+    if (f) {
+        const unsigned long long zero = 0;
+        GLI_CUDA(cudaMemcpyToSymbol(g_debug_fault, &zero, sizeof(zero)));
+        fail(GLI_ERR_INTERNAL, "device bounds check failed: site %llu, index %lld", f >> 56,
+             (long long)(f & ((1ull << 56) - 1)));
+    }
+#endif
+}
+
 // after the stream synchronised: errors of the evaluation, and the statistics
 static void check_status(int kind, i64 m, const EvalStatus& h, const LatticeTables& t, StageTimer& timer,
                          ContractStats* stats) {
+    check_debug_fault();
     if (h.bad) fail(GLI_ERR_ARGUMENT, "class index outside the %s tensor of the grid", kind ? "ERI" : "ERIDA");
     if (h.tc_err) fail(GLI_ERR_INTERNAL, "tensor-core stage: an mbarrier wait expired (code %d)", h.tc_err);
     ContractStats st;

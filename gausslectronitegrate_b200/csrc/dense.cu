@@ -579,50 +579,85 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     // canonical lookups, then contracted on the FP64 tensor-core GEMM (ERI
     // 7^3 onto 32 orbitals: the slab as FP64-level int8 slices on the tcgen05
     // tensor cores took 0.44 s, dominated by writing the slices)
-    const i64 per_i = N2 * N;
-    DevBuf<double> A1(N2 * M, s), A2(N * M * M, s), A3(N * M * M * M, s), S;
     KeyTable kt;
     build_key_table(G, g, d_idx, d_val, m, kt, s);
-    const bool slab32 = kt.ok && per_i < ((i64)1 << 32);
-    if (!(slab32 && M <= 32)) S.alloc(per_i, s);
+    const bool slab32 = kt.ok && N2 * N < ((i64)1 << 32);
     DevBuf<short4> pt;
     std::vector<short4> hpt;
+    // Rows of the basis that are zero contribute nothing: with the key table
+    // (entries computed from point coordinates) the contraction runs over the
+    // points whose rows are nonzero only -- a basis on a sub-grid of the sparse
+    // grid (the 6^3 orbitals of a 7^3 class list: (216/343)^4 of the work).
+    i64 Nx = N;
+    const double* bx = d_basis;
+    DevBuf<double> bcomp;
     if (slab32) {
         pt.alloc(N, s);
         k_dense_points<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(D, pt.p);
         GLI_CHECK_LAUNCH();
         hpt.resize(N);
+        std::vector<double> hb((size_t)(N * M));
         GLI_CUDA(cudaMemcpyAsync(hpt.data(), pt.p, N * sizeof(short4), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaMemcpyAsync(hb.data(), d_basis, N * M * sizeof(double), cudaMemcpyDeviceToHost, s));
         GLI_CUDA(cudaStreamSynchronize(s));
+        std::vector<i64> act;
+        for (i64 i = 0; i < N; ++i)
+            for (i64 c = 0; c < M; ++c)
+                if (hb[(size_t)(i * M + c)] != 0.0) {
+                    act.push_back(i);
+                    break;
+                }
+        if (act.empty()) {
+            GLI_CUDA(cudaMemsetAsync(d_out, 0, M * M * M * M * sizeof(double), s));
+            return;
+        }
+        if ((i64)act.size() < N) {
+            Nx = (i64)act.size();
+            std::vector<short4> hp((size_t)Nx);
+            std::vector<double> hbc((size_t)(Nx * M));
+            for (i64 a = 0; a < Nx; ++a) {
+                hp[(size_t)a] = hpt[(size_t)act[(size_t)a]];
+                for (i64 c = 0; c < M; ++c) hbc[(size_t)(a * M + c)] = hb[(size_t)(act[(size_t)a] * M + c)];
+            }
+            hpt.swap(hp);
+            GLI_CUDA(cudaMemcpyAsync(pt.p, hpt.data(), Nx * sizeof(short4), cudaMemcpyHostToDevice, s));
+            bcomp.alloc(Nx * M, s);
+            GLI_CUDA(cudaMemcpyAsync(bcomp.p, hbc.data(), Nx * M * sizeof(double), cudaMemcpyHostToDevice, s));
+            GLI_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+            bx = bcomp.p;
+        }
     }
+    const i64 Nx2 = Nx * Nx, per_i = Nx2 * Nx;
+    DevBuf<double> A1(Nx2 * M, s), A2(Nx * M * M, s), A3(Nx * M * M * M, s), S;
     // the first contraction with its slab computed as the GEMM stages it (at
     // most 32 orbitals), or from a filled slab
     const bool fused = slab32 && M <= 32;
-    for (i64 i = 0; i < N; ++i) {
+    if (!fused) S.alloc(per_i, s);
+    for (i64 i = 0; i < Nx; ++i) {
         if (fused) {
-            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, d_basis, A1.p, hpt[i], (int)N, (int)G.L, (int)M},
-                        dim3((unsigned)((N2 + DM_BM - 1) / DM_BM)), s);
+            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, bx, A1.p, hpt[i], (int)Nx, (int)G.L, (int)M},
+                        dim3((unsigned)((Nx2 + DM_BM - 1) / DM_BM)), s);
         } else {
             if (slab32)
-                k_fill_slab_keyed<<<grid_for(per_i), 256, 0, s>>>(pt.p, (uint32_t)N, (int)G.L, hpt[i], kt.t.p, S.p);
+                k_fill_slab_keyed<<<grid_for(per_i), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p, S.p);
             else if (kt.ok)
                 k_fill_eri_rows_keyed<<<grid_for(per_i), 256, 0, s>>>(D, kt.t.p, G.L, i * N, N, S.p);
             else
                 k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
             GLI_CHECK_LAUNCH();
             // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-            dgemm((int)N2, (int)M, (int)N, MatView{S.p, 0, N, 1}, MatView{d_basis, 0, M, 1}, A1.p, 0, M, 1, 1, false,
+            dgemm((int)Nx2, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false,
                   s);
         }
         // A2[j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j)
-        dgemm((int)M, (int)M, (int)N, MatView{d_basis, 0, 1, M}, MatView{A1.p, N * M, M, 1}, A2.p, M * M, M, 1,
-              (int)N, false, s);
+        dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, A2.p, M * M, M, 1,
+              (int)Nx, false, s);
         // A3[i][q][(r s)] = sum_j B[j][q] A2[j][(r s)]
-        dgemm((int)M, (int)(M * M), (int)N, MatView{d_basis, 0, 1, M}, MatView{A2.p, 0, M * M, 1},
+        dgemm((int)M, (int)(M * M), (int)Nx, MatView{bx, 0, 1, M}, MatView{A2.p, 0, M * M, 1},
               A3.p + i * M * M * M, 0, M * M, 1, 1, false, s);
     }
     // E[p][(q r s)] = sum_i B[i][p] A3[i][(q r s)]
-    dgemm((int)M, (int)(M * M * M), (int)N, MatView{d_basis, 0, 1, M}, MatView{A3.p, 0, M * M * M, 1}, d_out, 0,
+    dgemm((int)M, (int)(M * M * M), (int)Nx, MatView{bx, 0, 1, M}, MatView{A3.p, 0, M * M * M, 1}, d_out, 0,
           M * M * M, 1, 1, false, s);
 }
 
