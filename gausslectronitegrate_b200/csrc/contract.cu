@@ -1348,8 +1348,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     ClassDecode dec = a.d;
     dec.pd = nullptr;
     if (dec.kind == 1 && pair_desc_applies(dec)) {
-        // the pair-descriptor decode: every pass decodes the classes again
-        // instead of keeping 8 bytes of packed keys per class
+        // the pair-descriptor decode of the ERI classes
         pdesc.alloc(dec.N2, s);
         launch_pdl(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p);
         dec.pd = pdesc.p;
@@ -1358,8 +1357,10 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         launch_pdl(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
         dec.pt = pts.p;
     }
-    // packed key triple per class (none with the pair-descriptor decode)
-    DevBuf<uint64_t> keys(dec.pd ? 0 : m, s);
+    // packed key triple per class, written by the decode pass and read by the
+    // gather (decoding a class again in the gather measured slower than
+    // re-reading its 8 bytes: ERI 7^3 stage C 52 against 32 us)
+    DevBuf<uint64_t> keys(m, s);
     {
         const size_t lb = mark_local_bytes(nk);
         const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
@@ -1882,9 +1883,121 @@ static void host_copy(void* dst, const void* src, size_t bytes) {
 // The evaluation from and into host arrays: the class list goes to the device
 // in chunks, each chunk's DMA overlapping the host copy of the next into the
 // pinned staging buffer; the values come back the same way in reverse.
+// true for page-locked host memory the DMA engines can read and write directly
+static bool is_pinned(const void* p) {
+    cudaPointerAttributes a = {};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// the two copy streams of the page-locked host path (per thread and device)
+struct CopyStreams {
+    int device = -1;
+    cudaStream_t in = nullptr, out = nullptr;
+    void ensure(int dev) {
+        if (dev == device) return;
+        GLI_CUDA(cudaStreamCreateWithFlags(&in, cudaStreamNonBlocking));
+        GLI_CUDA(cudaStreamCreateWithFlags(&out, cudaStreamNonBlocking));
+        device = dev;
+    }
+    ~CopyStreams() {
+        if (in) cudaStreamDestroy(in);
+        if (out) cudaStreamDestroy(out);
+    }
+};
+static thread_local CopyStreams t_copy_streams;
+static thread_local PinnedBuf t_pin_status_chunks;
+
+// Page-locked class list and value arrays: the copies go straight between them
+// and the device buffers (no staging).  A list of a million classes or more is
+// evaluated in PINNED_CHUNKS contiguous ranges so that the copies overlap the
+// evaluations: the class list streams in on one copy stream, each range is
+// evaluated as soon as its part has arrived, and its values stream out on a
+// second copy stream (the two directions run concurrently) while the next
+// range is evaluated.  Each range is an evaluation of its own (its own plan
+// and sized graph); its values agree with one evaluation of the whole list
+// within the FP64 parity bar.
+constexpr i64 PINNED_CHUNKS = 4;
+static void sparse_values_pinned(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices,
+                                 i64 m, double tol, int form, double* h_out, cudaStream_t s) {
+    const Context& ctx = context();
+    t_host_call.ensure(ctx.device, m);
+    const i64 chunks = m >= ((i64)1 << 20) ? PINNED_CHUNKS : 1, per = (m + chunks - 1) / chunks;
+    EvalStatus* hs = (EvalStatus*)t_pin_status_chunks.get(chunks * sizeof(EvalStatus));
+    std::shared_ptr<const LatticeTables> tp;
+    StageTimer timer(t_timing && chunks == 1, s);
+    std::vector<const GraphEntry*> sized(chunks, nullptr);
+    int64_t* d_idx = t_host_call.idx->p;
+    double* d_val = t_host_call.val->p;
+    if (chunks == 1) {
+        GLI_CUDA(cudaMemcpyAsync(d_idx, h_indices, (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx, m, tol, form, d_val, s, hs, tp, timer, &sized[0]);
+            GLI_CUDA(cudaMemcpyAsync(h_out, d_val, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+            GLI_CUDA(cudaStreamSynchronize(s));
+            if (!hs->cnt.overflow) break;
+            drop_graph(sized[0]);  // the list outgrew its graph's sizes: once more, exactly
+        }
+        check_status(kind, m, *hs, *tp, timer, nullptr);
+        return;
+    }
+    t_copy_streams.ensure(ctx.device);
+    cudaStream_t s_in = t_copy_streams.in, s_out = t_copy_streams.out;
+    std::vector<cudaEvent_t> ev(2 * chunks + 1, nullptr);
+    struct Release {
+        std::vector<cudaEvent_t>& e;
+        ~Release() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } release{ev};
+    for (auto& e : ev) GLI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // the copy streams start after the work already queued on s
+    GLI_CUDA(cudaEventRecord(ev[2 * chunks], s));
+    GLI_CUDA(cudaStreamWaitEvent(s_in, ev[2 * chunks], 0));
+    GLI_CUDA(cudaStreamWaitEvent(s_out, ev[2 * chunks], 0));
+    for (i64 c = 0; c < chunks; ++c) {
+        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
+        if (n > 0)
+            GLI_CUDA(cudaMemcpyAsync(d_idx + b, h_indices + b, (size_t)n * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                     s_in));
+        GLI_CUDA(cudaEventRecord(ev[c], s_in));
+    }
+    for (i64 c = 0; c < chunks; ++c) {
+        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
+        GLI_CUDA(cudaStreamWaitEvent(s, ev[c], 0));
+        if (n > 0)
+            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx + b, n, tol, form, d_val + b, s, hs + c, tp, timer,
+                                  &sized[c]);
+        GLI_CUDA(cudaEventRecord(ev[chunks + c], s));
+        GLI_CUDA(cudaStreamWaitEvent(s_out, ev[chunks + c], 0));
+        if (n > 0)
+            GLI_CUDA(cudaMemcpyAsync(h_out + b, d_val + b, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s_out));
+    }
+    GLI_CUDA(cudaStreamSynchronize(s_out));
+    GLI_CUDA(cudaStreamSynchronize(s));
+    for (i64 c = 0; c < chunks; ++c) {
+        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
+        if (n <= 0) continue;
+        if (hs[c].cnt.overflow) {  // this range outgrew its graph's sizes: once more, exactly
+            drop_graph(sized[c]);
+            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx + b, n, tol, form, d_val + b, s, hs + c, tp, timer,
+                                  &sized[c]);
+            GLI_CUDA(cudaMemcpyAsync(h_out + b, d_val + b, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            GLI_CUDA(cudaStreamSynchronize(s));
+        }
+        check_status(kind, n, hs[c], *tp, timer, nullptr);
+    }
+}
+
 void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices, i64 m,
                         double tol, int form, double* h_out, cudaStream_t s) {
     if (m == 0) return;
+    if (is_pinned(h_indices) && is_pinned(h_out))
+        return sparse_values_pinned(kind, h_coeffs, nb, g, h_indices, m, tol, form, h_out, s);
     const Context& ctx = context();
     EvalStatus* hs = (EvalStatus*)t_pin_status.get(sizeof(EvalStatus));
     int64_t* pin_idx = (int64_t*)t_pin_idx.get((size_t)m * sizeof(int64_t));

@@ -200,17 +200,29 @@ __device__ __forceinline__ void dm_cluster_reduce(const Op& op, const typename O
     cl.sync();
     const int P = (int)cl.num_blocks(), r = (int)cl.block_rank();
     if (active) {
-        // rows r, r + P, ...; column pairs spread over the threads
+        // block r sums rows [r0, r1) of the tile: per column pair, the P
+        // partial pairs are loaded first (16-byte distributed shared-memory
+        // loads, all in flight together) and then added in rank order
         constexpr int PAIRS = Op::BN / 2;
-        for (int e = threadIdx.x; e < DM_BM * PAIRS; e += blockDim.x) {
+        const int r0 = (DM_BM * r) / P, r1 = (DM_BM * (r + 1)) / P;
+        const double2* part[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            part[q] = reinterpret_cast<const double2*>(cl.map_shared_rank(smem, q < P ? q : 0));
+        for (int e = r0 * PAIRS + threadIdx.x; e < r1 * PAIRS; e += blockDim.x) {
             const int row = e / PAIRS, c = 2 * (e % PAIRS);
-            if (row % P != r) continue;
-            double v0 = 0.0, v1 = 0.0;
-            for (int q = 0; q < P; ++q) {
-                const double* src = cl.map_shared_rank(smem + row * LD + c, q);
-                v0 += src[0];
-                v1 += src[1];
-            }
+            const int off = (row * LD + c) / 2;  // LD and c are even: 16-byte aligned pairs
+            double2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (q < P) v[q] = part[q][off];
+            double v0 = v[0].x, v1 = v[0].y;
+#pragma unroll
+            for (int q = 1; q < 8; ++q)
+                if (q < P) {
+                    v0 += v[q].x;
+                    v1 += v[q].y;
+                }
             op.store(blk, row, c, v0, v1);
         }
     }

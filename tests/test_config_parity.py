@@ -130,3 +130,24 @@ def test_nuclear_batch_24_pairs(gli, golden):
     by_id = dict(zip(ids, outs))
     got = np.array([by_id[int(k)][i, j] for k, i, j in zip(inst, golden["nuc24_i"], golden["nuc24_j"])])
     assert_parity(got, golden["nuc24_val"], what="nuclear 24^3 pair sample (3 chains x 48 pairs)")
+
+
+def test_eri7_pinned_host_buffers(gli, eri7):
+    # page-locked host arrays: the C call copies straight to and from them and
+    # evaluates the 3.57 million classes in overlapped ranges, each its own plan
+    import ctypes as C
+
+    import torch
+
+    from gausslectronitegrate_b200 import _abi
+    from gausslectronitegrate_b200 import workloads as W
+    s = eri7["fp64"]
+    idx = torch.from_numpy(s.indices).pin_memory()
+    out = torch.full((s.indices.size,), float("nan"), dtype=torch.float64).pin_memory()
+    gd, keep = gli._parse_coeffs(np.ascontiguousarray(g10()), "")
+    for _ in range(2):  # the second call replays the ranges' captured graphs
+        rc = gli.lib().gli_b200_sparse_values(_abi.GLI_KIND_ERI, C.byref(gd), C.byref(gli._grid_struct(W.ERI6_SPARSE)),
+                                              C.cast(idx.data_ptr(), _abi.lptr), s.indices.size, 1e-16,
+                                              _abi.GLI_FORM_FP64, C.cast(out.data_ptr(), _abi.dptr))
+        assert rc == 0, gli.lib().gli_b200_last_error_message().decode()
+        assert_parity(out.numpy(), s.values, what="ERI 7^3 through pinned host buffers")
