@@ -310,6 +310,110 @@ __device__ __forceinline__ uint64_t class_packed(const uint64_t* __restrict__ ke
     return class_keys(d, __ldg(&idx[n]), k) ? pack_keys(k) : BAD_KEYS;
 }
 
+// The decode pass for ERI classes through the pair descriptors.  A thread
+// takes four consecutive classes (16-byte loads of the indices and stores of
+// the packed keys when the arrays are 16-byte aligned): a sorted list keeps the
+// point pair (i, j) of neighbouring classes, so the quotient by N^2 and the
+// first descriptor are reused while the remainder stays below N^2 (any order
+// is still decoded correctly: an out-of-range remainder takes the quotient
+// again), and a pair bit already set by the thread's previous class is not
+// tested again.  Flags and pair bits as in k_mark.
+__global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
+                                                     uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
+                                                     uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
+    pdl_wait();
+    pdl_release();
+    extern __shared__ uint32_t sflag[];
+    const int nk = (int)d.nkeys;
+    const int words = (nk * nk + 31) >> 5;
+    uint32_t* sbits = sflag + 2 * nk;
+    if (local) {
+        for (int i = threadIdx.x; i < 2 * nk + words; i += blockDim.x) sflag[i] = 0;
+        __syncthreads();
+    }
+    uint32_t* flags = local ? sflag : used;
+    uint32_t* bits = local ? sbits : pairBits;
+    const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)keys & 15) == 0;
+    const uint64_t N2 = d.N2;
+    const uint32_t N2lo = (uint32_t)N2;
+    const int L2m1 = 2 * (int)d.L - 1;
+    const i64 groups = (m + 3) / 4;
+    for (i64 g = (i64)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (i64)gridDim.x * blockDim.x) {
+        const i64 n0 = 4 * g;
+        const bool full = n0 + 3 < m;
+        int64_t c[4];
+        if (vec && full) {
+            const longlong2 a = __ldg(reinterpret_cast<const longlong2*>(idx + n0));
+            const longlong2 b = __ldg(reinterpret_cast<const longlong2*>(idx + n0 + 2));
+            c[0] = a.x, c[1] = a.y, c[2] = b.x, c[3] = b.y;
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) c[v] = n0 + v < m ? __ldg(&idx[n0 + v]) : 0;
+        }
+        uint64_t hi = ~(uint64_t)0;
+        uint2 da = make_uint2(0, 0);
+        int last_slot = -1;
+        uint64_t kv[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            kv[v] = BAD_KEYS;
+            if (n0 + v >= m) continue;
+            const int64_t x = c[v];
+            if (x < 0) {
+                atomicOr(bad, 1);
+                continue;
+            }
+            const uint64_t u = (uint64_t)x;
+            if (hi == ~(uint64_t)0 || u - hi * N2 >= N2) {
+                hi = div_est(u, N2, d.invN2);
+                if (hi >= N2) {
+                    hi = ~(uint64_t)0;
+                    atomicOr(bad, 1);
+                    continue;
+                }
+                da = __ldg(&d.pd[hi]);
+            }
+            const uint32_t lo = (uint32_t)u - (uint32_t)hi * N2lo;
+            const uint2 db = __ldg(&d.pd[lo]);
+            int k[3];
+            k[0] = pd_axis_key(da.x & 0xffffu, db.x & 0xffffu, L2m1);
+            k[1] = pd_axis_key(da.x >> 16, db.x >> 16, L2m1);
+            k[2] = pd_axis_key(da.y, db.y, L2m1);
+            const int k0 = min(k[0], k[1]), k1 = max(k[0], k[1]);
+            const int s0 = min(k0, k[2]), s2 = max(k1, k[2]);
+            const int s1 = k0 + k1 + k[2] - s0 - s2;
+            if (!dcheck(s0 >= 0 && s2 < nk, 1, s2)) continue;
+            k[0] = s0, k[1] = s1, k[2] = s2;
+            kv[v] = pack_keys(k);
+            flags[s0] = 1;
+            flags[s1] = 1;
+            flags[s2] = 1;
+            flags[nk + s1] = 1;
+            const int slot = s1 * nk + s0;
+            if (slot != last_slot) {
+                last_slot = slot;
+                const uint32_t bit = 1u << (slot & 31);
+                if (!(bits[slot >> 5] & bit)) atomicOr(&bits[slot >> 5], bit);
+            }
+        }
+        if (vec && full) {
+            reinterpret_cast<ulonglong2*>(keys + n0)[0] = make_ulonglong2(kv[0], kv[1]);
+            reinterpret_cast<ulonglong2*>(keys + n0)[1] = make_ulonglong2(kv[2], kv[3]);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (n0 + v < m) keys[n0 + v] = kv[v];
+        }
+    }
+    if (local) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 2 * nk; i += blockDim.x)
+            if (sflag[i]) used[i] = 1;
+        for (int w = threadIdx.x; w < words; w += blockDim.x)
+            if (sbits[w]) atomicOr(&pairBits[w], sbits[w]);
+    }
+}
+
 // id of the pair in bit `slot` of the pair bitmap: the set bits before it
 __device__ inline i64 pair_id(const uint32_t* __restrict__ bits, const uint64_t* __restrict__ pre, i64 slot) {
     const i64 w = slot >> 5;
@@ -835,35 +939,56 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
     pdl_wait();
     pdl_release();
     if (cnt->overflow || !choice_runs(choice, cnt, m)) return;
-    // four classes per thread and step: each class is a chain of three
-    // dependent loads (keys, then pair id and key id, then Q); the four chains
-    // run side by side
-    constexpr int V = 4;
-    const i64 step = (i64)gridDim.x * blockDim.x;
-    for (i64 n0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; n0 < m; n0 += V * step) {
-        uint64_t p[V];
+    // four consecutive classes per thread (16-byte loads and stores where the
+    // arrays allow): each class is a chain of dependent loads (keys, then pair
+    // id and key id, then Q); the four chains run side by side, and a pair id
+    // equal to the previous class's is not looked up again
+    const bool vec = keys && ((uintptr_t)keys & 15) == 0 && ((uintptr_t)out & 15) == 0;
+    const i64 groups = (m + 3) / 4;
+    for (i64 g = (i64)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (i64)gridDim.x * blockDim.x) {
+        const i64 n0 = 4 * g;
+        const bool full = n0 + 3 < m;
+        uint64_t p[4];
+        if (vec && full) {
+            const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(keys + n0));
+            const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(keys + n0 + 2));
+            p[0] = a.x, p[1] = a.y, p[2] = b.x, p[3] = b.y;
+        } else {
 #pragma unroll
-        for (int v = 0; v < V; ++v) p[v] = n0 + v * step < m ? class_packed(keys, dec, idx, n0 + v * step) : BAD_KEYS;
-        i64 q[V];
+            for (int v = 0; v < 4; ++v) p[v] = n0 + v < m ? class_packed(keys, dec, idx, n0 + v) : BAD_KEYS;
+        }
+        i64 q[4];
+        i64 last_slot = -1, last_pid = 0;
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
+        for (int v = 0; v < 4; ++v) {
             q[v] = -1;
             if (p[v] != BAD_KEYS) {
                 int k[3];
                 unpack_keys(p[v], k);
-                q[v] = pair_id(pairBits, pairPre, (i64)k[1] * nk + k[0]) * ldq + (i64)kid[k[2]];
+                const i64 slot = (i64)k[1] * nk + k[0];
+                if (slot != last_slot) {
+                    last_slot = slot;
+                    last_pid = pair_id(pairBits, pairPre, slot);
+                }
+                q[v] = last_pid * ldq + (i64)kid[k[2]];
             }
         }
+        double acc[4];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const i64 n = n0 + v * step;
-            if (n >= m) continue;
-            double acc = 0.0;
+        for (int v = 0; v < 4; ++v) {
+            acc[v] = 0.0;
             if (q[v] >= 0 && dcheck(q[v] < part_stride, 3, q[v])) {
-                acc = Q[q[v]];
-                for (int z = 1; z < parts; ++z) acc += Q[z * part_stride + q[v]];
+                acc[v] = Q[q[v]];
+                for (int z = 1; z < parts; ++z) acc[v] += Q[z * part_stride + q[v]];
             }
-            out[n] = acc;
+        }
+        if (vec && full) {
+            reinterpret_cast<double2*>(out + n0)[0] = make_double2(acc[0], acc[1]);
+            reinterpret_cast<double2*>(out + n0)[1] = make_double2(acc[2], acc[3]);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (n0 + v < m) out[n0 + v] = acc[v];
         }
     }
 }
@@ -952,13 +1077,13 @@ struct PairRows {  // pair p: row W[pairB[p]], placed in the tiles of its A key
 // own pair and i + j mod y for j < reg_count(i, y): at most bn rows), and the
 // keys from y up host every pair with a key below y plus a regular tournament
 // among themselves (129 keys: 132 tiles of 64 instead of 195).
-__device__ __forceinline__ int reg_count(int i, int y) { return (y & 1) ? (y + 1) / 2 : y / 2 + (i < y / 2); }
-__device__ __forceinline__ int reg_prefix(int i, int y) {  // rows of the members below i
+__host__ __device__ __forceinline__ int reg_count(int i, int y) { return (y & 1) ? (y + 1) / 2 : y / 2 + (i < y / 2); }
+__host__ __device__ __forceinline__ int reg_prefix(int i, int y) {  // rows of the members below i
     if (y & 1) return i * ((y + 1) / 2);
     const int h = y / 2;
     return i <= h ? i * (h + 1) : h * (h + 1) + (i - h) * h;
 }
-__device__ __forceinline__ int bal_count(int h, int n, int y) {
+__host__ __device__ __forceinline__ int bal_count(int h, int n, int y) {
     return h < y ? reg_count(h, y) : y + reg_count(h - y, n - y);
 }
 __device__ __forceinline__ int bal_offset(int h, int n, int y) {
@@ -1082,10 +1207,17 @@ struct PairTiles {
     int *first = nullptr, *tile0 = nullptr, *batch = nullptr, *col0 = nullptr, *ncols = nullptr;
     int *rowPair = nullptr, *rowKey = nullptr;
     bool built = false;
-    void alloc(i64 nA, i64 nP, int tile_pairs, bool rows, cudaStream_t s) {
+    static i64 ints(i64 nA, i64 nP, int tile_pairs, bool rows) {
+        return 2 * nA + 3 * (nP / tile_pairs + nA + 1) + (rows ? 2 * nP : 0);
+    }
+    // mem: nullptr to allocate on the stream, or ints(...) ints lent by an owner
+    void alloc(i64 nA, i64 nP, int tile_pairs, bool rows, cudaStream_t s, int* mem = nullptr) {
         bn = tile_pairs;
         max_tiles = nP / bn + nA + 1;
-        buf.alloc(2 * nA + 3 * max_tiles + (rows ? 2 * nP : 0), s);
+        if (mem)
+            buf.borrow(mem, ints(nA, nP, tile_pairs, rows), s);
+        else
+            buf.alloc(ints(nA, nP, tile_pairs, rows), s);
         first = buf.p;
         tile0 = buf.p + nA;
         batch = buf.p + 2 * nA;
@@ -1094,6 +1226,43 @@ struct PairTiles {
         rowPair = rows ? ncols + max_tiles : nullptr;
         rowKey = rows ? rowPair + nP : nullptr;
     }
+};
+
+// The plan of a sized evaluation, kept between the replays of its graph: the
+// key and pair lists, word prefixes and stage-B tiles, plus the key flags, the
+// pair bitmap and the counts they were made from.  A replay decodes and marks
+// every class again; when its key flags and pair bitmap equal the saved ones
+// (checked on the device, every replay), the plan they determine is the saved
+// one and the plan kernel only restores its counts; otherwise it plans anew
+// and saves.  (The plan is a function of those flags and bits alone.)
+struct PlanReuse {
+    uint32_t* saved_used = nullptr;
+    uint32_t* saved_bits = nullptr;
+    PlanCounts* saved_cnt = nullptr;
+    int* valid = nullptr;  // null: no reuse (bounded plans)
+};
+struct PlanStore {
+    DevMem<uint64_t> ids, pairPre;
+    DevMem<int> keyOf, aId, aKey, pairA, pairB, tiles;
+    DevMem<uint32_t> saved_used, saved_bits;
+    DevMem<PlanCounts> saved_cnt;
+    DevMem<int> valid;
+    void alloc(i64 nk, i64 words, i64 capA, i64 capP, i64 tile_ints) {
+        ids.alloc((size_t)(2 * nk));
+        pairPre.alloc((size_t)words);
+        keyOf.alloc((size_t)nk);
+        aId.alloc((size_t)nk);
+        aKey.alloc((size_t)nk);
+        pairA.alloc((size_t)std::max<i64>(capP, 1));
+        pairB.alloc((size_t)std::max<i64>(capP, 1));
+        tiles.alloc((size_t)tile_ints);
+        saved_used.alloc((size_t)(2 * nk));
+        saved_bits.alloc((size_t)words);
+        saved_cnt.alloc(1);
+        valid.alloc(1);
+        GLI_CUDA(cudaMemset(valid.p, 0, sizeof(int)));
+    }
+    PlanReuse reuse() { return PlanReuse{saved_used.p, saved_bits.p, saved_cnt.p, valid.p}; }
 };
 
 // Bounded plans (at most 256 keys: 512 key flags, 2,048 pair-bitmap words):
@@ -1116,12 +1285,30 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
                                                      int max_tiles, int* __restrict__ first, int* __restrict__ tile0,
                                                      int* __restrict__ tile_batch, int* __restrict__ tile_col0,
                                                      int* __restrict__ tile_ncols, int* __restrict__ rowPair,
-                                                     int* __restrict__ rowKey, PlanCounts* __restrict__ cnt) {
+                                                     int* __restrict__ rowKey, PlanCounts* __restrict__ cnt,
+                                                     PlanReuse reuse) {
     pdl_wait();
     pdl_release();
     __shared__ uint32_t ws[32], total, nku_s;
     __shared__ uint32_t s_bits[PLAN_SMALL_WORDS], s_pre[PLAN_SMALL_WORDS];
     __shared__ int s_aId[PLAN_SMALL_KEYS], s_aKey[PLAN_SMALL_KEYS];
+    if (reuse.valid && *reuse.valid) {
+        // the saved plan stands if this list marked the same keys and pairs
+        bool same = true;
+        for (i64 i = threadIdx.x; i < 2 * nk; i += blockDim.x) same = same && used[i] == reuse.saved_used[i];
+        for (i64 w = threadIdx.x; w < words; w += blockDim.x) same = same && bits[w] == reuse.saved_bits[w];
+        if (__syncthreads_and(same)) {
+            if (threadIdx.x == 0) {
+                const PlanCounts c = *reuse.saved_cnt;
+                cnt->key_total = c.key_total;
+                cnt->nku = c.nku;
+                cnt->nA = c.nA;
+                cnt->nP = c.nP;
+                cnt->overflow = 0;
+            }
+            return;
+        }
+    }
     // keys: joint scan of [usedKey | usedA]
     const int k = threadIdx.x;  // flag k of 2 nk (<= 512)
     const uint32_t f = k < 2 * nk ? used[k] : 0u;
@@ -1159,6 +1346,7 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
     const bool over = nA > capA || (i64)nP > capP;  // the same on every thread
     if (over && tile_ncols)
         for (int t = threadIdx.x; t < max_tiles; t += blockDim.x) tile_ncols[t] = 0;  // stage B: no tiles
+    if (over && reuse.valid && threadIdx.x == 0) *reuse.valid = 0;
     if (threadIdx.x == 0) {
         cnt->key_total = over ? 0 : key_total;
         cnt->nku = over ? 0 : nku;
@@ -1186,6 +1374,21 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
     if (first)
         pair_tiles_block(true, pairA, pairB, aKey, nP, nA, (int)nku, bn, max_tiles, first, tile0, tile_batch,
                          tile_col0, tile_ncols, rowPair, rowKey);
+    if (reuse.valid) {
+        // save what this plan was made from, for the next replay's check
+        for (i64 i = threadIdx.x; i < 2 * nk; i += blockDim.x) reuse.saved_used[i] = used[i];
+        for (i64 w = threadIdx.x; w < words; w += blockDim.x) reuse.saved_bits[w] = s_bits[w];
+        if (threadIdx.x == 0) {
+            PlanCounts c;
+            c.key_total = key_total;
+            c.nku = nku;
+            c.nA = nA;
+            c.nP = nP;
+            c.overflow = 0;
+            *reuse.saved_cnt = c;
+            *reuse.valid = 1;
+        }
+    }
 }
 
 // G sliced once per table set (cached with the tables); the build synchronises
@@ -1328,7 +1531,7 @@ static bool sized_plan_fits(i64 nk) { return nk <= PLAN_SMALL_KEYS && (nk * nk +
 // the host sizes buffers and grids by `sz` (an input for PLAN_SIZED, an output
 // otherwise).
 static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
-                         cudaStream_t s) {
+                         cudaStream_t s, PlanStore* ps = nullptr) {
     const bool bounded = mode == PLAN_BOUNDED;
     const LatticeTables& t = *a.t;
     const i64 nk = t.nkeys, m = a.m;
@@ -1363,14 +1566,34 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     DevBuf<uint64_t> keys(m, s);
     {
         const size_t lb = mark_local_bytes(nk);
-        const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-        launch_pdl(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad, lb ? 1 : 0);
+        if (dec.pd) {
+            const i64 groups = (m + 3) / 4;
+            const unsigned mb = (unsigned)std::min<i64>((groups + 255) / 256, (i64)a.num_sms * 8);
+            launch_pdl(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
+                       lb ? 1 : 0);
+        } else {
+            const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
+            launch_pdl(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
+                       lb ? 1 : 0);
+        }
     }
-    DevBuf<uint64_t> ids(2 * nk, s);
-    DevBuf<int> keyOf(nk, s), aId(nk, s), aKey(nk, s);
-    DevBuf<uint64_t> pairPre(words, s);
+    DevBuf<uint64_t> ids, pairPre;
+    DevBuf<int> keyOf, aId, aKey;
     DevBuf<int> pairA, pairB;
     PairTiles tiles;
+    if (ps) {  // a sized graph's plan, kept between its replays
+        ids.borrow(ps->ids.p, 2 * nk, s);
+        keyOf.borrow(ps->keyOf.p, nk, s);
+        aId.borrow(ps->aId.p, nk, s);
+        aKey.borrow(ps->aKey.p, nk, s);
+        pairPre.borrow(ps->pairPre.p, words, s);
+    } else {
+        ids.alloc(2 * nk, s);
+        keyOf.alloc(nk, s);
+        aId.alloc(nk, s);
+        aKey.alloc(nk, s);
+        pairPre.alloc(words, s);
+    }
     const bool small_pairs = (bounded || mode == PLAN_SIZED) && words <= 8 * 1024;
     if (mode == PLAN_SIZED && !(small_pairs && nk <= PLAN_SMALL_KEYS))
         fail(GLI_ERR_INTERNAL, "sized plan for a key space of %lld keys", (long long)nk);
@@ -1385,13 +1608,21 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         // plans; for exact plans, whose counts are read back half way, the
         // single block's pass over nk^2 pair slots measured no faster than the
         // multi-block path: ERI 7^3 0.206 against 0.200 ms)
-        pairA.alloc(sz.nP, s);
-        pairB.alloc(sz.nP, s);
         const bool sliced = stage_b_sliced(a.mixed, sz.nA, sz.nP, U);
-        tiles.alloc(sz.nA, sz.nP, sliced ? tile_n(MIXED_SLICES) : DM_BM, !sliced, s);
+        const int tbn = sliced ? tile_n(MIXED_SLICES) : DM_BM;
+        if (ps) {
+            pairA.borrow(ps->pairA.p, sz.nP, s);
+            pairB.borrow(ps->pairB.p, sz.nP, s);
+            tiles.alloc(sz.nA, sz.nP, tbn, !sliced, s, ps->tiles.p);
+        } else {
+            pairA.alloc(sz.nP, s);
+            pairB.alloc(sz.nP, s);
+            tiles.alloc(sz.nA, sz.nP, tbn, !sliced, s);
+        }
         launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
-                   tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt);
+                   tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt,
+                   ps ? ps->reuse() : PlanReuse{});
         tiles.built = true;
     } else {
         if (2 * nk <= 1024) {
@@ -1522,15 +1753,29 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                        tiles.rowPair, tiles.rowKey);
         }
         const i64 max_tiles = tiles.max_tiles;
-        // the tile count is known on the device only: the split follows its bound
+        // the tile list is built on the device; the grid follows its bound and
+        // the split follows the tiles that hold pairs: with exact counts (exact
+        // and sized plans) those are known -- a full pair triangle with
+        // balanced hosts fills sum_h ceil(rows_h / 64) tiles, other pair sets
+        // about nP / 64 + nA / 2 -- with bounded plans the bound stands in
         // (64 u per tile: 80-row K-major gathers measured slower, ERIDA 129^3
         // stage B 0.32 against 0.21 ms)
+        i64 active = max_tiles;
+        if (!bounded) {
+            if (nku == nA && nP == nA * (nA + 1) / 2 && nA > DM_BM) {
+                const int y = (int)std::min<i64>(nA, 2 * DM_BM - 1);
+                active = 0;
+                for (int h = 0; h < (int)nA; ++h) active += (bal_count(h, (int)nA, y) + DM_BM - 1) / DM_BM;
+            } else {
+                active = std::min<i64>(max_tiles, (nP + DM_BM - 1) / DM_BM + nA / 2);
+            }
+        }
         const unsigned ub = (unsigned)((U + DM_BN - 1) / DM_BN);
         int v_chunk = U;
-        const int P = split_count(max_tiles * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
+        const int P = split_count(active * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
         // a split sums its parts inside a cluster of the P blocks of a tile
         const dim3 grid((unsigned)max_tiles, ub, (unsigned)P);
-        if ((i64)max_tiles * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
+        if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
             dmma_launch_cluster(StageBOp<false>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch,
                                                 tiles.col0, tiles.ncols, nS, U, Up, v_chunk, 0, H2.p},
                                 grid, s);
@@ -1569,7 +1814,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up, (int)nku,
                                   u_chunk, ps, Q.p, &st->products},
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
-        const unsigned gq = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
+        const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
         launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk, pairBits.p,
                    pairPre.p, (int)nku, cnt, c_prod, a.out);
     }
@@ -1605,6 +1850,7 @@ struct GraphEntry {
     long long launches = 0;  // kernels in the graph
     PlanMode mode = PLAN_BOUNDED;
     EvalSizes sz;            // the sizes a PLAN_SIZED graph was captured with
+    std::unique_ptr<PlanStore> plan;  // a PLAN_SIZED graph's plan, kept between replays
     int paths = 0;           // tensor-core stages of the captured evaluation
     DevMem<EvalStatus> status;
     ~GraphEntry() {
@@ -1670,13 +1916,18 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<80>, true>();
     dmma_prepare<StageBOp<true>, true>();
     dmma_prepare<StageBOp<false>, true>();
+    if (mode == PLAN_SIZED) {
+        const i64 nk = a.t->nkeys, words = (nk * nk + 31) / 32;
+        e->plan = std::make_unique<PlanStore>();
+        e->plan->alloc(nk, words, sized.nA, sized.nP, PairTiles::ints(sized.nA, sized.nP, 64, true));
+    }
     const long long l0 = launch_count();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     try {
         StageTimer timer(false, s);
         EvalSizes sz = sized;
-        enqueue_eval(a, mode, e->status.p, timer, sz, s);
+        enqueue_eval(a, mode, e->status.p, timer, sz, s, e->plan.get());
     } catch (...) {
         cudaStreamEndCapture(s, &graph);
         if (graph) cudaGraphDestroy(graph);

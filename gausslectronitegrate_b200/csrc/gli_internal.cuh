@@ -98,19 +98,28 @@ struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
     cudaStream_t s = 0;
+    bool owned = true;  // false: memory lent by a longer-lived owner, not freed here
     DevBuf() = default;
     DevBuf(size_t count, cudaStream_t stream) { alloc(count, stream); }
     void alloc(size_t count, cudaStream_t stream) {
         release();
         s = stream;
         n = count;
+        owned = true;
         if (count) GLI_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), stream));
+    }
+    void borrow(T* mem, size_t count, cudaStream_t stream) {
+        release();
+        s = stream;
+        n = count;
+        owned = false;
+        p = mem;
     }
     void zero() {
         if (n) GLI_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
     }
     void release() {
-        if (p) cudaFreeAsync(p, s);
+        if (p && owned) cudaFreeAsync(p, s);
         p = nullptr;
         n = 0;
     }
