@@ -763,12 +763,26 @@ __global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, doub
 // `grain`) so that a launch of `blocks` blocks reaches about `target` blocks:
 // small problems otherwise leave most SMs idle while each block walks the
 // whole loop.
+// The split minimises waves x chunks per block: `target` blocks run in one
+// wave, and a block's time grows with the K chunks it walks (ERIDA 33^3 stage
+// A: 170 tiles, three parts took two waves of 4 chunks, two parts one wave of
+// 6; ERI 7^3 stage A likewise two parts instead of three).
 static int split_count(i64 blocks, int U, int grain, i64 target, int* chunk) {
-    int P = (int)std::min<i64>((target + blocks - 1) / blocks, (U + grain - 1) / grain);
-    P = std::max(1, std::min(P, 8));
-    *chunk = ((U + P - 1) / P + grain - 1) / grain * grain;
-    P = (U + *chunk - 1) / *chunk;
-    return P;
+    const int most = (int)std::min<i64>(8, (U + grain - 1) / grain);
+    int best = 1;
+    i64 best_cost = -1;
+    for (int P = 1; P <= std::max(1, most); ++P) {
+        const int c = ((U + P - 1) / P + grain - 1) / grain * grain;
+        const int parts = (U + c - 1) / c;
+        const i64 waves = (blocks * parts + target - 1) / target;
+        const i64 cost = waves * (c / grain);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = parts;
+        }
+    }
+    *chunk = ((U + best - 1) / best + grain - 1) / grain * grain;
+    return (U + *chunk - 1) / *chunk;
 }
 
 // column-tile width of the FP64 tensor-core GEMM for n columns: 80 where it
