@@ -300,51 +300,57 @@ def run_ours(args):
     scale = 1.0 / SPACING  # grid units -> Hartree at this spacing
     max_abs_err_ha = float(np.max(np.abs(vals["mixed"] - vals["fp64"])) * scale)
 
-    def timed(name, steps, sample_clocks):
-        f = FORMS[name]
-        for _ in range(max(args.warmup, 3)):
-            step(f)
+    def timed_forms(steps):
+        """Both forms timed under the same conditions: after warm-up, their
+        timed steps alternate (chosen, other, chosen, ...), each behind its own
+        L2 flush, while the clock sampler runs."""
+        for name in (chosen, other):
+            for _ in range(max(args.warmup, 3)):
+                step(FORMS[name])
         stream.synchronize()
-        clocks = None
-        if sample_clocks:
-            # nvidia-smi samples every 200 ms, longer than the timed steps: the
-            # sampler runs across one second of further (untimed) steps of the
-            # same form that end where the timed steps begin
-            clocks = Clocks(local)
-            t_end = time.perf_counter() + 1.0
-            while time.perf_counter() < t_end:
-                for _ in range(20):
-                    step(f)
-                stream.synchronize()
+        # nvidia-smi samples every 200 ms, longer than the timed steps: the
+        # sampler runs across one second of further (untimed) steps of both
+        # forms that end where the timed steps begin, and across the timed steps
+        clocks = Clocks(local)
+        t_end = time.perf_counter() + 1.0
+        while time.perf_counter() < t_end:
+            for _ in range(10):
+                step(FORMS[chosen])
+                step(FORMS[other])
+            stream.synchronize()
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
-        launches0 = L.gli_b200_launch_count()
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ev = {n: ([torch.cuda.Event(enable_timing=True) for _ in range(steps)],
+                  [torch.cuda.Event(enable_timing=True) for _ in range(steps)]) for n in (chosen, other)}
+        launches = 0
         t_wall = time.perf_counter()
         for k in range(steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()  # L2 flush between timed steps, outside the events
-                starts[k].record(stream)
-            step(f)
-            with torch.cuda.stream(stream):
-                ends[k].record(stream)
+            for name in (chosen, other):
+                with torch.cuda.stream(stream):
+                    flush.zero_()  # L2 flush between timed steps, outside the events
+                    ev[name][0][k].record(stream)
+                l0 = L.gli_b200_launch_count()
+                step(FORMS[name])
+                if name == chosen:
+                    launches += L.gli_b200_launch_count() - l0
+                with torch.cuda.stream(stream):
+                    ev[name][1][k].record(stream)
         stream.synchronize()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t_wall
-        clk = clocks.stop() if clocks else None
-        if clk is not None:
-            clk["window"] = "1 s of untimed steps of the same form ending where the timed steps begin, and the timed steps"
-        launches = L.gli_b200_launch_count() - launches0
-        my_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
-        value, total_ms = weak_scaling_value(my_ms, m, steps, ws, f"cuda:{local}")
-        return {"value": value, "ms_per_step": total_ms / steps, "wall_s": wall, "launches": launches,
-                "clocks": clk}
+        clk = clocks.stop()
+        clk["window"] = "1 s of untimed steps of both forms ending where the timed steps begin, and the timed steps"
+        out = {}
+        for name in (chosen, other):
+            my_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(*ev[name]))
+            value, total_ms = weak_scaling_value(my_ms, m, steps, ws, f"cuda:{local}")
+            out[name] = {"value": value, "ms_per_step": total_ms / steps, "wall_s": wall, "launches": launches,
+                         "clocks": clk}
+        return out[chosen], out[other]
 
     log("timed steps")
-    main = timed(chosen, args.steps, True)
-    side = timed(other, args.steps, False)
+    main, side = timed_forms(args.steps)
 
     # arithmetic that ran in each form (the library's report of its last evaluation)
     paths = {}

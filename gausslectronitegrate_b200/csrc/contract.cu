@@ -748,6 +748,104 @@ struct StageBOp {
     }
 };
 
+// Stage B with the expanded H rows in memory: Hf[a][v][u] = H[a][sidx[v U + u]]
+// (pitch Up in u), written once per evaluation by k_expand_h where all of it
+// fits comfortably in L2 (small lattices: ERI 7^3 17 MB).  The B tile is then
+// two consecutive u of one v per 16-byte copy, with no index load in front of
+// each gather.  Otherwise as StageBOp (same tiles, rows and stores).
+__global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__ sidx, const PlanCounts* __restrict__ cnt,
+                           i64 nS, int U, int Up, double* __restrict__ Hf) {
+    pdl_wait();
+    pdl_release();
+    const i64 per = (i64)U * Up, total = cnt->nA * per;
+    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
+        const i64 a = e / per;
+        const int r = (int)(e - a * per), v = r / Up, u = r - v * Up;
+        Hf[e] = u < U ? H[a * nS + __ldg(&sidx[v * U + u])] : 0.0;
+    }
+}
+
+template <bool DEEP>
+struct StageBDenseOp {
+    static constexpr bool A_KMAJOR = false, B_KMAJOR = true;
+    static constexpr int BN = DM_BN;
+    static constexpr int STAGES = DEEP ? 3 : 2, MIN_BLOCKS = DEEP ? 3 : 4;
+    const double* W;
+    const double* Hf;  // [a][v][u], pitch Up
+    const int* rowKey;
+    const int* rowPair;
+    const int* tile_batch;
+    const int* tile_col0;
+    const int* tile_ncols;
+    int U, Up, v_chunk;
+    i64 part_stride;
+    double* H2;
+    struct Block {
+        int mvalid, nvalid, nk;
+        int p0, u0, v0, v1;
+        const double* h;  // Hf block of the tile's A key
+        double* H2;
+    };
+    struct AState {
+        i64 off[DM_BM / 16];
+    };
+    struct BState {};
+    __device__ bool begin(Block& b) const {
+        const int tile = blockIdx.x;
+        b.mvalid = tile_ncols[tile];
+        if (b.mvalid <= 0) return false;
+        b.p0 = tile_col0[tile];
+        b.h = Hf + (i64)tile_batch[tile] * U * Up;
+        b.u0 = blockIdx.y * DM_BN;
+        b.nvalid = min(DM_BN, U - b.u0);
+        b.v0 = blockIdx.z * v_chunk;
+        b.v1 = min(U, b.v0 + v_chunk);
+        b.nk = (b.v1 - b.v0 + DM_BK - 1) / DM_BK;
+        b.H2 = H2 + (i64)blockIdx.z * part_stride;
+        return b.nk > 0;
+    }
+    __device__ void a_init(const Block& b, AState& st) const {
+#pragma unroll
+        for (int q = 0; q < DM_BM / 16; ++q) {
+            const int r = dm_pair_row(threadIdx.x, q);
+            st.off[q] = r < b.mvalid ? (i64)rowKey[b.p0 + r] * Up : -1;
+        }
+    }
+    __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
+        const int k = dm_pair_k(threadIdx.x), v = b.v0 + kc * DM_BK + k;
+        const int bytes = dm_pair_bytes(v, b.v1);
+#pragma unroll
+        for (int q = 0; q < DM_BM / 16; ++q) {
+            const int n = st.off[q] >= 0 ? bytes : 0;
+            dm_cp16(tile + dm_rowmajor_at(dm_pair_row(threadIdx.x, q), k), n ? W + st.off[q] + v : W, n);
+        }
+    }
+    __device__ void b_init(const Block&, BState&) const {}
+    // pairs of rows (u, u + 1) at one k = v: 64 rows x 16 k = 512 pairs, four
+    // per thread; Up is a multiple of 4 and u0 of 64, so the pairs are 16-byte
+    // aligned in Hf and (68 doubles per k) in the K-major tile
+    __device__ void b_issue(const Block& b, BState&, int kc, double* tile) const {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int pidx = threadIdx.x + DM_THREADS * q, rp = pidx & 31, k = pidx >> 5;
+            const int n = 2 * rp, u = b.u0 + n, v = b.v0 + kc * DM_BK + k;
+            const int bytes = (v < b.v1 && n < b.nvalid) ? (n + 1 < b.nvalid ? 16 : 8) : 0;
+            dm_cp16(tile + dm_kmajor_at(n, k), bytes ? b.h + (i64)v * Up + u : b.h, bytes);
+        }
+    }
+    __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
+        if (m >= b.mvalid) return;
+        double* h2 = b.H2 + (i64)__ldg(&rowPair[b.p0 + m]) * Up + b.u0 + n;
+        if (n + 1 < b.nvalid)
+            *reinterpret_cast<double2*>(h2) = make_double2(v0, v1);
+        else if (n < b.nvalid)
+            h2[0] = v0;
+    }
+};
+
+// the expanded H of stage B held in memory when it takes at most this many bytes
+constexpr i64 DENSE_HF_BYTES = (i64)48 << 20;
+
 // out[i] = sum_p parts[p n + i], in order of p (deterministic)
 __global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, double* __restrict__ out) {
     pdl_wait();
@@ -1492,6 +1590,15 @@ struct EvalSizes {
 // product form of stage C.
 constexpr i64 BOUNDED_KEYS = 256;
 
+// (GLI_B200_DENSE_HF_BYTES overrides the dense stage-B threshold, for measurements)
+static i64 dense_hf_bytes() {
+    static const i64 v = [] {
+        const char* e = getenv("GLI_B200_DENSE_HF_BYTES");
+        return e && *e ? (i64)atoll(e) : DENSE_HF_BYTES;
+    }();
+    return v;
+}
+
 // stage A runs on the tensor cores (mixed form) from this many outputs nA nS
 // (GLI_B200_TC_A_OUTPUTS overrides it, for measurements)
 constexpr i64 TC_A_OUTPUTS = 1000000;
@@ -1789,7 +1896,20 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         const int P = split_count(active * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
         // a split sums its parts inside a cluster of the P blocks of a tile
         const dim3 grid((unsigned)max_tiles, ub, (unsigned)P);
-        if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
+        const i64 hf_doubles = nA * (i64)U * Up;
+        if (8 * hf_doubles <= dense_hf_bytes()) {
+            DevBuf<double> Hf(hf_doubles, s);
+            const unsigned eb = (unsigned)std::min<i64>((hf_doubles + 255) / 256, (i64)a.num_sms * 16);
+            launch_pdl(k_expand_h, dim3(eb), dim3(256), 0, s, H.p, t.sidx.p, cnt, (i64)nS, U, Up, Hf.p);
+            if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
+                dmma_launch_cluster(StageBDenseOp<false>{t.W.p, Hf.p, tiles.rowKey, tiles.rowPair, tiles.batch,
+                                                         tiles.col0, tiles.ncols, U, Up, v_chunk, 0, H2.p},
+                                    grid, s);
+            else
+                dmma_launch_cluster(StageBDenseOp<true>{t.W.p, Hf.p, tiles.rowKey, tiles.rowPair, tiles.batch,
+                                                        tiles.col0, tiles.ncols, U, Up, v_chunk, 0, H2.p},
+                                    grid, s);
+        } else if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
             dmma_launch_cluster(StageBOp<false>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch,
                                                 tiles.col0, tiles.ncols, nS, U, Up, v_chunk, 0, H2.p},
                                 grid, s);
@@ -1930,6 +2050,10 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<80>, true>();
     dmma_prepare<StageBOp<true>, true>();
     dmma_prepare<StageBOp<false>, true>();
+    dmma_prepare<StageBDenseOp<true>>();
+    dmma_prepare<StageBDenseOp<false>>();
+    dmma_prepare<StageBDenseOp<true>, true>();
+    dmma_prepare<StageBDenseOp<false>, true>();
     if (mode == PLAN_SIZED) {
         const i64 nk = a.t->nkeys, words = (nk * nk + 31) / 32;
         e->plan = std::make_unique<PlanStore>();
