@@ -1810,8 +1810,11 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         const unsigned mb = (unsigned)((nS + DM_BM - 1) / DM_BM);
         const int bn = (nA > 128 && nA <= 144) ? 144 : col_tile(nA);
         const unsigned nb = (unsigned)((nA + bn - 1) / bn);
+        // (the 144-column tiles are not split: their partial tiles would need the
+        // summing pass over HBM, which measured slower at ERIDA 129^3, 0.439
+        // against 0.410 ms)
         int t_chunk = U;
-        const int P = split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
+        const int P = bn == 144 ? 1 : split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
         const i64 ps = nA * (i64)nS;
         const dim3 grid(mb, nb, (unsigned)P);
         if (bn == 144) {
