@@ -861,10 +861,13 @@ __global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, doub
 // `grain`) so that a launch of `blocks` blocks reaches about `target` blocks:
 // small problems otherwise leave most SMs idle while each block walks the
 // whole loop.
-// The split minimises waves x chunks per block: `target` blocks run in one
+// The split minimises waves x time per block: `target` blocks run in one
 // wave, and a block's time grows with the K chunks it walks (ERIDA 33^3 stage
 // A: 170 tiles, three parts took two waves of 4 chunks, two parts one wave of
-// 6; ERI 7^3 stage A likewise two parts instead of three).
+// 6; ERI 7^3 stage A likewise two parts instead of three: 25 -> 21 us).
+// A block also pays a fixed cost of about three chunks (pipeline fill, drain
+// and store), and a split block two more for the cluster sum (measured: ERI
+// 7^3 stage B 27 us unsplit, 37 us in two parts, 48 us in five).
 static int split_count(i64 blocks, int U, int grain, i64 target, int* chunk) {
     const int most = (int)std::min<i64>(8, (U + grain - 1) / grain);
     int best = 1;
@@ -873,7 +876,7 @@ static int split_count(i64 blocks, int U, int grain, i64 target, int* chunk) {
         const int c = ((U + P - 1) / P + grain - 1) / grain * grain;
         const int parts = (U + c - 1) / c;
         const i64 waves = (blocks * parts + target - 1) / target;
-        const i64 cost = waves * (c / grain);
+        const i64 cost = waves * (c / grain + 3 + (parts > 1 ? 2 : 0));
         if (best_cost < 0 || cost < best_cost) {
             best_cost = cost;
             best = parts;
@@ -1051,56 +1054,70 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
     pdl_wait();
     pdl_release();
     if (cnt->overflow || !choice_runs(choice, cnt, m)) return;
-    // four consecutive classes per thread (16-byte loads and stores where the
-    // arrays allow): each class is a chain of dependent loads (keys, then pair
-    // id and key id, then Q); the four chains run side by side, and a pair id
-    // equal to the previous class's is not looked up again
+    // four consecutive classes per group, two groups per thread and step
+    // (16-byte loads and stores where the arrays allow): each class is a chain
+    // of dependent loads (keys, then pair id and key id, then Q); the eight
+    // chains run side by side, and a pair id equal to the previous class's is
+    // not looked up again
     const bool vec = keys && ((uintptr_t)keys & 15) == 0 && ((uintptr_t)out & 15) == 0;
-    const i64 groups = (m + 3) / 4;
-    for (i64 g = (i64)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (i64)gridDim.x * blockDim.x) {
-        const i64 n0 = 4 * g;
-        const bool full = n0 + 3 < m;
-        uint64_t p[4];
-        if (vec && full) {
-            const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(keys + n0));
-            const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(keys + n0 + 2));
-            p[0] = a.x, p[1] = a.y, p[2] = b.x, p[3] = b.y;
-        } else {
+    const i64 groups = (m + 3) / 4, stride = (i64)gridDim.x * blockDim.x;
+    constexpr int G = 2;
+    for (i64 g0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; g0 < groups; g0 += G * stride) {
+        uint64_t p[G][4];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) p[v] = n0 + v < m ? class_packed(keys, dec, idx, n0 + v) : BAD_KEYS;
+        for (int h = 0; h < G; ++h) {
+            const i64 n0 = 4 * (g0 + h * stride);
+            if (vec && n0 + 3 < m) {
+                const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(keys + n0));
+                const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(keys + n0 + 2));
+                p[h][0] = a.x, p[h][1] = a.y, p[h][2] = b.x, p[h][3] = b.y;
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) p[h][v] = n0 + v < m ? class_packed(keys, dec, idx, n0 + v) : BAD_KEYS;
+            }
         }
-        i64 q[4];
-        i64 last_slot = -1, last_pid = 0;
+        i64 q[G][4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            q[v] = -1;
-            if (p[v] != BAD_KEYS) {
-                int k[3];
-                unpack_keys(p[v], k);
-                const i64 slot = (i64)k[1] * nk + k[0];
-                if (slot != last_slot) {
-                    last_slot = slot;
-                    last_pid = pair_id(pairBits, pairPre, slot);
+        for (int h = 0; h < G; ++h) {
+            i64 last_slot = -1, last_pid = 0;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                q[h][v] = -1;
+                if (p[h][v] != BAD_KEYS) {
+                    int k[3];
+                    unpack_keys(p[h][v], k);
+                    const i64 slot = (i64)k[1] * nk + k[0];
+                    if (slot != last_slot) {
+                        last_slot = slot;
+                        last_pid = pair_id(pairBits, pairPre, slot);
+                    }
+                    q[h][v] = last_pid * ldq + (i64)kid[k[2]];
                 }
-                q[v] = last_pid * ldq + (i64)kid[k[2]];
             }
         }
-        double acc[4];
+        double acc[G][4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            acc[v] = 0.0;
-            if (q[v] >= 0 && dcheck(q[v] < part_stride, 3, q[v])) {
-                acc[v] = Q[q[v]];
-                for (int z = 1; z < parts; ++z) acc[v] += Q[z * part_stride + q[v]];
+        for (int h = 0; h < G; ++h)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                acc[h][v] = 0.0;
+                if (q[h][v] >= 0 && dcheck(q[h][v] < part_stride, 3, q[h][v])) {
+                    acc[h][v] = Q[q[h][v]];
+                    for (int z = 1; z < parts; ++z) acc[h][v] += Q[z * part_stride + q[h][v]];
+                }
             }
-        }
-        if (vec && full) {
-            reinterpret_cast<double2*>(out + n0)[0] = make_double2(acc[0], acc[1]);
-            reinterpret_cast<double2*>(out + n0)[1] = make_double2(acc[2], acc[3]);
-        } else {
 #pragma unroll
-            for (int v = 0; v < 4; ++v)
-                if (n0 + v < m) out[n0 + v] = acc[v];
+        for (int h = 0; h < G; ++h) {
+            const i64 n0 = 4 * (g0 + h * stride);
+            if (n0 >= m) continue;
+            if (vec && n0 + 3 < m) {
+                reinterpret_cast<double2*>(out + n0)[0] = make_double2(acc[h][0], acc[h][1]);
+                reinterpret_cast<double2*>(out + n0)[1] = make_double2(acc[h][2], acc[h][3]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v)
+                    if (n0 + v < m) out[n0 + v] = acc[h][v];
+            }
         }
     }
 }
