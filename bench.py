@@ -442,6 +442,7 @@ def run_ours(args):
     st = stage[chosen]
     dom = max(("A", "B", "C"), key=lambda k: st[k])
     roof = roofline(paths[chosen], dom, st, st["plan"], U, m, peak.value)
+    roof["traffic"] = measured_traffic(f"{args.workload}:{dom}{':tc' if roof['bound'] == 'hbm' and dom in 'AB' else ''}")
     line = {
         "metric": METRIC, "value": main["value"], "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": main["ms_per_step"], "higher_is_better": True,
@@ -604,7 +605,8 @@ def run_kinetic(args):
                    "l2": "inputs larger than L2 (1.53 GB written per step)"},
         "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak["hbm_gbs"], "unit": "GB/s",
                      "frac": gbs / peak["hbm_gbs"], "kernel": "k_kinetic_matrix",
-                     "peak_source": peak_source(peak), "traffic": None},
+                     "peak_source": peak_source(peak),
+                     "traffic": measured_traffic("kinetic24")},
         "e2e": {"value": bytes_ / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 8 * b.size,
                 "d2h_bytes_per_step": bytes_},
         "clocks": clk}), flush=True)
@@ -878,6 +880,18 @@ def roofline(paths, dom, st, plan, U, m, fp64_peak):
             "frac": achieved / peak if achieved and peak else None,
             "peak_source": peak_source(mp),
             "algorithmic_bytes_per_launch": bytes_, "traffic": None}
+
+
+def measured_traffic(key):
+    """DRAM bytes per launch of a workload's dominant kernel (key: the workload,
+    or workload:stage) from the committed ncu summaries
+    (profiles/dram_traffic.json), or None when no capture of it exists."""
+    try:
+        with open(os.path.join(REPO, "profiles", "dram_traffic.json")) as f:
+            d = json.load(f).get(key)
+        return d["bytes_per_launch"] if d else None
+    except Exception:
+        return None
 
 
 def peak_source(mp):
