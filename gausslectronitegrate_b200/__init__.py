@@ -245,9 +245,25 @@ def compute_kinetic_gausslet_integrals(gausslet_coeffs, grid):
     L.compute_kinetic_gausslet_integrals(C.byref(g), C.byref(_grid_struct(spec)), C.byref(out))
     _raise_if_failed(syntax)
     n = spec[0][1] * spec[1][1] * spec[2][1]
-    res = np.ctypeslib.as_array(out.integral_values, shape=(n, n)).copy()
-    L.delete_kinetic_gausslet_integrals(C.byref(out))
-    return res
+    return _adopt_matrix(out, n, L.delete_kinetic_gausslet_integrals)
+
+
+class _OwnedMatrix:
+    """A dense matrix that the library allocated in a result struct, handed
+    to numpy without a copy: numpy keeps this object as the array's base, and
+    the struct's delete_* runs when the array goes away."""
+
+    def __init__(self, struct, n, deleter):
+        self._struct, self._deleter = struct, deleter
+        self.__array_interface__ = {"data": (C.cast(struct.integral_values, C.c_void_p).value, False),
+                                    "shape": (n, n), "typestr": "<f8", "version": 3}
+
+    def __del__(self):
+        self._deleter(C.byref(self._struct))
+
+
+def _adopt_matrix(struct, n, deleter):
+    return np.asarray(_OwnedMatrix(struct, n, deleter))
 
 
 # ---------------------------------------------------------------------------
@@ -277,9 +293,7 @@ def compute_nuclear_gausslet_integrals(gausslet_coeffs, grid, nuclear_positions,
                                          C.byref(out))
     _raise_if_failed(syntax)
     npts = spec[0][1] * spec[1][1] * spec[2][1]
-    res = np.ctypeslib.as_array(out.integral_values, shape=(npts, npts)).copy()
-    L.delete_nuclear_gausslet_integrals(C.byref(out))
-    return res
+    return _adopt_matrix(out, npts, L.delete_nuclear_gausslet_integrals)
 
 
 def compute_nuclear_gausslet_integrals_batch(gausslet_coeffs, grids, nuclear_positions, nuclear_charges, tol,

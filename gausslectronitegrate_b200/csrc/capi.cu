@@ -7,6 +7,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <thread>
+#include <vector>
 #include <new>
 
 #include "gli_internal.cuh"
@@ -48,9 +50,69 @@ void to_device(DevBuf<T>& d, const T* h, i64 n, cudaStream_t s) {
     if (n) GLI_CUDA(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
+// Large device -> host copies into pageable memory (dense kinetic and nuclear
+// matrices, dense tensors: up to GBs) go through two page-locked staging
+// buffers: the DMA of one chunk overlaps the host copy of the previous one,
+// which is split over a few threads (one core's memcpy into freshly mapped
+// pages runs far below the link's rate).  Synchronous; smaller copies are one
+// asynchronous cudaMemcpyAsync on the stream.
+struct StagedD2H {
+    static constexpr size_t kChunk = (size_t)32 << 20;
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    void ensure() {
+        for (int k = 0; k < 2; ++k) {
+            if (!pin[k]) GLI_CUDA(cudaHostAlloc(&pin[k], kChunk, cudaHostAllocDefault));
+            if (!ev[k]) GLI_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+        }
+    }
+    ~StagedD2H() {
+        for (int k = 0; k < 2; ++k) {
+            if (pin[k]) cudaFreeHost(pin[k]);
+            if (ev[k]) cudaEventDestroy(ev[k]);
+        }
+    }
+};
+static thread_local StagedD2H t_staged;
+
+static void parallel_memcpy(void* dst, const void* src, size_t bytes) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<size_t>(std::min<size_t>(8, hw > 1 ? hw / 2 : 1), std::max<size_t>(1, bytes >> 22));
+    if (nt <= 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes / nt + 63) / 64 * 64;
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) {
+        const size_t b0 = std::min(bytes, k * part), b1 = std::min(bytes, (k + 1) * part);
+        if (b1 > b0) th.emplace_back([=] { memcpy((char*)dst + b0, (const char*)src + b0, b1 - b0); });
+    }
+    memcpy(dst, src, std::min(bytes, part));
+    for (auto& t : th) t.join();
+}
+
 template <class T>
 void to_host(T* h, const T* d, i64 n, cudaStream_t s) {
-    if (n) GLI_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+    const size_t bytes = (size_t)n * sizeof(T);
+    if (bytes < 2 * StagedD2H::kChunk) {
+        if (n) GLI_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s));
+        return;
+    }
+    t_staged.ensure();
+    const size_t chunks = (bytes + StagedD2H::kChunk - 1) / StagedD2H::kChunk;
+    for (size_t c = 0; c <= chunks; ++c) {
+        if (c < chunks) {
+            const size_t off = c * StagedD2H::kChunk, len = std::min(StagedD2H::kChunk, bytes - off);
+            GLI_CUDA(cudaMemcpyAsync(t_staged.pin[c & 1], (const char*)d + off, len, cudaMemcpyDeviceToHost, s));
+            GLI_CUDA(cudaEventRecord(t_staged.ev[c & 1], s));
+        }
+        if (c > 0) {  // the previous chunk: wait for its DMA, copy it out of the staging buffer
+            const size_t p = c - 1, off = p * StagedD2H::kChunk, len = std::min(StagedD2H::kChunk, bytes - off);
+            GLI_CUDA(cudaEventSynchronize(t_staged.ev[p & 1]));
+            parallel_memcpy((char*)h + off, t_staged.pin[p & 1], len);
+        }
+    }
 }
 
 void check_gdata(const struct gausslet_data* g) {
