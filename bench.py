@@ -9,22 +9,29 @@ Hartree.  Synthetic: the inputs are the coefficients and the grid.
 
 One step = one evaluation of every class value from the class list already
 resident in HBM (plan, staged contraction, write-back), i.e. one
-gli_b200_sparse_values_dev call with the lattice tables cached.  The class
+gli_b200_sparse_values_dev_async call (the stream-ordered form of
+gli_b200_sparse_values_dev) with the lattice tables cached; the statuses of the
+timed steps are read after the last one, and the synchronous call's step time
+is reported beside it (config.sync_call_ms_per_step).  The class
 enumeration is measured apart, and so is a cold step (caches dropped: tables,
 plan and graph built again inside the timed call).  The metric compares the
-two forms: `value` is the chosen form (--form, default mixed); the other form
+two forms: `value` is the chosen form (--form; the default, auto, takes the
+mixed form where it runs a stage on the tensor cores and FP64 where the mixed
+form keeps every stage in FP64, as at ERI 7^3); the other form
 is timed the same way beside it, and the mixed form's max abs error against
 the FP64 form (and both against the reference C core on a seeded sample) is
 reported in Hartree.  `dtype` names the arithmetic that ran, per stage, as the
 library reports it (gli_b200_last_paths).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form auto|mixed|fp64] [--impl ours|reference]
 
 Timing: W >= 3 untimed warm-up steps; each timed step is bracketed by CUDA
 events on the stream the library launches on; L2 (126 MB) is flushed by
-writing a 1 GB buffer between timed steps (outside the events).  Each library
-call synchronises (it reads back the evaluation's status), so the flush, about
-160 us on the device, is also the host's lead for queueing the next step.  The K
+writing a 1 GB buffer between timed steps (outside the events).  The queued
+steps run back to back on the device, each behind its flush; with the
+synchronous call the end event waits for the host's return after the status
+read-back (the flush, about 160 us on the device, is then the host's lead for
+queueing the next step).  The K
 steps are bracketed by a barrier and device synchronisation, and the slowest
 rank's time counts.  N > 1 (torchrun, one process per GPU): every rank
 evaluates its own copy of the workload (weak scaling, no data-path
@@ -250,7 +257,7 @@ def run_ours(args):
     L.gli_b200_set_device(local)
     FORMS = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}
     KIND_ID = _abi.GLI_KIND_ERI if KIND == "eri" else _abi.GLI_KIND_ERIDA
-    chosen = args.form
+    chosen = "mixed" if args.form == "auto" else args.form
     other = "fp64" if chosen == "mixed" else "mixed"
     b = np.ascontiguousarray(g10())
     spec = grid_spec()
@@ -282,6 +289,20 @@ def run_ours(args):
         if rc:
             raise RuntimeError(L.gli_b200_last_error_message().decode())
 
+    def queue(f):
+        # the stream-ordered call: queued without a host wait; the status is
+        # read by wait() after the timed steps
+        t = _abi.glong()
+        rc = L.gli_b200_sparse_values_dev_async(KIND_ID, coeff_p, b.size, C.byref(gs), d_idx, m, TOL, f,
+                                                C.c_void_p(out.data_ptr()), sptr, C.byref(t))
+        if rc:
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+        return t.value
+
+    def wait(ticket):
+        if L.gli_b200_sparse_values_wait(ticket):
+            raise RuntimeError(L.gli_b200_last_error_message().decode())
+
     if args.profile_only:
         # untimed evaluations of the chosen form only (the command profilers run)
         for _ in range(args.profile_only):
@@ -292,18 +313,29 @@ def run_ours(args):
         return 0
 
     log(f"{m} classes; accuracy check")
-    vals = {}
+    vals, ran = {}, {}
     for name, f in FORMS.items():
         step(f)
         stream.synchronize()
         vals[name] = out.cpu().numpy().copy()
+        p3 = (C.c_int * 3)()
+        L.gli_b200_last_paths(p3)
+        ran[name] = tuple(int(x) for x in p3)
     scale = 1.0 / SPACING  # grid units -> Hartree at this spacing
     max_abs_err_ha = float(np.max(np.abs(vals["mixed"] - vals["fp64"])) * scale)
+    if args.form == "auto" and not (ran["mixed"][0] or ran["mixed"][1]):
+        # the mixed form keeps every stage of this workload in FP64 (its
+        # tensor-core stages do not pay at these sizes): the FP64 form leads
+        chosen, other = "fp64", "mixed"
+        log("the mixed form runs no tensor-core stage here: FP64 form reported")
 
-    def timed_forms(steps):
+    def timed_forms(steps, queued=True):
         """Both forms timed under the same conditions: after warm-up, their
         timed steps alternate (chosen, other, chosen, ...), each behind its own
-        L2 flush, while the clock sampler runs."""
+        L2 flush, while the clock sampler runs.  queued: each step is the
+        stream-ordered call (the statuses read after the last step); else the
+        synchronous call, whose return after its status read-back the end
+        event waits for."""
         for name in (chosen, other):
             for _ in range(max(args.warmup, 3)):
                 step(FORMS[name])
@@ -324,6 +356,7 @@ def run_ours(args):
         ev = {n: ([torch.cuda.Event(enable_timing=True) for _ in range(steps)],
                   [torch.cuda.Event(enable_timing=True) for _ in range(steps)]) for n in (chosen, other)}
         launches = 0
+        tickets = []
         t_wall = time.perf_counter()
         for k in range(steps):
             for name in (chosen, other):
@@ -331,11 +364,16 @@ def run_ours(args):
                     flush.zero_()  # L2 flush between timed steps, outside the events
                     ev[name][0][k].record(stream)
                 l0 = L.gli_b200_launch_count()
-                step(FORMS[name])
+                if queued:
+                    tickets.append(queue(FORMS[name]))
+                else:
+                    step(FORMS[name])
                 if name == chosen:
                     launches += L.gli_b200_launch_count() - l0
                 with torch.cuda.stream(stream):
                     ev[name][1][k].record(stream)
+        if tickets:
+            wait(tickets[-1])  # every step's status, in order
         stream.synchronize()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t_wall
@@ -351,6 +389,8 @@ def run_ours(args):
 
     log("timed steps")
     main, side = timed_forms(args.steps)
+    log("timed steps through the synchronous call")
+    main_sync, side_sync = timed_forms(args.steps, queued=False)
 
     # arithmetic that ran in each form (the library's report of its last evaluation)
     paths = {}
@@ -454,6 +494,9 @@ def run_ours(args):
                    "max_abs_err_ha_mixed_vs_fp64": max_abs_err_ha,
                    "forms": {chosen: {"classes_per_s": main["value"], "ms_per_step": main["ms_per_step"]},
                              other: {"classes_per_s": side["value"], "ms_per_step": side["ms_per_step"]}},
+                   "step_call": "gli_b200_sparse_values_dev_async (stream-ordered; statuses read after the timed "
+                                "steps, every step's status checked)",
+                   "sync_call_ms_per_step": {chosen: main_sync["ms_per_step"], other: side_sync["ms_per_step"]},
                    "mixed_over_fp64": (main["value"] / side["value"]) if chosen == "mixed" else
                    (side["value"] / main["value"]),
                    "enumeration_ms": enum_ms,
@@ -913,7 +956,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--form", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--form", choices=["auto", "fp64", "mixed"], default="auto",
+                    help="auto: the mixed form where it runs a stage on the tensor cores, else FP64")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shard", action="store_true",
@@ -932,6 +976,8 @@ def main():
         L_GRID, SPACING, WORKLOAD, KIND = WORKLOADS[args.workload]
     if args.cpu_baseline_json:
         return cpu_baseline_main(args.cpu_baseline_json)
+    if args.form == "auto" and (args.workload not in WORKLOADS or args.shard or args.profile_only):
+        args.form = "mixed"  # (the choice between the forms is made in the sparse-value line only)
     if args.workload == "nuclear-batch":
         return run_nuclear_batch(args)
     if args.workload == "kinetic24":

@@ -76,7 +76,8 @@ EXPORTS = [
     "evaluate_octahedral_grid_permutations",
     # extensions
     "gli_b200_last_error", "gli_b200_last_error_message", "gli_b200_device_count", "gli_b200_set_device",
-    "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
+    "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values_dev_async",
+    "gli_b200_sparse_values_wait", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
     "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_last_plan",
     "gli_b200_last_paths", "gli_b200_clear_caches", "gli_b200_measure_fp64_peak",
     "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
@@ -139,6 +140,9 @@ def load(path=LIB_PATH):
     L.gli_b200_version.restype = C.c_char_p
     L.gli_b200_sparse_values_dev.argtypes = [C.c_int, dptr, glong, P(Grid), C.c_void_p, glong, C.c_double, C.c_int,
                                              C.c_void_p, C.c_void_p]
+    L.gli_b200_sparse_values_dev_async.argtypes = [C.c_int, dptr, glong, P(Grid), C.c_void_p, glong, C.c_double,
+                                                   C.c_int, C.c_void_p, C.c_void_p, P(glong)]
+    L.gli_b200_sparse_values_wait.argtypes = [glong]
     L.gli_b200_sparse_values.argtypes = [C.c_int, P(GaussletData), P(Grid), lptr, glong, C.c_double, C.c_int, dptr]
     L.gli_b200_enumerate_dev.argtypes = [C.c_int, P(Grid), P(C.c_void_p), P(glong), C.c_void_p]
     L.gli_b200_free_dev.argtypes = [C.c_void_p, C.c_void_p]

@@ -703,6 +703,31 @@ int gli_b200_sparse_values_dev(int kind, const double* coeffs, glong num_coeffs,
     return gli::last_error();
 }
 
+// The same evaluation queued on the stream without a host wait (stream order:
+// no synchronisation inside once the list's graph exists); the ticket is
+// passed to gli_b200_sparse_values_wait, which reads the status.
+int gli_b200_sparse_values_dev_async(int kind, const double* coeffs, glong num_coeffs,
+                                     const struct cartesian_grid_3d* grid, const glong* d_indices, glong num,
+                                     double tol, int form, double* d_values, void* stream, glong* ticket) {
+    guarded([&] {
+        if (kind != 0 && kind != 1) gli::fail(GLI_ERR_ARGUMENT, "kind must be 0 (ERIDA) or 1 (ERI)");
+        if (!coeffs) gli::fail(GLI_ERR_ARGUMENT, "coefficients missing");
+        if (!ticket) gli::fail(GLI_ERR_ARGUMENT, "ticket missing");
+        if (num < 0) gli::fail(GLI_ERR_ARGUMENT, "num must be non-negative");
+        const gli::GridDesc g = gli::grid_desc(grid);
+        gli::Context& ctx = gli::context();
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx.stream;
+        *ticket = gli::sparse_values_device_async(kind, coeffs, num_coeffs, g, (const int64_t*)d_indices, num, tol,
+                                                  form, d_values, s);
+    });
+    return gli::last_error();
+}
+
+int gli_b200_sparse_values_wait(glong ticket) {
+    guarded([&] { gli::sparse_values_wait(ticket); });
+    return gli::last_error();
+}
+
 // Batched nuclear-attraction matrices: every instance its own grid and nuclei
 // (same coefficients and tol), outputs in device memory.  Batches the matrix
 // entry point compute_nuclear_gausslet_integrals (reference

@@ -141,10 +141,13 @@ __device__ __forceinline__ uint32_t pd_field(int dax, int sax) {
     return (uint32_t)abs(dax) | ((uint32_t)sax << 8);
 }
 
-// descriptor of every point pair h = p N + q (N^2 entries)
-__global__ void k_pair_desc(ClassDecode d, uint2* __restrict__ pd) {
+// descriptor of every point pair h = p N + q (N^2 entries); skip (sized
+// replays): when *skip is set the table kept with the replay's saved plan is
+// current (a function of the grid alone, made by the replay that made the plan)
+__global__ void k_pair_desc(ClassDecode d, uint2* __restrict__ pd, const int* __restrict__ skip) {
     pdl_wait();
     pdl_release();
+    if (skip && *skip) return;
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if ((uint64_t)h >= d.N2) return;
     const uint32_t p = h / d.n32, q = h - p * d.n32;
@@ -310,6 +313,35 @@ __device__ __forceinline__ uint64_t class_packed(const uint64_t* __restrict__ ke
     return class_keys(d, __ldg(&idx[n]), k) ? pack_keys(k) : BAD_KEYS;
 }
 
+// Sorted axis keys s0 <= s1 <= s2 of ERI class x through the pair
+// descriptors; (hi, da) carry the point pair (i, j) and its descriptor from
+// the previous class of the same thread (hi all ones: none), reused while the
+// remainder stays below N^2.  False for an index outside the tensor.
+__device__ __forceinline__ bool pd_class_keys(const ClassDecode& d, int64_t x, uint64_t& hi, uint2& da, int& s0,
+                                              int& s1, int& s2) {
+    if (x < 0) return false;
+    const uint64_t u = (uint64_t)x, N2 = d.N2;
+    if (hi == ~(uint64_t)0 || u - hi * N2 >= N2) {
+        hi = div_est(u, N2, d.invN2);
+        if (hi >= N2) {
+            hi = ~(uint64_t)0;
+            return false;
+        }
+        da = __ldg(&d.pd[hi]);
+    }
+    const uint32_t lo = (uint32_t)u - (uint32_t)hi * (uint32_t)N2;
+    const uint2 db = __ldg(&d.pd[lo]);
+    const int L2m1 = 2 * (int)d.L - 1;
+    const int k0 = pd_axis_key(da.x & 0xffffu, db.x & 0xffffu, L2m1);
+    const int k1 = pd_axis_key(da.x >> 16, db.x >> 16, L2m1);
+    const int k2 = pd_axis_key(da.y, db.y, L2m1);
+    const int a = min(k0, k1), b = max(k0, k1);
+    s0 = min(a, k2);
+    s2 = max(b, k2);
+    s1 = a + b + k2 - s0 - s2;
+    return true;
+}
+
 // The decode pass for ERI classes through the pair descriptors.  A thread
 // takes four consecutive classes (16-byte loads of the indices and stores of
 // the packed keys when the arrays are 16-byte aligned): a sorted list keeps the
@@ -318,11 +350,17 @@ __device__ __forceinline__ uint64_t class_packed(const uint64_t* __restrict__ ke
 // is still decoded correctly: an out-of-range remainder takes the quotient
 // again), and a pair bit already set by the thread's previous class is not
 // tested again.  Flags and pair bits as in k_mark.
+// skip (non-null in sized replays that may reuse their plan): when *skip is
+// set, the saved plan stands for this replay unless the class gather finds a
+// class outside it, so the classes are not marked here (the gather decodes
+// and checks them).  keys may be null (such replays do not read them).
 __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
                                                      uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
-                                                     uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
+                                                     uint64_t* __restrict__ keys, int* __restrict__ bad, int local,
+                                                     const int* __restrict__ skip) {
     pdl_wait();
     pdl_release();
+    if (skip && *skip) return;
     extern __shared__ uint32_t sflag[];
     const int nk = (int)d.nkeys;
     const int words = (nk * nk + 31) >> 5;
@@ -334,9 +372,6 @@ __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_
     uint32_t* flags = local ? sflag : used;
     uint32_t* bits = local ? sbits : pairBits;
     const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)keys & 15) == 0;
-    const uint64_t N2 = d.N2;
-    const uint32_t N2lo = (uint32_t)N2;
-    const int L2m1 = 2 * (int)d.L - 1;
     const i64 groups = (m + 3) / 4;
     for (i64 g = (i64)blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += (i64)gridDim.x * blockDim.x) {
         const i64 n0 = 4 * g;
@@ -358,32 +393,13 @@ __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_
         for (int v = 0; v < 4; ++v) {
             kv[v] = BAD_KEYS;
             if (n0 + v >= m) continue;
-            const int64_t x = c[v];
-            if (x < 0) {
+            int s0, s1, s2;
+            if (!pd_class_keys(d, c[v], hi, da, s0, s1, s2)) {
                 atomicOr(bad, 1);
                 continue;
             }
-            const uint64_t u = (uint64_t)x;
-            if (hi == ~(uint64_t)0 || u - hi * N2 >= N2) {
-                hi = div_est(u, N2, d.invN2);
-                if (hi >= N2) {
-                    hi = ~(uint64_t)0;
-                    atomicOr(bad, 1);
-                    continue;
-                }
-                da = __ldg(&d.pd[hi]);
-            }
-            const uint32_t lo = (uint32_t)u - (uint32_t)hi * N2lo;
-            const uint2 db = __ldg(&d.pd[lo]);
-            int k[3];
-            k[0] = pd_axis_key(da.x & 0xffffu, db.x & 0xffffu, L2m1);
-            k[1] = pd_axis_key(da.x >> 16, db.x >> 16, L2m1);
-            k[2] = pd_axis_key(da.y, db.y, L2m1);
-            const int k0 = min(k[0], k[1]), k1 = max(k[0], k[1]);
-            const int s0 = min(k0, k[2]), s2 = max(k1, k[2]);
-            const int s1 = k0 + k1 + k[2] - s0 - s2;
             if (!dcheck(s0 >= 0 && s2 < nk, 1, s2)) continue;
-            k[0] = s0, k[1] = s1, k[2] = s2;
+            const int k[3] = {s0, s1, s2};
             kv[v] = pack_keys(k);
             flags[s0] = 1;
             flags[s1] = 1;
@@ -396,6 +412,7 @@ __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_
                 if (!(bits[slot >> 5] & bit)) atomicOr(&bits[slot >> 5], bit);
             }
         }
+        if (!keys) continue;
         if (vec && full) {
             reinterpret_cast<ulonglong2*>(keys + n0)[0] = make_ulonglong2(kv[0], kv[1]);
             reinterpret_cast<ulonglong2*>(keys + n0)[1] = make_ulonglong2(kv[2], kv[3]);
@@ -565,8 +582,10 @@ __global__ void k_pair_lists(i64 words, int nk, const uint32_t* __restrict__ bit
 // As a GEMM: C[j][a] = sum_t G[j][t] W[aKey[a]][t] with G[j][t] = T[S[j] + t^2]
 // gathered tile by tile into shared memory (consecutive j read neighbouring
 // table entries, so a warp's 32 gathers touch a few cache lines), and the
-// FP64 tensor-core tiles of dmma.cuh.  blockIdx.z selects a chunk of t: small
-// problems sum partial products afterwards (k_sum_parts).
+// FP64 tensor-core tiles of dmma.cuh.  blockIdx.z selects a chunk of t: the
+// split blocks of small problems sum their partial tiles in a cluster; the
+// 144-column tiles split only the m tiles of a partial last wave, in two
+// halves of t (dm_split_store).
 template <int BN_>
 struct StageAOp {
     static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
@@ -584,6 +603,16 @@ struct StageAOp {
     int nS, U, Up, t_chunk;
     i64 part_stride;
     double* H;
+    // tail split (k_dmma's dm_split_store; ws null: none): blocks from nfull on
+    // are the two K halves of the m tiles nfull, nfull + 1, ...
+    int nfull = 0;
+    double* ws = nullptr;
+    unsigned* tickets = nullptr;
+    static constexpr bool TAIL_SPLIT = true;
+    __device__ int split_half() const {
+        return ws && (int)blockIdx.x >= nfull ? (int)((blockIdx.x - nfull) & 1) : -1;
+    }
+    __device__ int split_slot() const { return (int)(blockIdx.x - nfull) >> 1; }
     struct Block {
         int mvalid, nvalid, nk;
         int m0, n0, t0, t1;
@@ -600,11 +629,18 @@ struct StageAOp {
         const int nA = (int)cnt->nA;
         b.n0 = blockIdx.y * BN;
         if (b.n0 >= nA) return false;  // grids are sized by a bound on nA
-        b.m0 = blockIdx.x * DM_BM;
+        const int half = split_half();
+        b.m0 = (half < 0 ? (int)blockIdx.x : nfull + split_slot()) * DM_BM;
         b.mvalid = min(DM_BM, nS - b.m0);
         b.nvalid = min(BN, nA - b.n0);
-        b.t0 = blockIdx.z * t_chunk;
-        b.t1 = min(U, b.t0 + t_chunk);
+        if (half < 0) {
+            b.t0 = blockIdx.z * t_chunk;
+            b.t1 = min(U, b.t0 + t_chunk);
+        } else {  // (the host splits only K ranges of at least two chunks)
+            const int hc = ((U + DM_BK - 1) / DM_BK + 1) / 2 * DM_BK;
+            b.t0 = half ? hc : 0;
+            b.t1 = half ? U : min(U, hc);
+        }
         b.nk = (b.t1 - b.t0 + DM_BK - 1) / DM_BK;
         b.H = H + (i64)blockIdx.z * part_stride;
         return b.nk > 0;
@@ -747,115 +783,6 @@ struct StageBOp {
             h2[0] = v0;
     }
 };
-
-// Stage B with the expanded H rows in memory: Hf[a][v][u] = H[a][sidx[v U + u]]
-// (pitch Up in u), written once per evaluation by k_expand_h where all of it
-// fits comfortably in L2 (small lattices: ERI 7^3 17 MB).  The B tile is then
-// two consecutive u of one v per 16-byte copy, with no index load in front of
-// each gather.  Otherwise as StageBOp (same tiles, rows and stores).
-__global__ void k_expand_h(const double* __restrict__ H, const int* __restrict__ sidx, const PlanCounts* __restrict__ cnt,
-                           i64 nS, int U, int Up, double* __restrict__ Hf) {
-    pdl_wait();
-    pdl_release();
-    const i64 per = (i64)U * Up, total = cnt->nA * per;
-    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
-        const i64 a = e / per;
-        const int r = (int)(e - a * per), v = r / Up, u = r - v * Up;
-        Hf[e] = u < U ? H[a * nS + __ldg(&sidx[v * U + u])] : 0.0;
-    }
-}
-
-template <bool DEEP>
-struct StageBDenseOp {
-    static constexpr bool A_KMAJOR = false, B_KMAJOR = true;
-    static constexpr int BN = DM_BN;
-    static constexpr int STAGES = DEEP ? 3 : 2, MIN_BLOCKS = DEEP ? 3 : 4;
-    const double* W;
-    const double* Hf;  // [a][v][u], pitch Up
-    const int* rowKey;
-    const int* rowPair;
-    const int* tile_batch;
-    const int* tile_col0;
-    const int* tile_ncols;
-    int U, Up, v_chunk;
-    i64 part_stride;
-    double* H2;
-    struct Block {
-        int mvalid, nvalid, nk;
-        int p0, u0, v0, v1;
-        const double* h;  // Hf block of the tile's A key
-        double* H2;
-    };
-    struct AState {
-        i64 off[DM_BM / 16];
-    };
-    struct BState {};
-    __device__ bool begin(Block& b) const {
-        const int tile = blockIdx.x;
-        b.mvalid = tile_ncols[tile];
-        if (b.mvalid <= 0) return false;
-        b.p0 = tile_col0[tile];
-        b.h = Hf + (i64)tile_batch[tile] * U * Up;
-        b.u0 = blockIdx.y * DM_BN;
-        b.nvalid = min(DM_BN, U - b.u0);
-        b.v0 = blockIdx.z * v_chunk;
-        b.v1 = min(U, b.v0 + v_chunk);
-        b.nk = (b.v1 - b.v0 + DM_BK - 1) / DM_BK;
-        b.H2 = H2 + (i64)blockIdx.z * part_stride;
-        return b.nk > 0;
-    }
-    __device__ void a_init(const Block& b, AState& st) const {
-#pragma unroll
-        for (int q = 0; q < DM_BM / 16; ++q) {
-            const int r = dm_pair_row(threadIdx.x, q);
-            st.off[q] = r < b.mvalid ? (i64)rowKey[b.p0 + r] * Up : -1;
-        }
-    }
-    __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
-        const int k = dm_pair_k(threadIdx.x), v = b.v0 + kc * DM_BK + k;
-        const int bytes = dm_pair_bytes(v, b.v1);
-#pragma unroll
-        for (int q = 0; q < DM_BM / 16; ++q) {
-            const int n = st.off[q] >= 0 ? bytes : 0;
-            dm_cp16(tile + dm_rowmajor_at(dm_pair_row(threadIdx.x, q), k), n ? W + st.off[q] + v : W, n);
-        }
-    }
-    __device__ void b_init(const Block&, BState&) const {}
-    // pairs of rows (u, u + 1) at one k = v: 64 rows x 16 k = 512 pairs, four
-    // per thread; Up is a multiple of 4 and u0 of 64, so the pairs are 16-byte
-    // aligned in Hf and (68 doubles per k) in the K-major tile
-    __device__ void b_issue(const Block& b, BState&, int kc, double* tile) const {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int pidx = threadIdx.x + DM_THREADS * q, rp = pidx & 31, k = pidx >> 5;
-            const int n = 2 * rp, u = b.u0 + n, v = b.v0 + kc * DM_BK + k;
-            const int bytes = (v < b.v1 && n < b.nvalid) ? (n + 1 < b.nvalid ? 16 : 8) : 0;
-            dm_cp16(tile + dm_kmajor_at(n, k), bytes ? b.h + (i64)v * Up + u : b.h, bytes);
-        }
-    }
-    __device__ void store(const Block& b, int m, int n, double v0, double v1) const {
-        if (m >= b.mvalid) return;
-        double* h2 = b.H2 + (i64)__ldg(&rowPair[b.p0 + m]) * Up + b.u0 + n;
-        if (n + 1 < b.nvalid)
-            *reinterpret_cast<double2*>(h2) = make_double2(v0, v1);
-        else if (n < b.nvalid)
-            h2[0] = v0;
-    }
-};
-
-// the expanded H of stage B held in memory when it takes at most this many bytes
-constexpr i64 DENSE_HF_BYTES = (i64)48 << 20;
-
-// out[i] = sum_p parts[p n + i], in order of p (deterministic)
-__global__ void k_sum_parts(const double* __restrict__ parts, int P, i64 n, double* __restrict__ out) {
-    pdl_wait();
-    pdl_release();
-    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
-        double acc = parts[i];
-        for (int p = 1; p < P; ++p) acc += parts[(i64)p * n + i];
-        out[i] = acc;
-    }
-}
 
 // Splits of a reduction loop of length U into P chunks (chunk a multiple of
 // `grain`) so that a launch of `blocks` blocks reaches about `target` blocks:
@@ -1122,6 +1049,103 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
     }
 }
 
+// The class gather of sized replays that reuse their plan without marking the
+// classes (k_mark_eri_pd skipped): each class is decoded here from its index
+// through the pair descriptors and checked against the plan -- its (A, B) pair
+// set in the plan's pair bitmap and its third key a used key (kid[k2 + 1] >
+// kid[k2]), which the marks of the list that made the plan guarantee for every
+// class of that list.  A class outside the plan (the list was rewritten in
+// place since) or outside the tensor sets the overflow flag, and the host
+// evaluates the list again with an exact plan.  This saves the mark pass's
+// read of the indices and the write and re-read of the packed keys (24 bytes
+// per class).
+__global__ void __launch_bounds__(256) k_gather_q_pd(const double* __restrict__ Q, int parts, i64 part_stride,
+                                                      ClassDecode dec, const int64_t* __restrict__ idx, i64 m,
+                                                      const uint64_t* __restrict__ kid, int nk,
+                                                      const uint32_t* __restrict__ pairBits,
+                                                      const uint64_t* __restrict__ pairPre, int ldq,
+                                                      PlanCounts* __restrict__ cnt, double* __restrict__ out) {
+    pdl_wait();
+    pdl_release();
+    if (cnt->overflow) return;
+    const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)out & 15) == 0;
+    const i64 groups = (m + 3) / 4, stride = (i64)gridDim.x * blockDim.x;
+    constexpr int G = 2;
+    bool miss = false;
+    for (i64 g0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; g0 < groups; g0 += G * stride) {
+        int64_t c[G][4];
+#pragma unroll
+        for (int h = 0; h < G; ++h) {
+            const i64 n0 = 4 * (g0 + h * stride);
+            if (vec && n0 + 3 < m) {
+                const longlong2 a = __ldg(reinterpret_cast<const longlong2*>(idx + n0));
+                const longlong2 b = __ldg(reinterpret_cast<const longlong2*>(idx + n0 + 2));
+                c[h][0] = a.x, c[h][1] = a.y, c[h][2] = b.x, c[h][3] = b.y;
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) c[h][v] = n0 + v < m ? __ldg(&idx[n0 + v]) : 0;
+            }
+        }
+        i64 q[G][4];
+#pragma unroll
+        for (int h = 0; h < G; ++h) {
+            const i64 n0 = 4 * (g0 + h * stride);
+            uint64_t hi = ~(uint64_t)0;
+            uint2 da = make_uint2(0, 0);
+            i64 last_slot = -1, last_pid = -1;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                q[h][v] = -1;
+                if (n0 + v >= m) continue;
+                int s0, s1, s2;
+                if (!pd_class_keys(dec, c[h][v], hi, da, s0, s1, s2)) {
+                    miss = true;
+                    continue;
+                }
+                if (!dcheck(s0 >= 0 && s2 < nk, 1, s2)) continue;
+                const i64 slot = (i64)s1 * nk + s0;
+                if (slot != last_slot) {
+                    last_slot = slot;
+                    const i64 w = slot >> 5;
+                    const uint32_t b = __ldg(&pairBits[w]), bit = (uint32_t)(slot & 31);
+                    last_pid = (b >> bit) & 1u ? (i64)__ldg(&pairPre[w]) + __popc(b & ((1u << bit) - 1u)) : -1;
+                }
+                const uint64_t k0 = __ldg(&kid[s2]), k1 = __ldg(&kid[s2 + 1]);
+                if (last_pid < 0 || k1 == k0) {
+                    miss = true;
+                    continue;
+                }
+                q[h][v] = last_pid * ldq + (i64)k0;
+            }
+        }
+        double acc[G][4];
+#pragma unroll
+        for (int h = 0; h < G; ++h)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                acc[h][v] = 0.0;
+                if (q[h][v] >= 0 && dcheck(q[h][v] < part_stride, 3, q[h][v])) {
+                    acc[h][v] = Q[q[h][v]];
+                    for (int z = 1; z < parts; ++z) acc[h][v] += Q[z * part_stride + q[h][v]];
+                }
+            }
+#pragma unroll
+        for (int h = 0; h < G; ++h) {
+            const i64 n0 = 4 * (g0 + h * stride);
+            if (n0 >= m) continue;
+            if (vec && n0 + 3 < m) {
+                reinterpret_cast<double2*>(out + n0)[0] = make_double2(acc[h][0], acc[h][1]);
+                reinterpret_cast<double2*>(out + n0)[1] = make_double2(acc[h][2], acc[h][3]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v)
+                    if (n0 + v < m) out[n0 + v] = acc[h][v];
+            }
+        }
+    }
+    if (miss) atomicExch(reinterpret_cast<unsigned long long*>(&cnt->overflow), 1ull);
+}
+
 // ---------------------------------------------------------------------------
 // mixed form: stages A and B as int8-sliced products on the tensor cores
 //   stage A:  H^T[j][a] = sum_t G[j][t] W[aKey[a]][t],   G[j][t] = T[S[j] + t^2]
@@ -1369,6 +1393,10 @@ struct PlanReuse {
     uint32_t* saved_bits = nullptr;
     PlanCounts* saved_cnt = nullptr;
     int* valid = nullptr;  // null: no reuse (bounded plans)
+    // set: the replay did not mark its classes (k_mark_eri_pd skipped them and
+    // k_gather_q_pd checks each against the plan), so a valid saved plan is
+    // restored without the comparison
+    int trust = 0;
 };
 struct PlanStore {
     DevMem<uint64_t> ids, pairPre;
@@ -1376,7 +1404,9 @@ struct PlanStore {
     DevMem<uint32_t> saved_used, saved_bits;
     DevMem<PlanCounts> saved_cnt;
     DevMem<int> valid;
-    void alloc(i64 nk, i64 words, i64 capA, i64 capP, i64 tile_ints) {
+    DevMem<uint2> pd;  // the ERI pair descriptors, when the decode uses them
+    void alloc(i64 nk, i64 words, i64 capA, i64 capP, i64 tile_ints, i64 pairs) {
+        if (pairs > 0) pd.alloc((size_t)pairs);
         ids.alloc((size_t)(2 * nk));
         pairPre.alloc((size_t)words);
         keyOf.alloc((size_t)nk);
@@ -1391,7 +1421,7 @@ struct PlanStore {
         valid.alloc(1);
         GLI_CUDA(cudaMemset(valid.p, 0, sizeof(int)));
     }
-    PlanReuse reuse() { return PlanReuse{saved_used.p, saved_bits.p, saved_cnt.p, valid.p}; }
+    PlanReuse reuse(bool trust) { return PlanReuse{saved_used.p, saved_bits.p, saved_cnt.p, valid.p, trust ? 1 : 0}; }
 };
 
 // Bounded plans (at most 256 keys: 512 key flags, 2,048 pair-bitmap words):
@@ -1423,9 +1453,12 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
     __shared__ int s_aId[PLAN_SMALL_KEYS], s_aKey[PLAN_SMALL_KEYS];
     if (reuse.valid && *reuse.valid) {
         // the saved plan stands if this list marked the same keys and pairs
+        // (or was not marked: the gather checks its classes instead)
         bool same = true;
-        for (i64 i = threadIdx.x; i < 2 * nk; i += blockDim.x) same = same && used[i] == reuse.saved_used[i];
-        for (i64 w = threadIdx.x; w < words; w += blockDim.x) same = same && bits[w] == reuse.saved_bits[w];
+        if (!reuse.trust) {
+            for (i64 i = threadIdx.x; i < 2 * nk; i += blockDim.x) same = same && used[i] == reuse.saved_used[i];
+            for (i64 w = threadIdx.x; w < words; w += blockDim.x) same = same && bits[w] == reuse.saved_bits[w];
+        }
         if (__syncthreads_and(same)) {
             if (threadIdx.x == 0) {
                 const PlanCounts c = *reuse.saved_cnt;
@@ -1607,15 +1640,6 @@ struct EvalSizes {
 // product form of stage C.
 constexpr i64 BOUNDED_KEYS = 256;
 
-// (GLI_B200_DENSE_HF_BYTES overrides the dense stage-B threshold, for measurements)
-static i64 dense_hf_bytes() {
-    static const i64 v = [] {
-        const char* e = getenv("GLI_B200_DENSE_HF_BYTES");
-        return e && *e ? (i64)atoll(e) : DENSE_HF_BYTES;
-    }();
-    return v;
-}
-
 // stage A runs on the tensor cores (mixed form) from this many outputs nA nS
 // (GLI_B200_TC_A_OUTPUTS overrides it, for measurements)
 constexpr i64 TC_A_OUTPUTS = 1000000;
@@ -1665,17 +1689,86 @@ enum PlanMode { PLAN_BOUNDED = 0, PLAN_EXACT = 1, PLAN_SIZED = 2 };
 // key spaces that the sized plan's single-block plan kernel holds
 static bool sized_plan_fits(i64 nk) { return nk <= PLAN_SMALL_KEYS && (nk * nk + 31) / 32 <= 8 * 1024; }
 
+// the u split of the stage-C product: 64-column tiles (the product's grid is
+// small, and wider tiles cost it parallelism: ERIDA 129^3 73 us with 80
+// columns, 66 us with 64).  A grid under a wave (four blocks per SM; about half
+// the column tiles are active after the A-key shift) splits u in up to three
+// where the classes are few beside the product (each class then sums the
+// slices: ERIDA 129^3 has 366,145 classes and 1.08 million products, 45 us
+// against 47 with two slices; ERI 7^3's 3.57 million classes would pay more in
+// the gather than the split saves).  Returns the slices; *u_chunk their length.
+static int product_split(i64 nP, i64 nku, int U, i64 m, int num_sms, int* u_chunk) {
+    const i64 mt = (nP + DM_BM - 1) / DM_BM, nt = (nku + DM_BN - 1) / DM_BN;
+    *u_chunk = U;
+    int P = std::min(3, split_count(mt * ((nt + 1) / 2), U, DM_BK, 4 * (i64)num_sms, u_chunk));
+    if (2 * m > nP * nku) P = 1;
+    *u_chunk = ((U + P - 1) / P + DM_BK - 1) / DM_BK * DM_BK;
+    return (U + *u_chunk - 1) / *u_chunk;
+}
+
+// Stage A with 129..144 A keys holds them in one 144-column tile and does not
+// split the whole K range (the partial 144-column tiles would not fit the
+// operand ring for the cluster sum, and summing them through HBM measured
+// slower, ERIDA 129^3 0.439 against 0.410 ms).  Only a last wave under half
+// full is split in K, two blocks per m tile (ERIDA 129^3: 1,072 m tiles on 444
+// block slots, 2.41 waves).  Returns the m tiles split so (0: none).
+static i64 stage_a_tail(i64 nA, int nS, int U, int num_sms) {
+    if (!(nA > 128 && nA <= 144)) return 0;
+    const i64 mb = (nS + DM_BM - 1) / DM_BM;
+    const i64 slots = (i64)dmma_blocks_per_sm<StageAOp<144>>() * num_sms;
+    const i64 tail = mb % slots;
+    return tail > 0 && 2 * tail <= slots && (U + DM_BK - 1) / DM_BK >= 2 ? tail : 0;
+}
+
+// Buffers of the three stages, sized by the plan's counts
+struct StageBufs {
+    DevBuf<double> H, H2, Q;
+    DevBuf<double> split_ws;  // stage A's tail split: two partial tiles per split m tile
+    DevBuf<unsigned> tickets;
+    int q_parts = 0, u_chunk = 0;
+    i64 tail = 0;
+    void alloc(const EvalArgs& a, const EvalSizes& sz, bool tc_a, bool product, cudaStream_t s) {
+        const LatticeTables& t = *a.t;
+        const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
+        if (sz.nA * (i64)U * U > ((i64)1 << 31))
+            fail(GLI_ERR_LIMIT, "stage buffers exceed 16 GB (%lld A keys, lattice extent %d)", (long long)sz.nA, U);
+        H.alloc(sz.nA * (i64)nS, s);
+        H2.alloc(sz.nP * (i64)Up, s);
+        if (product) {
+            q_parts = product_split(sz.nP, sz.nku, U, a.m, a.num_sms, &u_chunk);
+            Q.alloc(q_parts * sz.nP * sz.nku, s);
+        }
+        tail = tc_a ? 0 : stage_a_tail(sz.nA, nS, U, a.num_sms);
+        if (tail) {
+            split_ws.alloc(tail * 2 * DM_BM * 144, s);
+            tickets.alloc(tail, s);
+            tickets.zero();
+        }
+    }
+};
+
 // Queues one evaluation on stream s.  Kernels read the counts from st->cnt;
 // the host sizes buffers and grids by `sz` (an input for PLAN_SIZED, an output
 // otherwise).
 static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
-                         cudaStream_t s, PlanStore* ps = nullptr) {
+                         cudaStream_t s, PlanStore* pstore = nullptr) {
     const bool bounded = mode == PLAN_BOUNDED;
     const LatticeTables& t = *a.t;
     const i64 nk = t.nkeys, m = a.m;
     const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
     GLI_CUDA(cudaMemsetAsync(st, 0, sizeof(EvalStatus), s));
     PlanCounts* cnt = &st->cnt;
+    if (bounded) {
+        sz.nku = nk;
+        sz.nA = nk;
+        // pairs (A, B) have A >= B; every class has one pair
+        sz.nP = std::min(nk * (nk + 1) / 2, m);
+    }
+    // Bounded and sized evaluations know every size here: all their buffers
+    // are allocated and zeroed before the first kernel, so that a captured
+    // graph has its allocation and memset nodes at the root and its kernels
+    // follow one another directly (programmatic launch edges throughout)
+    const bool known = mode != PLAN_EXACT;
     // usedKey and usedA side by side so that one scan serves both; pair flags
     // over all key pairs (slot k2 * nk + k1)
     const i64 words = (nk * nk + 31) / 32;
@@ -1688,43 +1781,42 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     DevBuf<uint2> pdesc;
     ClassDecode dec = a.d;
     dec.pd = nullptr;
+    const int* pd_skip = nullptr;
     if (dec.kind == 1 && pair_desc_applies(dec)) {
-        // the pair-descriptor decode of the ERI classes
-        pdesc.alloc(dec.N2, s);
-        launch_pdl(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p);
+        // the pair-descriptor decode of the ERI classes (a sized replay keeps
+        // the table with its plan, and remakes it only with the plan)
+        if (pstore && pstore->pd.p) {
+            pdesc.borrow(pstore->pd.p, dec.N2, s);
+            pd_skip = pstore->valid.p;
+        } else {
+            pdesc.alloc(dec.N2, s);
+        }
         dec.pd = pdesc.p;
     } else if (dec.kind == 1) {
         pts.alloc(dec.N, s);
-        launch_pdl(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
         dec.pt = pts.p;
     }
+    // Sized replays of the product form through the pair descriptors mark
+    // their classes only when the saved plan is not valid: otherwise the plan
+    // is restored and the gather decodes and checks every class (the list may
+    // have been rewritten in place since the plan was made).
+    const bool fused = pstore && dec.pd && mode == PLAN_SIZED && product_pays((double)sz.nP, (double)sz.nku, m);
     // packed key triple per class, written by the decode pass and read by the
-    // gather (decoding a class again in the gather measured slower than
-    // re-reading its 8 bytes: ERI 7^3 stage C 52 against 32 us)
-    DevBuf<uint64_t> keys(m, s);
-    {
-        const size_t lb = mark_local_bytes(nk);
-        if (dec.pd) {
-            const i64 groups = (m + 3) / 4;
-            const unsigned mb = (unsigned)std::min<i64>((groups + 255) / 256, (i64)a.num_sms * 8);
-            launch_pdl(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
-                       lb ? 1 : 0);
-        } else {
-            const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-            launch_pdl(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
-                       lb ? 1 : 0);
-        }
-    }
+    // gather (decoding a class twice, in the mark pass and again in the gather,
+    // measured slower than re-reading its 8 bytes: ERI 7^3 stage C 52 against
+    // 32 us)
+    DevBuf<uint64_t> keys;
+    if (!fused) keys.alloc(m, s);
     DevBuf<uint64_t> ids, pairPre;
     DevBuf<int> keyOf, aId, aKey;
     DevBuf<int> pairA, pairB;
     PairTiles tiles;
-    if (ps) {  // a sized graph's plan, kept between its replays
-        ids.borrow(ps->ids.p, 2 * nk, s);
-        keyOf.borrow(ps->keyOf.p, nk, s);
-        aId.borrow(ps->aId.p, nk, s);
-        aKey.borrow(ps->aKey.p, nk, s);
-        pairPre.borrow(ps->pairPre.p, words, s);
+    if (pstore) {  // a sized graph's plan, kept between its replays
+        ids.borrow(pstore->ids.p, 2 * nk, s);
+        keyOf.borrow(pstore->keyOf.p, nk, s);
+        aId.borrow(pstore->aId.p, nk, s);
+        aKey.borrow(pstore->aKey.p, nk, s);
+        pairPre.borrow(pstore->pairPre.p, words, s);
     } else {
         ids.alloc(2 * nk, s);
         keyOf.alloc(nk, s);
@@ -1735,32 +1827,57 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     const bool small_pairs = (bounded || mode == PLAN_SIZED) && words <= 8 * 1024;
     if (mode == PLAN_SIZED && !(small_pairs && nk <= PLAN_SMALL_KEYS))
         fail(GLI_ERR_INTERNAL, "sized plan for a key space of %lld keys", (long long)nk);
-    if (bounded) {
-        sz.nku = nk;
-        sz.nA = nk;
-        // pairs (A, B) have A >= B; every class has one pair
-        sz.nP = std::min(nk * (nk + 1) / 2, m);
-    }
-    if (small_pairs && nk <= PLAN_SMALL_KEYS) {
-        // the whole plan and stage B's tiles in one launch (bounded and sized
-        // plans; for exact plans, whose counts are read back half way, the
-        // single block's pass over nk^2 pair slots measured no faster than the
-        // multi-block path: ERI 7^3 0.206 against 0.200 ms)
+    // the whole plan and stage B's tiles in one launch (bounded and sized
+    // plans; for exact plans, whose counts are read back half way, the single
+    // block's pass over nk^2 pair slots measured no faster than the multi-block
+    // path: ERI 7^3 0.206 against 0.200 ms)
+    const bool plan_small = small_pairs && nk <= PLAN_SMALL_KEYS;
+    if (plan_small) {
         const bool sliced = stage_b_sliced(a.mixed, sz.nA, sz.nP, U);
         const int tbn = sliced ? tile_n(MIXED_SLICES) : DM_BM;
-        if (ps) {
-            pairA.borrow(ps->pairA.p, sz.nP, s);
-            pairB.borrow(ps->pairB.p, sz.nP, s);
-            tiles.alloc(sz.nA, sz.nP, tbn, !sliced, s, ps->tiles.p);
+        if (pstore) {
+            pairA.borrow(pstore->pairA.p, sz.nP, s);
+            pairB.borrow(pstore->pairB.p, sz.nP, s);
+            tiles.alloc(sz.nA, sz.nP, tbn, !sliced, s, pstore->tiles.p);
         } else {
             pairA.alloc(sz.nP, s);
             pairB.alloc(sz.nP, s);
             tiles.alloc(sz.nA, sz.nP, tbn, !sliced, s);
         }
+    }
+    // the mixed form runs a stage on the tensor cores when it is large enough
+    // for them to pay off; smaller stages (latency-bound either way) stay FP64
+    // (decided on the sizes: bounds for bounded plans, counts otherwise)
+    StageBufs sb;
+    auto stage_bufs = [&]() {
+        const bool tc = a.mixed && sz.nA * (i64)nS >= tc_a_outputs();
+        const bool prod = product_pays((double)sz.nP, (double)sz.nku, m) || (bounded && m >= 65536);
+        sb.alloc(a, sz, tc, prod, s);
+    };
+    if (known) stage_bufs();
+
+    if (dec.pd)
+        launch_pdl(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p, pd_skip);
+    else if (dec.kind == 1)
+        launch_pdl(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
+    {
+        const size_t lb = mark_local_bytes(nk);
+        if (dec.pd) {
+            const i64 groups = (m + 3) / 4;
+            const unsigned mb = (unsigned)std::min<i64>((groups + 255) / 256, (i64)a.num_sms * 8);
+            launch_pdl(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
+                       lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
+        } else {
+            const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
+            launch_pdl(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
+                       lb ? 1 : 0);
+        }
+    }
+    if (plan_small) {
         launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
                    tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt,
-                   ps ? ps->reuse() : PlanReuse{});
+                   pstore ? pstore->reuse(fused) : PlanReuse{});
         tiles.built = true;
     } else {
         if (2 * nk <= 1024) {
@@ -1794,15 +1911,15 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
             launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk,
                        pairBits.p, pairPre.p, aId.p, pairA.p, pairB.p);
     }
+    if (!known) stage_bufs();
 
     const i64 nA = sz.nA, nP = sz.nP, nku = sz.nku;
-    if (nA * (i64)U * U > ((i64)1 << 31))
-        fail(GLI_ERR_LIMIT, "stage buffers exceed 16 GB (%lld A keys, lattice extent %d)", (long long)nA, U);
-    DevBuf<double> H(nA * (i64)nS, s);
+    DevBuf<double>& H = sb.H;
     // the mixed form runs a stage on the tensor cores when it is large enough for
     // them to pay off; smaller stages (latency-bound either way) stay FP64
     const bool tc_a = a.mixed && nA * (i64)nS >= tc_a_outputs();
     const bool tc_b = stage_b_sliced(a.mixed, nA, nP, U);
+    DevBuf<double>& H2 = sb.H2;
     t_enq_paths = (tc_a ? 1 : 0) | (tc_b ? 2 : 0);
     timer.mark();
     // ---- stage A
@@ -1822,31 +1939,26 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         w.cs = nS;
         tc_gemm_tiled(a.G, Wa.view(), w, nbt, &st->tc_err, s);
     } else {
-        // small problems split the t loop so that enough blocks exist
-        // (partial sums, then one summing pass)
+        // small problems split the t loop so that enough blocks exist (the
+        // partial tiles summed in a cluster)
         const unsigned mb = (unsigned)((nS + DM_BM - 1) / DM_BM);
         const int bn = (nA > 128 && nA <= 144) ? 144 : col_tile(nA);
         const unsigned nb = (unsigned)((nA + bn - 1) / bn);
-        // (the 144-column tiles are not split: their partial tiles would need the
-        // summing pass over HBM, which measured slower at ERIDA 129^3, 0.439
-        // against 0.410 ms)
         int t_chunk = U;
         const int P = bn == 144 ? 1 : split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
-        const i64 ps = nA * (i64)nS;
         const dim3 grid(mb, nb, (unsigned)P);
         if (bn == 144) {
-            // (no split: 129..144 A keys fill the GPU; the split partial sums of
-            // 144-column tiles would not fit the operand ring for the cluster sum)
-            DevBuf<double> parts;
-            double* dst = H.p;
-            if (P > 1) {
-                parts.alloc((i64)P * ps, s);
-                dst = parts.p;
+            // one 144-column tile; a last wave under half full split in K
+            // (stage_a_tail)
+            StageAOp<144> op{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, U, 0, H.p};
+            dim3 g = grid;
+            if (sb.tail) {
+                op.nfull = (int)(mb - sb.tail);
+                op.ws = sb.split_ws.p;
+                op.tickets = sb.tickets.p;
+                g.x = (unsigned)(mb + sb.tail);
             }
-            dmma_launch(StageAOp<144>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, ps, dst}, grid, s);
-            if (P > 1)
-                launch_pdl(k_sum_parts, dim3((unsigned)std::min<i64>((ps + 255) / 256, (i64)a.num_sms * 16)),
-                           dim3(256), 0, s, parts.p, P, ps, H.p);
+            dmma_launch(op, g, s);
         } else if (bn == 80) {
             // a split sums its parts inside a cluster of the P blocks of a tile
             dmma_launch_cluster(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}, grid, s);
@@ -1856,7 +1968,6 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     }
     timer.mark();
     // ---- stage B
-    DevBuf<double> H2(nP * (i64)Up, s);
     if (tiles.built && tiles.bn != (tc_b ? tile_n(MIXED_SLICES) : DM_BM)) tiles.built = false;
     if (tc_b) {
         constexpr int BN = tile_n(MIXED_SLICES);
@@ -1916,20 +2027,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         const int P = split_count(active * ub, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &v_chunk);
         // a split sums its parts inside a cluster of the P blocks of a tile
         const dim3 grid((unsigned)max_tiles, ub, (unsigned)P);
-        const i64 hf_doubles = nA * (i64)U * Up;
-        if (8 * hf_doubles <= dense_hf_bytes()) {
-            DevBuf<double> Hf(hf_doubles, s);
-            const unsigned eb = (unsigned)std::min<i64>((hf_doubles + 255) / 256, (i64)a.num_sms * 16);
-            launch_pdl(k_expand_h, dim3(eb), dim3(256), 0, s, H.p, t.sidx.p, cnt, (i64)nS, U, Up, Hf.p);
-            if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
-                dmma_launch_cluster(StageBDenseOp<false>{t.W.p, Hf.p, tiles.rowKey, tiles.rowPair, tiles.batch,
-                                                         tiles.col0, tiles.ncols, U, Up, v_chunk, 0, H2.p},
-                                    grid, s);
-            else
-                dmma_launch_cluster(StageBDenseOp<true>{t.W.p, Hf.p, tiles.rowKey, tiles.rowPair, tiles.batch,
-                                                        tiles.col0, tiles.ncols, U, Up, v_chunk, 0, H2.p},
-                                    grid, s);
-        } else if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
+        if (active * ub * P >= 4 * (i64)DM_SPLIT_TARGET * a.num_sms)
             dmma_launch_cluster(StageBOp<false>{t.W.p, H.p, t.sidx.p, tiles.rowKey, tiles.rowPair, tiles.batch,
                                                 tiles.col0, tiles.ncols, nS, U, Up, v_chunk, 0, H2.p},
                                 grid, s);
@@ -1949,28 +2047,22 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     const bool undecided = bounded && !product_host && m >= 65536;
     const int c_prod = undecided ? 1 : 0, c_class = undecided ? 2 : 0;
     if (undecided || product_host) {
-        // 64-column tiles: the product's grid is small, and wider tiles cost it
-        // parallelism (ERIDA 129^3: 73 us with 80 columns, 66 us with 64).  A
-        // grid under a wave (four blocks per SM; about half the column tiles
-        // are active after the A-key shift) splits u in up to three where the
-        // classes are few beside the product (each class then sums the slices:
-        // ERIDA 129^3 has 366,145 classes and 1.08 million products, 45 us
-        // against 47 with two slices; ERI 7^3's 3.57 million classes would pay
-        // more in the gather than the split saves)
+        // (Q and its u split sized with the stage buffers: product_split)
         const i64 mt = (nP + DM_BM - 1) / DM_BM, nt = (nku + DM_BN - 1) / DM_BN;
-        int u_chunk = U;
-        int P = std::min(3, split_count(mt * ((nt + 1) / 2), U, DM_BK, 4 * (i64)a.num_sms, &u_chunk));
-        if (2 * m > nP * nku) P = 1;
-        u_chunk = ((U + P - 1) / P + DM_BK - 1) / DM_BK * DM_BK;
-        P = (U + u_chunk - 1) / u_chunk;
+        const int P = sb.q_parts, u_chunk = sb.u_chunk;
         const i64 ps = nP * nku;
-        DevBuf<double> Q(P * ps, s);
+        const DevBuf<double>& Q = sb.Q;
+        if (P < 1 || !Q.p) fail(GLI_ERR_INTERNAL, "stage C product without its buffer");
         dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up, (int)nku,
                                   u_chunk, ps, Q.p, &st->products},
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
-        launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk, pairBits.p,
-                   pairPre.p, (int)nku, cnt, c_prod, a.out);
+        if (fused)  // the plan's own pair bitmap: this replay's stays empty when the mark pass skipped
+            launch_pdl(k_gather_q_pd, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
+                       (const uint32_t*)pstore->saved_bits.p, pairPre.p, (int)nku, cnt, a.out);
+        else
+            launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
+                       pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
@@ -2063,6 +2155,7 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<64>>();
     dmma_prepare<StageAOp<80>>();
     dmma_prepare<StageAOp<144>>();
+    dmma_blocks_per_sm<StageAOp<144>>();
     dmma_prepare<StageBOp<true>>();
     dmma_prepare<StageBOp<false>>();
     dmma_prepare<ProductOp<64>>();
@@ -2070,14 +2163,11 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<80>, true>();
     dmma_prepare<StageBOp<true>, true>();
     dmma_prepare<StageBOp<false>, true>();
-    dmma_prepare<StageBDenseOp<true>>();
-    dmma_prepare<StageBDenseOp<false>>();
-    dmma_prepare<StageBDenseOp<true>, true>();
-    dmma_prepare<StageBDenseOp<false>, true>();
     if (mode == PLAN_SIZED) {
         const i64 nk = a.t->nkeys, words = (nk * nk + 31) / 32;
         e->plan = std::make_unique<PlanStore>();
-        e->plan->alloc(nk, words, sized.nA, sized.nP, PairTiles::ints(sized.nA, sized.nP, 64, true));
+        e->plan->alloc(nk, words, sized.nA, sized.nP, PairTiles::ints(sized.nA, sized.nP, 64, true),
+                       pair_desc_applies(a.d) ? (i64)a.d.N2 : 0);
     }
     const long long l0 = launch_count();
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -2243,6 +2333,120 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
         GLI_CUDA(cudaStreamSynchronize(s));
     }
     check_status(kind, m, *h, *tp, timer, stats);
+}
+
+// Stream-ordered evaluations: queued without a host wait, their status read
+// when the caller waits for them.  A pending evaluation keeps what it needs to
+// be evaluated again (the coefficients, the grid, the device pointers) and its
+// own page-locked status slot; the tables stay alive with it.  Waiting for a
+// ticket waits for that evaluation and every one queued before it on this
+// thread, in order; one whose sized graph overflowed (its list outgrew the
+// plan the graph was sized for) is evaluated again there, exactly.
+struct PendingEval {
+    i64 ticket = 0;
+    int kind = 0;
+    std::vector<double> coeffs;
+    GridDesc g;
+    const int64_t* idx = nullptr;
+    i64 m = 0;
+    double tol = 0.0;
+    int form = 0;
+    double* out = nullptr;
+    cudaStream_t s = nullptr;
+    EvalStatus* h_status = nullptr;  // page-locked slot (from t_status_slots)
+    cudaEvent_t done = nullptr;
+    std::shared_ptr<const LatticeTables> tp;
+    const GraphEntry* sized = nullptr;
+};
+
+struct StatusSlots {  // page-locked status blocks, reused
+    std::vector<EvalStatus*> free;
+    EvalStatus* get() {
+        if (free.empty()) {
+            void* p = nullptr;
+            GLI_CUDA(cudaHostAlloc(&p, sizeof(EvalStatus), cudaHostAllocDefault));
+            return (EvalStatus*)p;
+        }
+        EvalStatus* p = free.back();
+        free.pop_back();
+        return p;
+    }
+    ~StatusSlots() {
+        for (EvalStatus* p : free) cudaFreeHost(p);
+    }
+};
+static thread_local StatusSlots t_status_slots;
+static thread_local std::list<PendingEval> t_pending;
+static thread_local i64 t_next_ticket = 1;
+constexpr size_t MAX_PENDING = 256;
+
+static void finish_pending(PendingEval& e) {
+    struct Recycle {
+        PendingEval& e;
+        ~Recycle() {
+            if (e.done) cudaEventDestroy(e.done);
+            e.done = nullptr;
+            if (e.h_status) t_status_slots.free.push_back(e.h_status);
+            e.h_status = nullptr;
+        }
+    } recycle{e};
+    if (e.m == 0) return;
+    GLI_CUDA(cudaEventSynchronize(e.done));
+    if (e.h_status->cnt.overflow) {
+        drop_graph(e.sized);
+        sparse_values_device(e.kind, e.coeffs.data(), (i64)e.coeffs.size(), e.g, e.idx, e.m, e.tol, e.form, e.out,
+                             e.s, nullptr);
+        return;
+    }
+    StageTimer timer(false, e.s);
+    check_status(e.kind, e.m, *e.h_status, *e.tp, timer, nullptr);
+}
+
+void sparse_values_wait(i64 ticket) {
+    bool found = false;
+    for (const PendingEval& e : t_pending) found = found || e.ticket == ticket;
+    if (!found) fail(GLI_ERR_ARGUMENT, "no pending evaluation %lld on this thread", (long long)ticket);
+    // in order: every evaluation up to this one (the first error ends the wait
+    // and is reported; the evaluations after it stay pending)
+    while (!t_pending.empty()) {
+        PendingEval e = std::move(t_pending.front());
+        t_pending.pop_front();
+        const bool last = e.ticket == ticket;
+        finish_pending(e);
+        if (last) break;
+    }
+}
+
+i64 sparse_values_device_async(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
+                               i64 m, double tol, int form, double* d_out, cudaStream_t s) {
+    if (t_pending.size() >= MAX_PENDING) sparse_values_wait(t_pending.front().ticket);
+    PendingEval e;
+    e.ticket = t_next_ticket++;
+    e.kind = kind;
+    e.coeffs.assign(h_coeffs, h_coeffs + nb);
+    e.g = g;
+    e.idx = d_indices;
+    e.m = m;
+    e.tol = tol;
+    e.form = form;
+    e.out = d_out;
+    e.s = s;
+    if (m > 0) {
+        e.h_status = t_status_slots.get();
+        try {
+            StageTimer timer(false, s);
+            sparse_values_enqueue(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, e.h_status, e.tp, timer,
+                                  &e.sized);
+            GLI_CUDA(cudaEventCreateWithFlags(&e.done, cudaEventDisableTiming));
+            GLI_CUDA(cudaEventRecord(e.done, s));
+        } catch (...) {
+            if (e.done) cudaEventDestroy(e.done);
+            t_status_slots.free.push_back(e.h_status);
+            throw;
+        }
+    }
+    t_pending.push_back(std::move(e));
+    return t_pending.back().ticket;
 }
 
 // Device copies of a host class list and its values, kept per thread and

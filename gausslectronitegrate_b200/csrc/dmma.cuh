@@ -229,6 +229,61 @@ __device__ __forceinline__ void dm_cluster_reduce(const Op& op, const typename O
     cl.sync();  // no block leaves while another still reads its tile
 }
 
+// Tail split (an Op that declares TAIL_SPLIT): the last, partial wave of a
+// launch would leave most SMs idle, so its m tiles are each computed by two
+// blocks over the two halves of K, and the blocks of a full wave's worth of
+// tiles run whole before them.  Both halves write their partial tile to
+// global scratch in the threads' own fragment order (coalesced, no shared
+// memory), then take a ticket for the tile; the second to arrive adds the
+// other's partial to its own and stores the sum (a + b = b + a exactly, so
+// the result does not depend on which half came second), and resets the
+// ticket for the next evaluation.  No block waits on another.
+//   Op::split_half()  -1 for a whole tile, else 0 or 1 (uniform in a block)
+//   Op::split_slot()  the tile's scratch slot; Op::ws, Op::tickets
+template <class Op, class = void>
+struct dm_tail_split {
+    static constexpr bool value = false;
+};
+template <class Op>
+struct dm_tail_split<Op, std::void_t<decltype(Op::TAIL_SPLIT)>> {
+    static constexpr bool value = Op::TAIL_SPLIT;
+};
+
+template <class Op>
+__device__ __forceinline__ void dm_split_store(const Op& op, const typename Op::Block& blk, int half, int wm, int wn,
+                                               int mt, int nt, const double (&acc)[4][Op::BN / 16][2]) {
+    constexpr int NJ = Op::BN / 16, TILE = DM_BM * Op::BN;
+    const int lane = threadIdx.x & 31, slot = op.split_slot();
+    __shared__ unsigned s_ticket;
+    double* mine = op.ws + ((i64)slot * 2 + half) * TILE;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+            if (i < mt && j < nt) {
+                __stcg(mine + ((i * NJ + j) * 2) * DM_THREADS + threadIdx.x, acc[i][j][0]);
+                __stcg(mine + ((i * NJ + j) * 2 + 1) * DM_THREADS + threadIdx.x, acc[i][j][1]);
+            }
+    __threadfence();  // the partial is visible before the ticket is taken
+    __syncthreads();
+    if (threadIdx.x == 0) s_ticket = atomicAdd(op.tickets + slot, 1u);
+    __syncthreads();
+    if (s_ticket == 0) return;  // the other half arrives second and sums
+    __threadfence();
+    const double* other = op.ws + ((i64)slot * 2 + (half ^ 1)) * TILE;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+            if (i < mt && j < nt) {
+                const double o0 = __ldcg(other + ((i * NJ + j) * 2) * DM_THREADS + threadIdx.x);
+                const double o1 = __ldcg(other + ((i * NJ + j) * 2 + 1) * DM_THREADS + threadIdx.x);
+                op.store(blk, wm + 8 * i + (lane >> 2), wn + 8 * j + 2 * (lane & 3), acc[i][j][0] + o0,
+                         acc[i][j][1] + o1);
+            }
+    if (threadIdx.x == 0) op.tickets[slot] = 0u;
+}
+
 template <class Op, bool CLUSTER = false>
 __global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(const Op op) {
     constexpr int NJ = Op::BN / 16, STAGE = DM_TILE_A + dm_tile_b(Op::BN), NS = dm_stages_of<Op>::value;
@@ -279,6 +334,13 @@ __global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(co
         dm_cluster_reduce<Op, CLUSTER>(op, blk, true, dm_smem, wm, wn, mt, nt, acc);
         return;
     }
+    if constexpr (dm_tail_split<Op>::value) {
+        const int half = op.split_half();
+        if (half >= 0) {
+            dm_split_store(op, blk, half, wm, wn, mt, nt, acc);
+            return;
+        }
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -301,6 +363,20 @@ void dmma_prepare() {
     GLI_CUDA(cudaFuncSetAttribute(k_dmma<Op, CLUSTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   dm_smem(Op::BN, dm_stages_of<Op>::value)));
     done.fetch_or(bit);
+}
+
+// blocks of k_dmma<Op> resident on one SM (registers and shared memory)
+template <class Op>
+int dmma_blocks_per_sm() {
+    static std::atomic<int> cached{0};
+    int v = cached.load();
+    if (v > 0) return v;
+    dmma_prepare<Op>();
+    GLI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_dmma<Op>, DM_THREADS,
+                                                           dm_smem(Op::BN, dm_stages_of<Op>::value)));
+    v = v > 0 ? v : 1;
+    cached.store(v);
+    return v;
 }
 
 // one launch of k_dmma<Op> on grid `grid`

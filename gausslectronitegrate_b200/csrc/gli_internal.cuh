@@ -188,6 +188,12 @@ void clear_table_cache();
 void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
                           const int64_t* d_indices, i64 m, double tol, int form,
                           double* d_out, cudaStream_t s, ContractStats* stats);
+// the same queued without a host wait: returns a ticket; sparse_values_wait
+// reads its status (and that of every evaluation queued before it on this
+// thread), evaluating again where a sized graph overflowed
+i64 sparse_values_device_async(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
+                               i64 m, double tol, int form, double* d_out, cudaStream_t s);
+void sparse_values_wait(i64 ticket);
 // the same from host buffers (pinned staging, one synchronisation)
 void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices, i64 m,
                         double tol, int form, double* h_out, cudaStream_t s);

@@ -268,10 +268,27 @@ const char* gli_b200_version(void);
  * semantics as compute_sparse_{eri,erida}_gausslet_integrals (reference
  * src/eri_integrals.c:544-678, src/erida_integrals.c:429-542).  stream is a
  * cudaStream_t (NULL = the library's per-thread stream); the call returns
- * after the work is queued on it.  Returns a gli_b200_status. */
+ * when the values are complete (it reads the evaluation's status back).
+ * Returns a gli_b200_status. */
 int gli_b200_sparse_values_dev(int kind, const double* coeffs, glong num_coeffs,
 	const struct cartesian_grid_3d* grid, const glong* d_indices, glong num,
 	double tol, int form, double* d_values, void* stream);
+
+/* The same evaluation in stream order: queued on stream without waiting for
+ * it (the first call for a class list plans it exactly and waits once).  The
+ * values in d_values are defined once gli_b200_sparse_values_wait(*ticket)
+ * has returned 0; until then the class list and d_values must not be written
+ * by other work.  Tickets belong to the calling thread. */
+int gli_b200_sparse_values_dev_async(int kind, const double* coeffs, glong num_coeffs,
+	const struct cartesian_grid_3d* grid, const glong* d_indices, glong num,
+	double tol, int form, double* d_values, void* stream, glong* ticket);
+
+/* Waits for the evaluation of `ticket` and every one queued before it on this
+ * thread, in order, and reads their status.  An evaluation whose class list
+ * no longer fits the plan its graph was sized for (the list was rewritten in
+ * place) is evaluated again here.  Returns the first error met (the
+ * evaluations after it stay pending). */
+int gli_b200_sparse_values_wait(glong ticket);
 
 /* Same evaluation with host buffers (copies inside): the reference call with a
  * form switch.  values receives num doubles. */

@@ -1,0 +1,131 @@
+"""Repeated evaluations of one class list in device memory (the ERI 7^3
+stand-in of the 6x6x6 configuration, 364 axis keys: the exact plan, then CUDA
+graph replays sized by it).  A replay reuses the plan of the one before it
+while the list is unchanged, and decodes and checks each class in the gather
+instead of marking the list.  The caller may rewrite the list in place between
+calls: a permutation of the same classes reuses the plan, classes outside it
+make the library evaluate again with an exact plan, and an index outside the
+tensor is still reported.  Every result is checked against one evaluation of
+the whole list (the parity bar of the reference's tests)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from _common import assert_parity, g10
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gli():
+    import gausslectronitegrate_b200 as m
+    if m.lib().gli_b200_device_count() == 0:
+        pytest.fail("no CUDA device: the gpu tests need a B200")
+    return m
+
+
+def test_replays_follow_the_list_in_device_memory(gli):
+    import torch
+
+    from gausslectronitegrate_b200 import _abi
+    from gausslectronitegrate_b200 import workloads as W
+    full = gli.compute_sparse_eri_gausslet_integrals(g10(), W.ERI6_SPARSE, 1e-16)
+    m = full.indices.size // 2
+    first, second = full.indices[:m], full.indices[m:2 * m]
+    ref_first, ref_second = full.values[:m], full.values[m:2 * m]
+    b = np.ascontiguousarray(g10())
+    gs = gli._grid_struct(W.ERI6_SPARSE)
+    d_idx = torch.from_numpy(first.copy()).cuda()
+    d_out = torch.empty(m, dtype=torch.float64, device="cuda")
+    L = gli.lib()
+
+    def run():
+        d_out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        rc = L.gli_b200_sparse_values_dev(_abi.GLI_KIND_ERI, b.ctypes.data_as(_abi.dptr), b.size, C.byref(gs),
+                                          C.c_void_p(d_idx.data_ptr()), m, 1e-16, _abi.GLI_FORM_FP64,
+                                          C.c_void_p(d_out.data_ptr()), None)
+        torch.cuda.synchronize()
+        return rc
+
+    # exact plan and capture; the first replay plans; later replays reuse it
+    for k in range(4):
+        assert run() == 0, L.gli_b200_last_error_message().decode()
+        assert_parity(d_out.cpu().numpy(), ref_first, what=f"first half, call {k}")
+    # the same classes in another order: every class lies in the reused plan
+    perm = np.random.default_rng(5).permutation(m)
+    d_idx.copy_(torch.from_numpy(first[perm]))
+    for k in range(2):
+        assert run() == 0, L.gli_b200_last_error_message().decode()
+        assert_parity(d_out.cpu().numpy(), ref_first[perm], what=f"permuted first half, call {k}")
+    # other classes: keys and pairs outside the plan
+    d_idx.copy_(torch.from_numpy(second))
+    for k in range(3):
+        assert run() == 0, L.gli_b200_last_error_message().decode()
+        assert_parity(d_out.cpu().numpy(), ref_second, what=f"second half, call {k}")
+    # an index outside the tensor, then the list repaired
+    d_idx[12345] = -1
+    assert run() != 0
+    assert "outside" in L.gli_b200_last_error_message().decode()
+    d_idx[12345] = int(second[12345])
+    assert run() == 0, L.gli_b200_last_error_message().decode()
+    assert_parity(d_out.cpu().numpy(), ref_second, what="second half after the bad index")
+
+
+def test_stream_ordered_evaluations(gli):
+    # gli_b200_sparse_values_dev_async: several evaluations queued on one
+    # stream, their status read by one wait; a list rewritten in place between
+    # them (so that a queued replay overflows its plan) is evaluated again in
+    # the wait; an index outside the tensor is reported by the wait
+    import torch
+
+    from gausslectronitegrate_b200 import _abi
+    from gausslectronitegrate_b200 import workloads as W
+    full = gli.compute_sparse_eri_gausslet_integrals(g10(), W.ERI6_SPARSE, 1e-16)
+    m = full.indices.size // 3
+    parts = [full.indices[k * m:(k + 1) * m] for k in range(3)]
+    refs = [full.values[k * m:(k + 1) * m] for k in range(3)]
+    b = np.ascontiguousarray(g10())
+    gs = gli._grid_struct(W.ERI6_SPARSE)
+    L = gli.lib()
+    stream = torch.cuda.Stream()
+    d_idx = torch.from_numpy(parts[0].copy()).cuda()
+    outs = [torch.full((m,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
+
+    def queue(out):
+        t = _abi.glong()
+        rc = L.gli_b200_sparse_values_dev_async(_abi.GLI_KIND_ERI, b.ctypes.data_as(_abi.dptr), b.size, C.byref(gs),
+                                                C.c_void_p(d_idx.data_ptr()), m, 1e-16, _abi.GLI_FORM_FP64,
+                                                C.c_void_p(out.data_ptr()), C.c_void_p(stream.cuda_stream),
+                                                C.byref(t))
+        assert rc == 0, L.gli_b200_last_error_message().decode()
+        return t.value
+
+    # per output buffer, the first call plans exactly (and waits once); the
+    # next ones replay its sized graph, the first replay planning again and the
+    # later ones reusing that plan
+    tickets = [queue(outs[0]) for _ in range(3)] + [queue(outs[1]) for _ in range(3)]
+    assert tickets == sorted(tickets)
+    assert L.gli_b200_sparse_values_wait(tickets[-1]) == 0, L.gli_b200_last_error_message().decode()
+    for o in outs[:2]:
+        assert_parity(o.cpu().numpy(), refs[0], what="queued evaluations of the first third")
+    # a replay queued after an in-place rewrite on the same stream
+    with torch.cuda.stream(stream):
+        d_idx.copy_(torch.from_numpy(parts[1]).to("cuda", non_blocking=False))
+    t = queue(outs[0])
+    assert L.gli_b200_sparse_values_wait(t) == 0, L.gli_b200_last_error_message().decode()
+    assert_parity(outs[0].cpu().numpy(), refs[1], what="queued evaluation after the rewrite")
+    # an unknown ticket, then an index outside the tensor
+    assert L.gli_b200_sparse_values_wait(t) != 0
+    with torch.cuda.stream(stream):
+        d_idx.copy_(torch.from_numpy(parts[2]).cuda())
+        d_idx[7] = -5
+    t = queue(outs[1])
+    assert L.gli_b200_sparse_values_wait(t) != 0
+    assert "outside" in L.gli_b200_last_error_message().decode()
+    with torch.cuda.stream(stream):
+        d_idx[7] = int(parts[2][7])
+    t = queue(outs[1])
+    assert L.gli_b200_sparse_values_wait(t) == 0, L.gli_b200_last_error_message().decode()
+    assert_parity(outs[1].cpu().numpy(), refs[2], what="queued evaluation after the repair")
