@@ -126,8 +126,6 @@ __device__ inline void decode_pt(const ClassDecode& d, uint32_t lin, int p[3]) {
 
 // coordinates of every grid point (ERI decoding)
 __global__ void k_point_table(ClassDecode d, short4* __restrict__ pt) {
-    pdl_wait();
-    pdl_release();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n32) return;
     int p[3];
@@ -145,8 +143,6 @@ __device__ __forceinline__ uint32_t pd_field(int dax, int sax) {
 // replays): when *skip is set the table kept with the replay's saved plan is
 // current (a function of the grid alone, made by the replay that made the plan)
 __global__ void k_pair_desc(ClassDecode d, uint2* __restrict__ pd, const int* __restrict__ skip) {
-    pdl_wait();
-    pdl_release();
     if (skip && *skip) return;
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if ((uint64_t)h >= d.N2) return;
@@ -250,8 +246,6 @@ struct PlanCounts {
 __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
                                               uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
                                               uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
-    pdl_wait();
-    pdl_release();
     extern __shared__ uint32_t sflag[];
     const int nk = (int)d.nkeys;
     const int words = (nk * nk + 31) >> 5;
@@ -358,8 +352,6 @@ __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_
                                                      uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
                                                      uint64_t* __restrict__ keys, int* __restrict__ bad, int local,
                                                      const int* __restrict__ skip) {
-    pdl_wait();
-    pdl_release();
     if (skip && *skip) return;
     extern __shared__ uint32_t sflag[];
     const int nk = (int)d.nkeys;
@@ -448,8 +440,6 @@ static size_t mark_local_bytes(i64 nk) {
 __global__ void k_plan_keys(i64 nk, const uint32_t* __restrict__ used, const uint64_t* __restrict__ ids,
                             int* __restrict__ keyOf, int* __restrict__ aId, int* __restrict__ aKey,
                             PlanCounts* __restrict__ cnt) {
-    pdl_wait();
-    pdl_release();
     const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t nku = ids[nk];  // exclusive scan at nk = number of used keys
     if (k == 0) {
@@ -496,8 +486,6 @@ __global__ void __launch_bounds__(1024) k_plan_keys_small(i64 nk, const uint32_t
                                                           uint64_t* __restrict__ ids, int* __restrict__ keyOf,
                                                           int* __restrict__ aId, int* __restrict__ aKey,
                                                           PlanCounts* __restrict__ cnt) {
-    pdl_wait();
-    pdl_release();
     __shared__ uint32_t ws[32], total, nku_s;
     const int k = threadIdx.x;  // flag k of 2 nk (<= 512)
     const uint32_t f = k < 2 * nk ? used[k] : 0u;
@@ -526,8 +514,6 @@ __global__ void __launch_bounds__(1024) k_pairs_small(i64 words, int nk, const u
                                                       const int* __restrict__ aId, uint64_t* __restrict__ pre,
                                                       int* __restrict__ pairA, int* __restrict__ pairB,
                                                       PlanCounts* __restrict__ cnt) {
-    pdl_wait();
-    pdl_release();
     __shared__ uint32_t ws[32], total;
     uint32_t carry = 0;
     for (i64 base = 0; base < words; base += 1024) {
@@ -551,16 +537,12 @@ __global__ void __launch_bounds__(1024) k_pairs_small(i64 words, int nk, const u
 
 // set bits per word of the pair bitmap (the exclusive scan of which gives pre)
 __global__ void k_word_counts(i64 words, const uint32_t* __restrict__ bits, uint32_t* __restrict__ counts) {
-    pdl_wait();
-    pdl_release();
     const i64 w = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (w < words) counts[w] = __popc(bits[w]);
 }
 
 __global__ void k_pair_lists(i64 words, int nk, const uint32_t* __restrict__ bits, const uint64_t* __restrict__ pre,
                              const int* __restrict__ aId, int* __restrict__ pairA, int* __restrict__ pairB) {
-    pdl_wait();
-    pdl_release();
     const i64 w = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= words) return;
     uint32_t b = bits[w];
@@ -852,8 +834,6 @@ __global__ void __launch_bounds__(256) k_stage_c(const double* __restrict__ W, c
                                                   const uint64_t* __restrict__ pairPre, i64 m, int U, int Up,
                                                   const PlanCounts* __restrict__ cnt, int choice,
                                                   double* __restrict__ out) {
-    pdl_wait();
-    pdl_release();
     if (cnt->overflow || !choice_runs(choice, cnt, m)) return;
     const int lane = threadIdx.x & 31;
     const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
@@ -978,8 +958,6 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
                                                    const uint64_t* __restrict__ pairPre, int ldq,
                                                    const PlanCounts* __restrict__ cnt, int choice,
                                                    double* __restrict__ out) {
-    pdl_wait();
-    pdl_release();
     if (cnt->overflow || !choice_runs(choice, cnt, m)) return;
     // four consecutive classes per group, two groups per thread and step
     // (16-byte loads and stores where the arrays allow): each class is a chain
@@ -1065,8 +1043,6 @@ __global__ void __launch_bounds__(256) k_gather_q_pd(const double* __restrict__ 
                                                       const uint32_t* __restrict__ pairBits,
                                                       const uint64_t* __restrict__ pairPre, int ldq,
                                                       PlanCounts* __restrict__ cnt, double* __restrict__ out) {
-    pdl_wait();
-    pdl_release();
     if (cnt->overflow) return;
     const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)out & 15) == 0;
     const i64 groups = (m + 3) / 4, stride = (i64)gridDim.x * blockDim.x;
@@ -1344,8 +1320,6 @@ __global__ void __launch_bounds__(1024) k_pair_tiles(const int* __restrict__ pai
                                                       int* __restrict__ tile0, int* __restrict__ tile_batch,
                                                       int* __restrict__ tile_col0, int* __restrict__ tile_ncols,
                                                       int* __restrict__ rowPair, int* __restrict__ rowKey) {
-    pdl_wait();
-    pdl_release();
     pair_tiles_block(false, pairA, pairB, aKey, (int)cnt->nP, (int)cnt->nA, (int)cnt->nku, bn, max_tiles, first,
                      tile0, tile_batch, tile_col0, tile_ncols, rowPair, rowKey);
 }
@@ -1446,8 +1420,6 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
                                                      int* __restrict__ tile_ncols, int* __restrict__ rowPair,
                                                      int* __restrict__ rowKey, PlanCounts* __restrict__ cnt,
                                                      PlanReuse reuse) {
-    pdl_wait();
-    pdl_release();
     __shared__ uint32_t ws[32], total, nku_s;
     __shared__ uint32_t s_bits[PLAN_SMALL_WORDS], s_pre[PLAN_SMALL_WORDS];
     __shared__ int s_aId[PLAN_SMALL_KEYS], s_aKey[PLAN_SMALL_KEYS];
@@ -1767,7 +1739,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     // Bounded and sized evaluations know every size here: all their buffers
     // are allocated and zeroed before the first kernel, so that a captured
     // graph has its allocation and memset nodes at the root and its kernels
-    // follow one another directly (programmatic launch edges throughout)
+    // follow one another directly
     const bool known = mode != PLAN_EXACT;
     // usedKey and usedA side by side so that one scan serves both; pair flags
     // over all key pairs (slot k2 * nk + k1)
@@ -1857,39 +1829,39 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     if (known) stage_bufs();
 
     if (dec.pd)
-        launch_pdl(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p, pd_skip);
+        launch_kernel(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p, pd_skip);
     else if (dec.kind == 1)
-        launch_pdl(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
+        launch_kernel(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
     {
         const size_t lb = mark_local_bytes(nk);
         if (dec.pd) {
             const i64 groups = (m + 3) / 4;
             const unsigned mb = (unsigned)std::min<i64>((groups + 255) / 256, (i64)a.num_sms * 8);
-            launch_pdl(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
+            launch_kernel(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
                        lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
         } else {
             const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
-            launch_pdl(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
+            launch_kernel(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
                        lb ? 1 : 0);
         }
     }
     if (plan_small) {
-        launch_pdl(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
+        launch_kernel(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
                    tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt,
                    pstore ? pstore->reuse(fused) : PlanReuse{});
         tiles.built = true;
     } else {
         if (2 * nk <= 1024) {
-            launch_pdl(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
+            launch_kernel(k_plan_keys_small, dim3(1), dim3(1024), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
         } else {
             exclusive_scan_u32_dev(used.p, ids.p, 2 * nk, &cnt->key_total, s);
-            launch_pdl(k_plan_keys, dim3(kb), dim3(256), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
+            launch_kernel(k_plan_keys, dim3(kb), dim3(256), 0, s, nk, used.p, ids.p, keyOf.p, aId.p, aKey.p, cnt);
         }
         DevBuf<uint32_t> counts;
         if (!small_pairs) {
             counts.alloc(words, s);
-            launch_pdl(k_word_counts, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, pairBits.p,
+            launch_kernel(k_word_counts, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, pairBits.p,
                        counts.p);
             exclusive_scan_u32_dev(counts.p, pairPre.p, words, &cnt->nP, s);
         }
@@ -1905,10 +1877,10 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         pairA.alloc(sz.nP, s);
         pairB.alloc(sz.nP, s);
         if (small_pairs)
-            launch_pdl(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p,
+            launch_kernel(k_pairs_small, dim3(1), dim3(1024), 0, s, words, (int)nk, pairBits.p, aId.p, pairPre.p,
                        pairA.p, pairB.p, cnt);
         else
-            launch_pdl(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk,
+            launch_kernel(k_pair_lists, dim3((unsigned)((words + 255) / 256)), dim3(256), 0, s, words, (int)nk,
                        pairBits.p, pairPre.p, aId.p, pairA.p, pairB.p);
     }
     if (!known) stage_bufs();
@@ -1977,7 +1949,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         slice_tiled(ExpandedHRows{H.p, t.sidx.p, cnt, nS, U, mb}, nA * U, U, Hs, s);
         if (!tiles.built) {
             tiles.alloc(nA, nP, BN, false, s);
-            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, pairB.p, aKey.p, cnt, BN,
+            launch_kernel(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, pairB.p, aKey.p, cnt, BN,
                        (int)tiles.max_tiles, tiles.first, tiles.tile0, tiles.batch, tiles.col0, tiles.ncols,
                        (int*)nullptr, (int*)nullptr);
         }
@@ -2000,7 +1972,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         // tiles of 64 rows of one host A key, then (tile, 64 u, chunk of v) blocks
         if (!tiles.built) {
             tiles.alloc(nA, nP, DM_BM, true, s);
-            launch_pdl(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, pairB.p, aKey.p, cnt, DM_BM,
+            launch_kernel(k_pair_tiles, dim3(1), dim3(1024), 0, s, pairA.p, pairB.p, aKey.p, cnt, DM_BM,
                        (int)tiles.max_tiles, tiles.first, tiles.tile0, tiles.batch, tiles.col0, tiles.ncols,
                        tiles.rowPair, tiles.rowKey);
         }
@@ -2058,16 +2030,16 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
         if (fused)  // the plan's own pair bitmap: this replay's stays empty when the mark pass skipped
-            launch_pdl(k_gather_q_pd, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
+            launch_kernel(k_gather_q_pd, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
                        (const uint32_t*)pstore->saved_bits.p, pairPre.p, (int)nku, cnt, a.out);
         else
-            launch_pdl(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
+            launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
                        pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
-        launch_pdl(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, dec, a.idx, (int)nk, pairBits.p, pairPre.p, m, U, Up,
+        launch_kernel(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, dec, a.idx, (int)nk, pairBits.p, pairPre.p, m, U, Up,
                    cnt, c_class, a.out);
     }
     timer.mark();

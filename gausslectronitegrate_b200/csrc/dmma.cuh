@@ -292,8 +292,6 @@ __global__ void __launch_bounds__(DM_THREADS, dm_blocks_of<Op>::value) k_dmma(co
     static_assert(NS >= 2 && NS <= 3, "two or three stages");
     static_assert(!CLUSTER || DM_BM * (Op::BN + DM_RED_LD) <= NS * STAGE, "reduction tile exceeds the operand ring");
     extern __shared__ __align__(16) double dm_smem[];
-    pdl_wait();  // the previous kernel's results are visible from here
-    pdl_release();
     typename Op::Block blk;
     const bool active = op.begin(blk);
     if (!active) {
@@ -384,7 +382,7 @@ template <class Op>
 void dmma_launch(const Op& op, dim3 grid, cudaStream_t s) {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
     dmma_prepare<Op>();
-    launch_pdl(k_dmma<Op>, grid, dim3(DM_THREADS), dm_smem(Op::BN, dm_stages_of<Op>::value), s, op);
+    launch_kernel(k_dmma<Op>, grid, dim3(DM_THREADS), dm_smem(Op::BN, dm_stages_of<Op>::value), s, op);
 }
 
 // the same with K split over grid.z (2..8) blocks that sum their partial tiles
@@ -400,15 +398,13 @@ void dmma_launch_cluster(const Op& op, dim3 grid, cudaStream_t s) {
     cfg.blockDim = dim3(DM_THREADS);
     cfg.dynamicSmemBytes = dm_smem(Op::BN, dm_stages_of<Op>::value);
     cfg.stream = s;
-    cudaLaunchAttribute attr[2];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    attr[1].id = cudaLaunchAttributeClusterDimension;
-    attr[1].val.clusterDim.x = 1;
-    attr[1].val.clusterDim.y = 1;
-    attr[1].val.clusterDim.z = grid.z;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = grid.z;
     cfg.attrs = attr;
-    cfg.numAttrs = 2;
+    cfg.numAttrs = 1;
     GLI_CUDA(cudaLaunchKernelEx(&cfg, k_dmma<Op, true>, op));
     count_launch();
 }

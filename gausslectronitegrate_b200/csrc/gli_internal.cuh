@@ -57,28 +57,14 @@ void count_launch();
         GLI_CUDA(cudaGetLastError()); \
     } while (0)
 
-// Programmatic dependent launch.  A kernel launched by launch_pdl may be
-// scheduled while the kernel before it on the stream finishes; it calls
-// pdl_wait() before its first global-memory access (griddepcontrol.wait
-// returns once the preceding grid has completed and its writes are visible: a
-// hardware dependency, not a flag spin) and pdl_release() to let the next
-// such launch be scheduled.  Both are no-ops for a plain launch.  This hides
-// the gap between the dozen short kernels of a small evaluation.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-
+// one launch on stream s (the arguments converted to the kernel's parameter types)
 template <typename... KArgs, typename... Args>
-void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+void launch_kernel(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
     GLI_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...));
     count_launch();
 }

@@ -170,8 +170,6 @@ __global__ void __launch_bounds__(256, 1) k_tc_gemm(TiledOperand A, TiledOperand
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
 
-    pdl_wait();  // launched with programmatic dependent launch: the inputs are ready from here
-    pdl_release();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int t = blockIdx.x, mt = blockIdx.y;
     const int batch = w.tile_batch ? w.tile_batch[t] : 0;
@@ -315,7 +313,7 @@ static void launch_variant(const TiledOperand& A, const TiledOperand& B, const T
                            cudaStream_t s) {
     constexpr int smem = smem_bytes<S>();
     dim3 grid((unsigned)ntiles, (unsigned)w.a_blocks);
-    launch_pdl(k_tc_gemm<S, R>, grid, dim3(256), smem, s, A, B, w, err);
+    launch_kernel(k_tc_gemm<S, R>, grid, dim3(256), smem, s, A, B, w, err);
 }
 
 void tc_gemm_tiled(const TiledOperand& A, const TiledOperand& B, const TileWork& w, int ntiles, int* d_err,

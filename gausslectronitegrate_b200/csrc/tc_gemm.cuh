@@ -102,8 +102,6 @@ template <class Src>
 __global__ void __launch_bounds__(256) k_slice_group(Src src, i64 rows, int K, int nkc, int S, int RB,
                                                      int8_t* __restrict__ dst, int* __restrict__ e) {
     __shared__ __align__(16) int8_t stage[SLICE_GROUP_NKC][SLICE_GROUP_S][512];
-    pdl_wait();
-    pdl_release();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const i64 d0 = (i64)blockIdx.x * 8, dr = d0 + w;
     i64 sr = src.source(dr, rows);
@@ -151,8 +149,6 @@ __global__ void __launch_bounds__(256) k_slice_group(Src src, i64 rows, int K, i
 template <class Src>
 __global__ void k_slice_rows_any(Src src, i64 rows, int K, int nkc, int S, int RB, int8_t* __restrict__ dst,
                                  int* __restrict__ e) {
-    pdl_wait();
-    pdl_release();
     const i64 r = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (r >= rows || !src.valid(r)) return;  // uniform across the warp
@@ -187,10 +183,10 @@ void launch_slice(const Src& src, i64 rows, i64 padded_rows, int K, int nkc, int
                   cudaStream_t s) {
     if (rows <= 0 || padded_rows <= 0) return;
     if (nkc <= SLICE_GROUP_NKC && S <= SLICE_GROUP_S && RB % 8 == 0)
-        launch_pdl(k_slice_group<Src>, dim3((unsigned)(padded_rows / 8)), dim3(256), 0, s, src, rows, K, nkc, S, RB,
+        launch_kernel(k_slice_group<Src>, dim3((unsigned)(padded_rows / 8)), dim3(256), 0, s, src, rows, K, nkc, S, RB,
                    dst, e);
     else
-        launch_pdl(k_slice_rows_any<Src>, dim3((unsigned)((rows * 32 + 255) / 256)), dim3(256), 0, s, src, rows, K,
+        launch_kernel(k_slice_rows_any<Src>, dim3((unsigned)((rows * 32 + 255) / 256)), dim3(256), 0, s, src, rows, K,
                    nkc, S, RB, dst, e);
 }
 
