@@ -243,9 +243,13 @@ struct PlanCounts {
 // merges them once.  used = [usedKey | usedA], 2 nk flags.  keys may be null:
 // the later passes then decode the classes again (the pair-descriptor decode
 // costs less than writing and re-reading 8 bytes per class).
+// skip: as in k_mark_eri_pd (replays whose gather decodes and checks the
+// classes against a saved plan).
 __global__ void __launch_bounds__(256) k_mark(ClassDecode d, const int64_t* __restrict__ idx, i64 m,
                                               uint32_t* __restrict__ used, uint32_t* __restrict__ pairBits,
-                                              uint64_t* __restrict__ keys, int* __restrict__ bad, int local) {
+                                              uint64_t* __restrict__ keys, int* __restrict__ bad, int local,
+                                              const int* __restrict__ skip) {
+    if (skip && *skip) return;
     extern __shared__ uint32_t sflag[];
     const int nk = (int)d.nkeys;
     const int words = (nk * nk + 31) >> 5;
@@ -344,7 +348,7 @@ __device__ __forceinline__ bool pd_class_keys(const ClassDecode& d, int64_t x, u
 // is still decoded correctly: an out-of-range remainder takes the quotient
 // again), and a pair bit already set by the thread's previous class is not
 // tested again.  Flags and pair bits as in k_mark.
-// skip (non-null in sized replays that may reuse their plan): when *skip is
+// skip (non-null in replays that may reuse their plan): when *skip is
 // set, the saved plan stands for this replay unless the class gather finds a
 // class outside it, so the classes are not marked here (the gather decodes
 // and checks them).  keys may be null (such replays do not read them).
@@ -1027,22 +1031,23 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
     }
 }
 
-// The class gather of sized replays that reuse their plan without marking the
-// classes (k_mark_eri_pd skipped): each class is decoded here from its index
-// through the pair descriptors and checked against the plan -- its (A, B) pair
-// set in the plan's pair bitmap and its third key a used key (kid[k2 + 1] >
-// kid[k2]), which the marks of the list that made the plan guarantee for every
-// class of that list.  A class outside the plan (the list was rewritten in
-// place since) or outside the tensor sets the overflow flag, and the host
-// evaluates the list again with an exact plan.  This saves the mark pass's
-// read of the indices and the write and re-read of the packed keys (24 bytes
-// per class).
-__global__ void __launch_bounds__(256) k_gather_q_pd(const double* __restrict__ Q, int parts, i64 part_stride,
-                                                      ClassDecode dec, const int64_t* __restrict__ idx, i64 m,
-                                                      const uint64_t* __restrict__ kid, int nk,
-                                                      const uint32_t* __restrict__ pairBits,
-                                                      const uint64_t* __restrict__ pairPre, int ldq,
-                                                      PlanCounts* __restrict__ cnt, double* __restrict__ out) {
+// The class gather of replays that reuse their plan without marking the
+// classes (the mark pass skipped): each class is decoded here from its index
+// (through the pair descriptors where PD, else class_keys) and checked against
+// the plan -- its (A, B) pair set in the plan's pair bitmap and its third key
+// a used key (kid[k2 + 1] > kid[k2]), which the marks of the list that made
+// the plan guarantee for every class of that list.  A class outside the plan
+// (the list was rewritten in place since) or outside the tensor sets the
+// overflow flag, and the host evaluates the list again with a new plan.  This
+// saves the mark pass's read of the indices and the write and re-read of the
+// packed keys (24 bytes per class).
+template <bool PD>
+__global__ void __launch_bounds__(256) k_gather_q_plan(const double* __restrict__ Q, int parts, i64 part_stride,
+                                                        ClassDecode dec, const int64_t* __restrict__ idx, i64 m,
+                                                        const uint64_t* __restrict__ kid, int nk,
+                                                        const uint32_t* __restrict__ pairBits,
+                                                        const uint64_t* __restrict__ pairPre, int ldq,
+                                                        PlanCounts* __restrict__ cnt, double* __restrict__ out) {
     if (cnt->overflow) return;
     const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)out & 15) == 0;
     const i64 groups = (m + 3) / 4, stride = (i64)gridDim.x * blockDim.x;
@@ -1074,9 +1079,18 @@ __global__ void __launch_bounds__(256) k_gather_q_pd(const double* __restrict__ 
                 q[h][v] = -1;
                 if (n0 + v >= m) continue;
                 int s0, s1, s2;
-                if (!pd_class_keys(dec, c[h][v], hi, da, s0, s1, s2)) {
-                    miss = true;
-                    continue;
+                if constexpr (PD) {
+                    if (!pd_class_keys(dec, c[h][v], hi, da, s0, s1, s2)) {
+                        miss = true;
+                        continue;
+                    }
+                } else {
+                    int k[3];
+                    if (!class_keys(dec, c[h][v], k)) {
+                        miss = true;
+                        continue;
+                    }
+                    s0 = k[0], s1 = k[1], s2 = k[2];
                 }
                 if (!dcheck(s0 >= 0 && s2 < nk, 1, s2)) continue;
                 const i64 slot = (i64)s1 * nk + s0;
@@ -1355,20 +1369,23 @@ struct PairTiles {
     }
 };
 
-// The plan of a sized evaluation, kept between the replays of its graph: the
-// key and pair lists, word prefixes and stage-B tiles, plus the key flags, the
-// pair bitmap and the counts they were made from.  A replay decodes and marks
-// every class again; when its key flags and pair bitmap equal the saved ones
-// (checked on the device, every replay), the plan they determine is the saved
-// one and the plan kernel only restores its counts; otherwise it plans anew
-// and saves.  (The plan is a function of those flags and bits alone.)
+// The plan of a captured evaluation (bounded or sized), kept between the
+// replays of its graph: the key and pair lists, word prefixes and stage-B
+// tiles, plus the key flags, the pair bitmap and the counts they were made
+// from.  A replay that marks its classes compares its key flags and pair
+// bitmap with the saved ones on the device: when they are equal, the plan
+// they determine is the saved one and the plan kernel only restores its
+// counts; otherwise it plans anew and saves.  (The plan is a function of those
+// flags and bits alone.)  Replays of the product form do not mark at all while
+// the saved plan is valid: their gather checks every class instead
+// (k_gather_q_plan).
 struct PlanReuse {
     uint32_t* saved_used = nullptr;
     uint32_t* saved_bits = nullptr;
     PlanCounts* saved_cnt = nullptr;
     int* valid = nullptr;  // null: no reuse (bounded plans)
-    // set: the replay did not mark its classes (k_mark_eri_pd skipped them and
-    // k_gather_q_pd checks each against the plan), so a valid saved plan is
+    // set: the replay did not mark its classes (the mark pass skipped them and
+    // k_gather_q_plan checks each against the plan), so a valid saved plan is
     // restored without the comparison
     int trust = 0;
 };
@@ -1768,11 +1785,11 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         pts.alloc(dec.N, s);
         dec.pt = pts.p;
     }
-    // Sized replays of the product form through the pair descriptors mark
-    // their classes only when the saved plan is not valid: otherwise the plan
-    // is restored and the gather decodes and checks every class (the list may
-    // have been rewritten in place since the plan was made).
-    const bool fused = pstore && dec.pd && mode == PLAN_SIZED && product_pays((double)sz.nP, (double)sz.nku, m);
+    // Replays of the product form (the host's choice) mark their classes only
+    // when the saved plan is not valid: otherwise the plan is restored and the
+    // gather decodes and checks every class (the list may have been rewritten
+    // in place since the plan was made).
+    const bool fused = pstore && mode != PLAN_EXACT && product_pays((double)sz.nP, (double)sz.nku, m);
     // packed key triple per class, written by the decode pass and read by the
     // gather (decoding a class twice, in the mark pass and again in the gather,
     // measured slower than re-reading its 8 bytes: ERI 7^3 stage C 52 against
@@ -1837,12 +1854,12 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         if (dec.pd) {
             const i64 groups = (m + 3) / 4;
             const unsigned mb = (unsigned)std::min<i64>((groups + 255) / 256, (i64)a.num_sms * 8);
-            launch_kernel(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
-                       lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
+            launch_kernel(k_mark_eri_pd, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p,
+                          &st->bad, lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
         } else {
             const unsigned mb = (unsigned)std::min<i64>(cb, (i64)a.num_sms * 8);
             launch_kernel(k_mark, dim3(mb), dim3(256), lb, s, dec, a.idx, m, used.p, pairBits.p, keys.p, &st->bad,
-                       lb ? 1 : 0);
+                          lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
         }
     }
     if (plan_small) {
@@ -2029,12 +2046,18 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                                   u_chunk, ps, Q.p, &st->products},
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
-        if (fused)  // the plan's own pair bitmap: this replay's stays empty when the mark pass skipped
-            launch_kernel(k_gather_q_pd, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
-                       (const uint32_t*)pstore->saved_bits.p, pairPre.p, (int)nku, cnt, a.out);
+        // (fused: the plan's own pair bitmap, since this replay's stays empty
+        // when the mark pass skipped)
+        const uint32_t* saved = fused ? (const uint32_t*)pstore->saved_bits.p : nullptr;
+        if (fused && dec.pd)
+            launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
+                          saved, pairPre.p, (int)nku, cnt, a.out);
+        else if (fused)
+            launch_kernel(k_gather_q_plan<false>, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p,
+                          (int)nk, saved, pairPre.p, (int)nku, cnt, a.out);
         else
             launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
-                       pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
+                          pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
@@ -2135,10 +2158,14 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<80>, true>();
     dmma_prepare<StageBOp<true>, true>();
     dmma_prepare<StageBOp<false>, true>();
-    if (mode == PLAN_SIZED) {
+    {
+        // the plan kept between replays, with room for the sized counts or the
+        // bounds of a bounded plan
         const i64 nk = a.t->nkeys, words = (nk * nk + 31) / 32;
+        const i64 capA = mode == PLAN_SIZED ? sized.nA : nk;
+        const i64 capP = mode == PLAN_SIZED ? sized.nP : std::min(nk * (nk + 1) / 2, a.m);
         e->plan = std::make_unique<PlanStore>();
-        e->plan->alloc(nk, words, sized.nA, sized.nP, PairTiles::ints(sized.nA, sized.nP, 64, true),
+        e->plan->alloc(nk, words, capA, capP, PairTiles::ints(capA, capP, 64, true),
                        pair_desc_applies(a.d) ? (i64)a.d.N2 : 0);
     }
     const long long l0 = launch_count();
@@ -2186,9 +2213,9 @@ struct PinnedBuf {
 
 // Queues one evaluation on stream s and an asynchronous copy of its status
 // block into h_status (pinned); the caller synchronises and checks it.
-// *sized receives the sized graph that was replayed (null otherwise): when its
-// status reports an overflow, the caller drops it and calls again, which
-// evaluates exactly.
+// *sized receives the graph that was replayed (null otherwise): when its
+// status reports an overflow (a sized plan outgrown, or a class outside a
+// reused plan), the caller drops it and calls again, which plans anew.
 static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
                                   const int64_t* d_indices, i64 m, double tol, int form, double* d_out, cudaStream_t s,
                                   EvalStatus* h_status, std::shared_ptr<const LatticeTables>& tp, StageTimer& timer,
@@ -2237,7 +2264,7 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
         add_launches(e->launches);
         t_paths = e->paths;
         GLI_CUDA(cudaMemcpyAsync(h_status, e->status.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
-        if (e->mode == PLAN_SIZED) *sized = e;
+        *sized = e;
         return;
     }
     DevBuf<EvalStatus> st(1, s);

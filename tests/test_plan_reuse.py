@@ -1,10 +1,11 @@
-"""Repeated evaluations of one class list in device memory (the ERI 7^3
-stand-in of the 6x6x6 configuration, 364 axis keys: the exact plan, then CUDA
-graph replays sized by it).  A replay reuses the plan of the one before it
-while the list is unchanged, and decodes and checks each class in the gather
-instead of marking the list.  The caller may rewrite the list in place between
+"""Repeated evaluations of one class list in device memory: the ERI 7^3
+stand-in of the 6x6x6 configuration (364 axis keys: the exact plan, then CUDA
+graph replays sized by it) and ERIDA lists (bounded plans, captured at once).
+A replay reuses the plan of the one before it while the list is unchanged;
+replays of the product form decode and check each class in the gather instead
+of marking the list.  The caller may rewrite the list in place between
 calls: a permutation of the same classes reuses the plan, classes outside it
-make the library evaluate again with an exact plan, and an index outside the
+make the library evaluate again with a new plan, and an index outside the
 tensor is still reported.  Every result is checked against one evaluation of
 the whole list (the parity bar of the reference's tests)."""
 import ctypes as C
@@ -25,17 +26,31 @@ def gli():
     return m
 
 
-def test_replays_follow_the_list_in_device_memory(gli):
+CASES = {
+    # (kind, grid): ERI 7^3 (sized plan, product form, pair-descriptor decode),
+    # ERIDA 129^3 (bounded plan, product form), ERIDA 33^3 (bounded plan,
+    # per-class stage C: the replays mark and compare with the saved plan)
+    "eri7": (1, lambda W: W.ERI6_SPARSE),
+    "erida129": (0, lambda W: W.sym_grid(129)),
+    "erida33": (0, lambda W: W.sym_grid(33)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_replays_follow_the_list_in_device_memory(gli, case):
     import torch
 
     from gausslectronitegrate_b200 import _abi
     from gausslectronitegrate_b200 import workloads as W
-    full = gli.compute_sparse_eri_gausslet_integrals(g10(), W.ERI6_SPARSE, 1e-16)
+    kind, grid_of = CASES[case]
+    grid = grid_of(W)
+    compute = gli.compute_sparse_eri_gausslet_integrals if kind else gli.compute_sparse_erida_gausslet_integrals
+    full = compute(g10(), grid, 1e-16)
     m = full.indices.size // 2
     first, second = full.indices[:m], full.indices[m:2 * m]
     ref_first, ref_second = full.values[:m], full.values[m:2 * m]
     b = np.ascontiguousarray(g10())
-    gs = gli._grid_struct(W.ERI6_SPARSE)
+    gs = gli._grid_struct(grid)
     d_idx = torch.from_numpy(first.copy()).cuda()
     d_out = torch.empty(m, dtype=torch.float64, device="cuda")
     L = gli.lib()
@@ -43,7 +58,7 @@ def test_replays_follow_the_list_in_device_memory(gli):
     def run():
         d_out.fill_(float("nan"))
         torch.cuda.synchronize()
-        rc = L.gli_b200_sparse_values_dev(_abi.GLI_KIND_ERI, b.ctypes.data_as(_abi.dptr), b.size, C.byref(gs),
+        rc = L.gli_b200_sparse_values_dev(kind, b.ctypes.data_as(_abi.dptr), b.size, C.byref(gs),
                                           C.c_void_p(d_idx.data_ptr()), m, 1e-16, _abi.GLI_FORM_FP64,
                                           C.c_void_p(d_out.data_ptr()), None)
         torch.cuda.synchronize()
@@ -65,10 +80,11 @@ def test_replays_follow_the_list_in_device_memory(gli):
         assert run() == 0, L.gli_b200_last_error_message().decode()
         assert_parity(d_out.cpu().numpy(), ref_second, what=f"second half, call {k}")
     # an index outside the tensor, then the list repaired
-    d_idx[12345] = -1
+    bad = m // 3
+    d_idx[bad] = -1
     assert run() != 0
     assert "outside" in L.gli_b200_last_error_message().decode()
-    d_idx[12345] = int(second[12345])
+    d_idx[bad] = int(second[bad])
     assert run() == 0, L.gli_b200_last_error_message().decode()
     assert_parity(d_out.cpu().numpy(), ref_second, what="second half after the bad index")
 
