@@ -15,15 +15,14 @@ timed steps are read after the last one, and the synchronous call's step time
 is reported beside it (config.sync_call_ms_per_step).  The class
 enumeration is measured apart, and so is a cold step (caches dropped: tables,
 plan and graph built again inside the timed call).  The metric compares the
-two forms: `value` is the chosen form (--form; the default, auto, takes the
-mixed form where it runs a stage on the tensor cores and FP64 where the mixed
-form keeps every stage in FP64, as at ERI 7^3); the other form
+two forms: `value` is the chosen form (--form, default fp64: the drop-in, whose
+values match the reference's own at its tol); the other form
 is timed the same way beside it, and the mixed form's max abs error against
 the FP64 form (and both against the reference C core on a seeded sample) is
 reported in Hartree.  `dtype` names the arithmetic that ran, per stage, as the
 library reports it (gli_b200_last_paths).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form auto|mixed|fp64] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|mixed] [--impl ours|reference]
 
 Timing: W >= 3 untimed warm-up steps; each timed step is bracketed by CUDA
 events on the stream the library launches on; L2 (126 MB) is flushed by
@@ -257,7 +256,7 @@ def run_ours(args):
     L.gli_b200_set_device(local)
     FORMS = {"fp64": _abi.GLI_FORM_FP64, "mixed": _abi.GLI_FORM_MIXED}
     KIND_ID = _abi.GLI_KIND_ERI if KIND == "eri" else _abi.GLI_KIND_ERIDA
-    chosen = "mixed" if args.form == "auto" else args.form
+    chosen = args.form
     other = "fp64" if chosen == "mixed" else "mixed"
     b = np.ascontiguousarray(g10())
     spec = grid_spec()
@@ -313,21 +312,16 @@ def run_ours(args):
         return 0
 
     log(f"{m} classes; accuracy check")
-    vals, ran = {}, {}
+    vals, screening = {}, {}
     for name, f in FORMS.items():
         step(f)
         stream.synchronize()
         vals[name] = out.cpu().numpy().copy()
-        p3 = (C.c_int * 3)()
-        L.gli_b200_last_paths(p3)
-        ran[name] = tuple(int(x) for x in p3)
+        scr = (C.c_double * 2)()
+        L.gli_b200_last_screening(scr)
+        screening[name] = {"product_threshold": scr[0], "bound_grid_units": scr[1]}
     scale = 1.0 / SPACING  # grid units -> Hartree at this spacing
     max_abs_err_ha = float(np.max(np.abs(vals["mixed"] - vals["fp64"])) * scale)
-    if args.form == "auto" and not (ran["mixed"][0] or ran["mixed"][1]):
-        # the mixed form keeps every stage of this workload in FP64 (its
-        # tensor-core stages do not pay at these sizes): the FP64 form leads
-        chosen, other = "fp64", "mixed"
-        log("the mixed form runs no tensor-core stage here: FP64 form reported")
 
     def timed_forms(steps, queued=True):
         """Both forms timed under the same conditions: after warm-up, their
@@ -424,7 +418,7 @@ def run_ours(args):
     stage = {}
     for name, f in FORMS.items():
         L.gli_b200_set_timing(1)
-        for _ in range(2):
+        for _ in range(3):  # (the third replay of the timed graph reuses its plan, as the timed steps do)
             step(f)
             stream.synchronize()
         ms4 = (C.c_float * 4)()
@@ -435,7 +429,7 @@ def run_ours(args):
         L.gli_b200_last_plan(plan4)
         stage[name] = {"tables": float(ms4[0]), "A": float(ms4[1]), "B": float(ms4[2]), "C": float(ms4[3]),
                        "sizes": (int(sz3[0]), int(sz3[1]), int(sz3[2])), "plan": tuple(int(x) for x in plan4)}
-    nA, nP, U = stage["fp64"]["sizes"]
+    nA, nP, U = stage[chosen]["sizes"]
     peak = C.c_double()
     L.gli_b200_measure_fp64_peak(C.byref(peak))
 
@@ -492,6 +486,7 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "classes": m, "form": chosen, "tol": TOL, "spacing_bohr": SPACING,
                    "l2": "flushed between timed steps (1 GB write)",
                    "max_abs_err_ha_mixed_vs_fp64": max_abs_err_ha,
+                   "screening": screening,
                    "forms": {chosen: {"classes_per_s": main["value"], "ms_per_step": main["ms_per_step"]},
                              other: {"classes_per_s": side["value"], "ms_per_step": side["ms_per_step"]}},
                    "step_call": "gli_b200_sparse_values_dev_async (stream-ordered; statuses read after the timed "
@@ -503,10 +498,11 @@ def run_ours(args):
                    "cold_step_ms": cold,
                    "stage_paths": {k: {"A": "s8 tcgen05" if v[0] else "f64 dmma",
                                        "B": "s8 tcgen05" if v[1] else "f64 dmma",
-                                       "C": "f64 product gemm + gather" if v[2] else "f64 per-class dots"}
+                                       "C": ("f64 product gemm + " + GATHERS[v[2]]) if v[2] else "f64 per-class dots"}
                                    for k, v in paths.items()},
                    "stage_ms": {k: {s_: v[s_] for s_ in ("tables", "A", "B", "C")} for k, v in stage.items()},
-                   "stage_sizes": {"keys_A": nA, "key_pairs": nP, "lattice_U": U},
+                   "stage_sizes": {k: {"keys_A": v["sizes"][0], "key_pairs": v["sizes"][1], "lattice_U": v["sizes"][2]}
+                                   for k, v in stage.items()},
                    "wall_s_timed_region": main["wall_s"]},
         "roofline": roof,
         "e2e": {"value": m / e2e_s, "unit": "classes/s", "h2d_bytes_per_step": 8 * m + 8 * b.size,
@@ -851,6 +847,10 @@ def run_surrogate(args):
     return 0
 
 
+# the class gather of a product-form stage C (gli_b200_last_paths out[2])
+GATHERS = {1: "k_gather_q", 2: "k_gather_q_plan"}
+
+
 def dtype_label(paths):
     """The arithmetic of an evaluation from the library's per-stage report:
     f64 unless a stage ran as int8-sliced products on the tensor cores."""
@@ -893,7 +893,7 @@ def roofline(paths, dom, st, plan, U, m, fp64_peak):
         achieved = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
         mp = measured_peaks()
         peak = mp["hbm_gbs"]
-        return {"bound": "hbm", "stage": dom, "kernel": "k_gather_q (+ k_dmma<ProductOp> in the stage time)",
+        return {"bound": "hbm", "stage": dom, "kernel": f"{GATHERS[paths[2]]} (+ k_dmma<ProductOp> in the stage time)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved and peak else None,
                 "peak_source": peak_source(mp),
@@ -956,8 +956,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--form", choices=["auto", "fp64", "mixed"], default="auto",
-                    help="auto: the mixed form where it runs a stage on the tensor cores, else FP64")
+    ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64",
+                    help="the form of the line's value (the other is timed beside it)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shard", action="store_true",
@@ -976,8 +976,6 @@ def main():
         L_GRID, SPACING, WORKLOAD, KIND = WORKLOADS[args.workload]
     if args.cpu_baseline_json:
         return cpu_baseline_main(args.cpu_baseline_json)
-    if args.form == "auto" and (args.workload not in WORKLOADS or args.shard or args.profile_only):
-        args.form = "mixed"  # (the choice between the forms is made in the sparse-value line only)
     if args.workload == "nuclear-batch":
         return run_nuclear_batch(args)
     if args.workload == "kinetic24":

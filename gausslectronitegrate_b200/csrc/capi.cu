@@ -314,7 +314,14 @@ int gli_b200_last_paths(int out[3]) {
     const gli::ContractStats& st = gli::last_stats();
     out[0] = st.tc_a;
     out[1] = st.tc_b;
-    out[2] = st.product ? 1 : 0;
+    out[2] = st.product ? (st.gather ? st.gather : 1) : 0;
+    return GLI_OK;
+}
+
+int gli_b200_last_screening(double out[2]) {
+    const gli::ContractStats& st = gli::last_stats();
+    out[0] = st.screen_tol;
+    out[1] = st.screen_bound;
     return GLI_OK;
 }
 

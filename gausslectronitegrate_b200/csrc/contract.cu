@@ -1565,25 +1565,34 @@ void dgemm_prepare();  // dense.cu: attributes of the strided FP64 GEMM
 static thread_local bool t_timing = false;
 static thread_local ContractStats t_last;
 static thread_local int t_paths = 0;  // tensor-core stages of the evaluation being completed
+// product threshold of the evaluation being completed and its screening bound
+static thread_local double t_screen_tol = 0.0, t_screen_bound = 0.0;
+// the stage marks of the timed graph the evaluation being completed replayed
+static thread_local struct StageTimer* t_graph_timer = nullptr;
 
 void set_timing(bool on) { t_timing = on; }
 const ContractStats& last_stats() { return t_last; }
 
+// (external: the marks are recorded inside a graph capture, as event record
+// nodes of the graph, so that every replay of the graph records them)
 struct StageTimer {
     static constexpr int kMax = 8;
     bool on;
     cudaStream_t s;
+    bool external;
     cudaEvent_t ev[kMax];
     int n = 0;
-    StageTimer(bool enabled, cudaStream_t st) : on(enabled), s(st) {
+    StageTimer(bool enabled, cudaStream_t st, bool in_graph = false) : on(enabled), s(st), external(in_graph) {
         if (on)
             for (auto& e : ev) GLI_CUDA(cudaEventCreate(&e));
     }
     void mark() {
         if (!on) return;
         if (n >= kMax) fail(GLI_ERR_INTERNAL, "stage timer overflow");
-        GLI_CUDA(cudaEventRecord(ev[n++], s));
+        GLI_CUDA(external ? cudaEventRecordWithFlags(ev[n++], s, cudaEventRecordExternal) : cudaEventRecord(ev[n++], s));
     }
+    StageTimer(const StageTimer&) = delete;
+    StageTimer& operator=(const StageTimer&) = delete;
     ~StageTimer() {
         if (on)
             for (auto& e : ev) cudaEventDestroy(e);
@@ -1641,7 +1650,8 @@ static i64 tc_a_outputs() {
 }
 
 // the tensor-core stages of the last evaluation queued by this thread (bit 0:
-// stage A, bit 1: stage B)
+// stage A, bit 1: stage B) and its class gather (bits 2-3: 1 k_gather_q, 2
+// k_gather_q_plan; 0 none, the per-class stage C)
 static thread_local int t_enq_paths = 0;
 
 // Stage B on the tensor cores slices every row of the expanded Hf (nA U^2
@@ -2049,6 +2059,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         // (fused: the plan's own pair bitmap, since this replay's stays empty
         // when the mark pass skipped)
         const uint32_t* saved = fused ? (const uint32_t*)pstore->saved_bits.p : nullptr;
+        t_enq_paths |= (fused ? 2 : 1) << 2;  // the class gather that ran
         if (fused && dec.pd)
             launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
                           saved, pairPre.p, (int)nku, cnt, a.out);
@@ -2091,7 +2102,11 @@ struct GraphEntry {
     long long launches = 0;  // kernels in the graph
     PlanMode mode = PLAN_BOUNDED;
     EvalSizes sz;            // the sizes a PLAN_SIZED graph was captured with
-    std::unique_ptr<PlanStore> plan;  // a PLAN_SIZED graph's plan, kept between replays
+    std::unique_ptr<PlanStore> plan;  // the graph's plan, kept between replays
+    // timed graphs (evaluations while stage timing is on): the stage marks
+    // recorded by every replay, before stage A and after stages A, B and C
+    bool timed = false;
+    std::unique_ptr<StageTimer> timer;
     int paths = 0;           // tensor-core stages of the captured evaluation
     DevMem<EvalStatus> status;
     ~GraphEntry() {
@@ -2103,10 +2118,11 @@ static thread_local std::list<std::unique_ptr<GraphEntry>> t_graphs;
 static constexpr size_t kGraphEntries = 8;
 static const bool g_graphs_enabled = getenv("GLI_B200_NO_GRAPHS") == nullptr;
 
-static GraphEntry* find_graph(const EvalArgs& a, int device) {
+static GraphEntry* find_graph(const EvalArgs& a, int device, bool timed) {
     for (auto it = t_graphs.begin(); it != t_graphs.end(); ++it) {
         GraphEntry& e = **it;
-        if (e.tables == a.t && e.device == device && e.mixed == (int)a.mixed && e.idx == a.idx && e.out == a.out &&
+        if (e.tables == a.t && e.device == device && e.timed == timed && e.mixed == (int)a.mixed && e.idx == a.idx &&
+            e.out == a.out &&
             e.m == a.m && e.istart[0] == a.d.istart[0] && e.istart[1] == a.d.istart[1] &&
             e.istart[2] == a.d.istart[2] && e.num[0] == a.d.num[0] && e.num[1] == a.d.num[1] &&
             e.num[2] == a.d.num[2]) {
@@ -2128,8 +2144,10 @@ static void drop_graph(const GraphEntry* e) {
 }
 
 static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const LatticeTables>& tp, int device,
-                                 cudaStream_t s, PlanMode mode, const EvalSizes& sized) {
+                                 cudaStream_t s, PlanMode mode, const EvalSizes& sized, bool timed) {
     auto e = std::make_unique<GraphEntry>();
+    e->timed = timed;
+    if (timed) e->timer = std::make_unique<StageTimer>(true, s, true);
     e->mode = mode;
     e->sz = sized;
     e->tables = a.t;
@@ -2172,9 +2190,9 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     try {
-        StageTimer timer(false, s);
+        StageTimer untimed(false, s);
         EvalSizes sz = sized;
-        enqueue_eval(a, mode, e->status.p, timer, sz, s, e->plan.get());
+        enqueue_eval(a, mode, e->status.p, timed ? *e->timer : untimed, sz, s, e->plan.get());
     } catch (...) {
         cudaStreamEndCapture(s, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -2226,7 +2244,14 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
     const Context& ctx = context();
     timer.mark();
-    tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), tol, s);
+    // the mixed form screens the products within its error budget
+    // (mixed_screen_tol: a first-order bound of MIXED_SCREEN_BOUND grid units)
+    double screen_bound = 0.0;
+    const double ttol = form == FORM_MIXED ? mixed_screen_tol(kind, h_coeffs, nb, g.max_range(), tol, &screen_bound, s)
+                                           : tol;
+    t_screen_tol = ttol;
+    t_screen_bound = screen_bound;
+    tp = lattice_tables(kind, h_coeffs, nb, g.max_range(), ttol, s);
     const LatticeTables& t = *tp;
     EvalArgs a;
     a.mixed = form == FORM_MIXED;
@@ -2256,9 +2281,11 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     a.out = d_out;
     a.num_sms = ctx.num_sms;
     const bool bounded = t.nkeys <= BOUNDED_KEYS;
-    const bool graphs = !t_timing && g_graphs_enabled;
-    GraphEntry* e = graphs && (bounded || sized_plan_fits(t.nkeys)) ? find_graph(a, ctx.device) : nullptr;
-    if (!e && graphs && bounded) e = capture_graph(a, tp, ctx.device, s, PLAN_BOUNDED, EvalSizes{});
+    const bool graphs = g_graphs_enabled;
+    // (stage timing replays graphs of its own, whose stage marks are nodes)
+    GraphEntry* e = graphs && (bounded || sized_plan_fits(t.nkeys)) ? find_graph(a, ctx.device, t_timing) : nullptr;
+    if (!e && graphs && bounded) e = capture_graph(a, tp, ctx.device, s, PLAN_BOUNDED, EvalSizes{}, t_timing);
+    t_graph_timer = e ? e->timer.get() : nullptr;
     if (e) {
         GLI_CUDA(cudaGraphLaunch(e->exec, s));
         add_launches(e->launches);
@@ -2273,7 +2300,7 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     t_paths = t_enq_paths;
     GLI_CUDA(cudaMemcpyAsync(h_status, st.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
     // the exact counts of this list size the graph that its next evaluations replay
-    if (graphs && !bounded && sized_plan_fits(t.nkeys)) capture_graph(a, tp, ctx.device, s, PLAN_SIZED, sz);
+    if (graphs && !bounded && sized_plan_fits(t.nkeys)) capture_graph(a, tp, ctx.device, s, PLAN_SIZED, sz, t_timing);
 }
 
 // debug builds: a device bounds check that failed during the evaluation
@@ -2305,11 +2332,17 @@ static void check_status(int kind, i64 m, const EvalStatus& h, const LatticeTabl
     st.products = st.product ? (i64)h.products : 0;
     st.tc_a = t_paths & 1;
     st.tc_b = (t_paths >> 1) & 1;
+    st.gather = (t_paths >> 2) & 3;
+    st.screen_tol = t_screen_tol;
+    st.screen_bound = t_screen_bound;
     if (t_timing) {
         st.ms_tables = timer.between(0, 1);
-        st.ms_a = timer.between(2, 3);
-        st.ms_b = timer.between(3, 4);
-        st.ms_c = timer.between(4, 5);
+        // a replayed graph's own marks, else those of the uncaptured evaluation
+        StageTimer& g = t_graph_timer ? *t_graph_timer : timer;
+        const int b = t_graph_timer ? 0 : 2;
+        st.ms_a = g.between(b, b + 1);
+        st.ms_b = g.between(b + 1, b + 2);
+        st.ms_c = g.between(b + 2, b + 3);
     }
     t_last = st;
     if (stats) *stats = st;

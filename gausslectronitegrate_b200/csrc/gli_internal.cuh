@@ -162,6 +162,10 @@ struct ContractStats {
     int product = 0;    // stage C ran as the (pair, key) product GEMM
     i64 products = 0;   // ... and computed this many (pair, key) products
     int tc_a = 0, tc_b = 0;  // stage A / B ran as int8-sliced products on the tcgen05 tensor cores
+    int gather = 0;          // the class gather of a product-form stage C: 1 packed keys, 2 decoding
+                             // and checking against a kept plan
+    double screen_tol = 0;    // the product threshold the tables were built with (mixed form: screened)
+    double screen_bound = 0;  // bound on the change of a class value by that screening (grid units)
     float ms_tables = 0, ms_a = 0, ms_b = 0, ms_c = 0;
 };
 

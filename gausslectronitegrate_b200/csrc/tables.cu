@@ -18,7 +18,9 @@
 //   positions u >= 0 and T is read at u^2 + v^2 + t^2.
 #include <math.h>
 
+#include <algorithm>
 #include <list>
+#include <vector>
 #include <mutex>
 
 #include "tables.cuh"
@@ -258,6 +260,90 @@ std::shared_ptr<const LatticeTables> lattice_tables(int kind, const double* h_co
     g_cache.push_front(CacheEntry{kind, device, L, tol, std::move(c), t});
     while (g_cache.size() > kCacheEntries) g_cache.pop_back();
     return t;
+}
+
+namespace {
+struct ScreenEntry {
+    int kind, device;
+    i64 L;
+    double tol, tau, bound;
+    std::vector<double> coeffs;
+};
+std::list<ScreenEntry> g_screen;  // (guarded by g_cache_mu)
+}  // namespace
+
+double mixed_screen_tol(int kind, const double* h_coeffs, i64 nb, i64 L, double tol, double* bound, cudaStream_t s) {
+    if (nb <= 0 || nb % 2 != 1) fail(GLI_ERR_ARGUMENT, "gausslet coefficient count must be odd, got %lld", (long long)nb);
+    if (nb > 4096) fail(GLI_ERR_LIMIT, "gausslet coefficient count %lld exceeds 4096", (long long)nb);
+    int device = 0;
+    GLI_CUDA(cudaGetDevice(&device));
+    std::vector<double> c(h_coeffs, h_coeffs + nb);
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        for (const ScreenEntry& e : g_screen)
+            if (e.kind == kind && e.device == device && e.L == L && e.tol == tol && e.coeffs == c) {
+                *bound = e.bound;
+                return e.tau;
+            }
+    }
+    // the product vectors without a mask (the same kernels as the tables)
+    DevBuf<double> b(nb, s);
+    GLI_CUDA(cudaMemcpyAsync(b.p, h_coeffs, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    DevBuf<int> maxabs(1, s);
+    GLI_CUDA(cudaMemsetAsync(maxabs.p, 0xff, sizeof(int), s));
+    i64 npairs = 1, xl = 2 * nb - 1;
+    DevBuf<double> prod;
+    if (kind == 0) {
+        prod.alloc(xl, s);
+        k_erida_products<<<(unsigned)((xl + 127) / 128), 128, 0, s>>>(b.p, (int)nb, 0.0, prod.p, maxabs.p);
+        GLI_CHECK_LAUNCH();
+    } else {
+        const i64 nf = 2 * nb - 1;
+        xl = 4 * nb - 3;
+        npairs = L * (L + 1) / 2;
+        DevBuf<double> F(L * nf, s);
+        k_factors<<<dim3((unsigned)((nf + 127) / 128), (unsigned)L), 128, 0, s>>>(b.p, (int)nb, (int)L, F.p);
+        GLI_CHECK_LAUNCH();
+        prod.alloc(npairs * xl, s);
+        k_eri_products<<<dim3((unsigned)((xl + 127) / 128), (unsigned)npairs), 128, 0, s>>>(F.p, (int)nb, 0.0, prod.p,
+                                                                                              maxabs.p);
+        GLI_CHECK_LAUNCH();
+    }
+    std::vector<double> P((size_t)(npairs * xl));
+    GLI_CUDA(cudaMemcpyAsync(P.data(), prod.p, P.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GLI_CUDA(cudaStreamSynchronize(s));
+    // candidates tau = 10^(-16 + k/4) up to 1e-4, the largest whose bound holds
+    const double T0 = kind ? 2.3936536824085962 : 1.6925687506432689;  // T(0), as k_coulomb_table
+    double S = 0.0;
+    for (i64 p = 0; p < npairs; ++p) {
+        double l1 = 0.0;
+        for (i64 x = 0; x < xl; ++x)
+            if (fabs(P[p * xl + x]) > tol) l1 += fabs(P[p * xl + x]);
+        S = std::max(S, l1);
+    }
+    double tau = tol, tau_bound = 0.0;
+    for (int k = 0; k <= 48; ++k) {
+        const double cand = pow(10.0, -16.0 + 0.25 * k);
+        if (cand <= tol) continue;
+        double D = 0.0;
+        for (i64 p = 0; p < npairs; ++p) {
+            double d = 0.0;
+            for (i64 x = 0; x < xl; ++x) {
+                const double a = fabs(P[p * xl + x]);
+                if (a > tol && a <= cand) d += a;
+            }
+            D = std::max(D, d);
+        }
+        const double bnd = 3.0 * T0 * D * S * S;
+        if (bnd > MIXED_SCREEN_BOUND) break;
+        tau = cand;
+        tau_bound = bnd;
+    }
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_screen.push_front(ScreenEntry{kind, device, L, tol, tau, tau_bound, std::move(c)});
+    while (g_screen.size() > kCacheEntries) g_screen.pop_back();
+    *bound = tau_bound;
+    return tau;
 }
 
 }  // namespace gli

@@ -62,6 +62,17 @@ struct LatticeTables {
 std::shared_ptr<const LatticeTables> lattice_tables(int kind, const double* h_coeffs, i64 nb, i64 L, double tol,
                                                     cudaStream_t s);
 
+// Screening of the mixed form: the largest threshold tau >= tol at which
+// dropping the product entries tol < |P| <= tau changes no class value by
+// more than MIXED_SCREEN_BOUND grid units, by the first-order bound
+//   |dV| <= 3 T(0) D S^2,  D = max_p sum_{tol<|P_p|<=tau} |P_p|,  S = max_p sum_{|P_p|>tol} |P_p|
+// (a class value is sum W_x W_y W_z T over the lattice, each folded weight
+// row W takes every entry of its product vector at most once, and 0 < T <=
+// T(0)).  *bound receives the bound at the returned tau (0 when tau = tol).
+// Cached per (kind, coefficients, L, tol, device).
+constexpr double MIXED_SCREEN_BOUND = 1e-9;
+double mixed_screen_tol(int kind, const double* h_coeffs, i64 nb, i64 L, double tol, double* bound, cudaStream_t s);
+
 // dense ERI key of one axis: shift pair (|s01|, |s23|) unordered and |c|/3
 __host__ __device__ inline i64 eri_axis_key(i64 s01, i64 s23, i64 cc, i64 L) {
     i64 a = s01 < 0 ? -s01 : s01;

@@ -439,9 +439,19 @@ int gli_b200_last_plan(glong out[4]);
 /* Arithmetic of the calling thread's last sparse evaluation, per stage:
  * out[0] stage A, out[1] stage B: 1 when the stage ran as int8-sliced products
  * on the tcgen05 tensor cores, 0 when it ran on the FP64 tensor-core GEMM;
- * out[2] stage C: 1 for the (pair, key) product GEMM plus the class gather, 0
- * for the per-class FP64 dot products.  No reference counterpart. */
+ * out[2] stage C: 0 for the per-class FP64 dot products, else the (pair, key)
+ * product GEMM plus a class gather: 1 through the classes' packed keys, 2
+ * decoding and checking each class against a plan kept from an earlier
+ * evaluation of the list.  No reference counterpart. */
 int gli_b200_last_paths(int out[3]);
+
+/* Screening of the calling thread's last sparse evaluation: out[0] the
+ * threshold its Gaussian-pair products were masked at (the caller's tol for
+ * the FP64 form; the mixed form raises it within its error budget), out[1] a
+ * bound on how much that changes any class value against masking at the
+ * caller's tol, in grid units (0 when the threshold is the caller's).  No
+ * reference counterpart. */
+int gli_b200_last_screening(double out[2]);
 
 /* Drops the calling thread's captured evaluation graphs and every cached
  * lattice-table set, so that the next evaluation builds its tables and plans

@@ -1,7 +1,9 @@
 """The mixed form of the sparse ERI/ERIDA evaluation (form="mixed").
 
-The two bulk lattice stages run as int8-sliced products on the tcgen05 tensor
-cores; tables and the last stage stay FP64.  Its bar is an absolute error of at
+It screens the Gaussian-pair products within a first-order error bound
+(gli_b200_last_screening), and the two bulk lattice stages run as int8-sliced
+products on the tcgen05 tensor cores where they are large enough; tables and
+the last stage stay FP64.  Its bar is an absolute error of at
 most 1e-8 Ha on every class value.  Values are in grid units (spacing 1); an
 integral on a grid of spacing h is the grid-unit value / h, so the strictest
 workload in use (spacing 0.5 bohr) needs a grid-unit error below 5e-9, the
@@ -75,6 +77,30 @@ def test_mixed_erida_129_against_fp64_form(gli):
     fp = gli.compute_sparse_erida_gausslet_integrals(g10(), sym_grid(129), 1e-10)
     mx = gli.compute_sparse_erida_gausslet_integrals(g10(), sym_grid(129), 1e-10, form="mixed")
     _check(mx.values, fp.values, "mixed ERIDA 129^3 tol 1e-10")
+
+
+@pytest.mark.parametrize("kind,L", [("eri", 7), ("erida", 33)])
+def test_mixed_screening_within_its_bound(gli, kind, L):
+    # at tol 1e-16 the mixed form masks the products at a higher threshold;
+    # without a tensor-core stage (neither of these sizes has one) the
+    # screening is its only departure from the FP64 form, and every class
+    # value stays within the stated bound
+    fn = gli.compute_sparse_eri_gausslet_integrals if kind == "eri" else gli.compute_sparse_erida_gausslet_integrals
+    fp = fn(g10(), sym_grid(L), 1e-16)
+    mx = fn(g10(), sym_grid(L), 1e-16, form="mixed")
+    scr = (C.c_double * 2)()
+    gli.lib().gli_b200_last_screening(scr)
+    paths = (C.c_int * 3)()
+    gli.lib().gli_b200_last_paths(paths)
+    tau, bound = scr[0], scr[1]
+    assert 1e-16 < tau and 0 < bound <= 1e-9
+    assert paths[0] == 0 and paths[1] == 0
+    err = float(np.max(np.abs(mx.values - fp.values)))
+    assert err <= bound, f"{kind} {L}^3: screening error {err:.3e} above its bound {bound:.3e} (tau {tau:.1e})"
+    # the FP64 form masks at the caller's tol
+    fn(g10(), sym_grid(L), 1e-16)
+    gli.lib().gli_b200_last_screening(scr)
+    assert scr[0] == 1e-16 and scr[1] == 0
 
 
 def test_mixed_arbitrary_eri_list(gli):
