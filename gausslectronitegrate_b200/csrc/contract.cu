@@ -1042,7 +1042,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
 // saves the mark pass's read of the indices and the write and re-read of the
 // packed keys (24 bytes per class).
 template <bool PD>
-__global__ void __launch_bounds__(256) k_gather_q_plan(const double* __restrict__ Q, int parts, i64 part_stride,
+__global__ void __launch_bounds__(256, 8) k_gather_q_plan(const double* __restrict__ Q, int parts, i64 part_stride,
                                                         ClassDecode dec, const int64_t* __restrict__ idx, i64 m,
                                                         const uint64_t* __restrict__ kid, int nk,
                                                         const uint32_t* __restrict__ pairBits,
@@ -1051,7 +1051,10 @@ __global__ void __launch_bounds__(256) k_gather_q_plan(const double* __restrict_
     if (cnt->overflow) return;
     const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)out & 15) == 0;
     const i64 groups = (m + 3) / 4, stride = (i64)gridDim.x * blockDim.x;
-    constexpr int G = 2;
+    // one group of four classes per thread and step, at most 32 registers:
+    // eight blocks per SM hide the dependent loads better than two groups
+    // at four blocks (ERI 7^3 stage C 45 against 49 us)
+    constexpr int G = 1;
     bool miss = false;
     for (i64 g0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; g0 < groups; g0 += G * stride) {
         int64_t c[G][4];
@@ -1542,6 +1545,29 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
     }
 }
 
+// The first kernel of a replay that trusts its kept plan (the host has seen an
+// earlier replay of the graph complete): the plan's counts, or, should no
+// valid plan be kept, an overflow (the host then evaluates anew).  Such a
+// replay launches neither the mark pass nor the plan kernel; its class gather
+// checks every class against the kept plan (k_gather_q_plan).
+__global__ void k_restore_plan(PlanReuse reuse, PlanCounts* __restrict__ cnt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (*reuse.valid) {
+        const PlanCounts c = *reuse.saved_cnt;
+        cnt->key_total = c.key_total;
+        cnt->nku = c.nku;
+        cnt->nA = c.nA;
+        cnt->nP = c.nP;
+        cnt->overflow = 0;
+    } else {
+        cnt->key_total = 0;
+        cnt->nku = 0;
+        cnt->nA = 0;
+        cnt->nP = 0;
+        cnt->overflow = 1;
+    }
+}
+
 // G sliced once per table set (cached with the tables); the build synchronises
 // the stream so that the slices are ready for any stream that uses them later
 static TiledOperand lattice_g_slices(const LatticeTables& t, cudaStream_t s) {
@@ -1749,8 +1775,11 @@ struct StageBufs {
 // Queues one evaluation on stream s.  Kernels read the counts from st->cnt;
 // the host sizes buffers and grids by `sz` (an input for PLAN_SIZED, an output
 // otherwise).
+// trusted: a replay that launches neither the mark pass nor the plan (the
+// plan kept in pstore stands; k_restore_plan): for evaluations whose class
+// gather checks every class (product form, kept plan).
 static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
-                         cudaStream_t s, PlanStore* pstore = nullptr) {
+                         cudaStream_t s, PlanStore* pstore = nullptr, bool trusted = false) {
     const bool bounded = mode == PLAN_BOUNDED;
     const LatticeTables& t = *a.t;
     const i64 nk = t.nkeys, m = a.m;
@@ -1771,9 +1800,13 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     // usedKey and usedA side by side so that one scan serves both; pair flags
     // over all key pairs (slot k2 * nk + k1)
     const i64 words = (nk * nk + 31) / 32;
-    DevBuf<uint32_t> used(2 * nk, s), pairBits(words, s);
-    used.zero();
-    pairBits.zero();
+    DevBuf<uint32_t> used, pairBits;
+    if (!trusted) {
+        used.alloc(2 * nk, s);
+        pairBits.alloc(words, s);
+        used.zero();
+        pairBits.zero();
+    }
     const unsigned cb = (unsigned)((m + 255) / 256);
     const unsigned kb = (unsigned)((nk + 255) / 256);
     DevBuf<short4> pts;
@@ -1800,6 +1833,8 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     // gather decodes and checks every class (the list may have been rewritten
     // in place since the plan was made).
     const bool fused = pstore && mode != PLAN_EXACT && product_pays((double)sz.nP, (double)sz.nku, m);
+    if (trusted && !(fused && pstore->pd.p == dec.pd))
+        fail(GLI_ERR_INTERNAL, "a trusted replay needs a kept plan and the product form");
     // packed key triple per class, written by the decode pass and read by the
     // gather (decoding a class twice, in the mark pass and again in the gather,
     // measured slower than re-reading its 8 bytes: ERI 7^3 stage C 52 against
@@ -1855,11 +1890,11 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     };
     if (known) stage_bufs();
 
-    if (dec.pd)
+    if (dec.pd && !trusted)
         launch_kernel(k_pair_desc, dim3((unsigned)((dec.N2 + 255) / 256)), dim3(256), 0, s, dec, pdesc.p, pd_skip);
-    else if (dec.kind == 1)
+    else if (!dec.pd && dec.kind == 1)
         launch_kernel(k_point_table, dim3((unsigned)((dec.N + 255) / 256)), dim3(256), 0, s, dec, pts.p);
-    {
+    if (!trusted) {
         const size_t lb = mark_local_bytes(nk);
         if (dec.pd) {
             const i64 groups = (m + 3) / 4;
@@ -1872,7 +1907,10 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                           lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
         }
     }
-    if (plan_small) {
+    if (plan_small && trusted) {
+        launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), cnt);
+        tiles.built = true;
+    } else if (plan_small) {
         launch_kernel(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
                    pairBits.p, pairPre.p, pairA.p, pairB.p, tiles.bn, (int)tiles.max_tiles, tiles.first, tiles.tile0,
                    tiles.batch, tiles.col0, tiles.ncols, tiles.rowPair, tiles.rowKey, cnt,
@@ -2100,17 +2138,24 @@ struct GraphEntry {
     i64 istart[3] = {}, num[3] = {};
     cudaGraphExec_t exec = nullptr;
     long long launches = 0;  // kernels in the graph
+    // the trusted variant (no mark pass, no plan kernel; k_restore_plan), for
+    // product-form evaluations, replayed once the host has seen a replay of
+    // `exec` complete (planned), which leaves a valid plan kept
+    cudaGraphExec_t exec_trust = nullptr;
+    long long launches_trust = 0;
+    bool planned = false;
     PlanMode mode = PLAN_BOUNDED;
     EvalSizes sz;            // the sizes a PLAN_SIZED graph was captured with
     std::unique_ptr<PlanStore> plan;  // the graph's plan, kept between replays
     // timed graphs (evaluations while stage timing is on): the stage marks
     // recorded by every replay, before stage A and after stages A, B and C
     bool timed = false;
-    std::unique_ptr<StageTimer> timer;
+    std::unique_ptr<StageTimer> timer, timer_trust;
     int paths = 0;           // tensor-core stages of the captured evaluation
     DevMem<EvalStatus> status;
     ~GraphEntry() {
         if (exec) cudaGraphExecDestroy(exec);
+        if (exec_trust) cudaGraphExecDestroy(exec_trust);
     }
 };
 
@@ -2134,6 +2179,17 @@ static GraphEntry* find_graph(const EvalArgs& a, int device, bool timed) {
 }
 
 void clear_eval_caches() { t_graphs.clear(); }
+
+// a replay of the graph completed without overflow: its plan is kept and
+// valid, and later replays may trust it (e may have been dropped since: it is
+// looked up, not dereferenced)
+static void graph_replayed(const GraphEntry* e) {
+    for (auto& g : t_graphs)
+        if (g.get() == e) {
+            g->planned = true;
+            return;
+        }
+}
 
 static void drop_graph(const GraphEntry* e) {
     for (auto it = t_graphs.begin(); it != t_graphs.end(); ++it)
@@ -2186,25 +2242,39 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
         e->plan->alloc(nk, words, capA, capP, PairTiles::ints(capA, capP, 64, true),
                        pair_desc_applies(a.d) ? (i64)a.d.N2 : 0);
     }
-    const long long l0 = launch_count();
-    GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    cudaGraph_t graph = nullptr;
-    try {
-        StageTimer untimed(false, s);
-        EvalSizes sz = sized;
-        enqueue_eval(a, mode, e->status.p, timed ? *e->timer : untimed, sz, s, e->plan.get());
-    } catch (...) {
-        cudaStreamEndCapture(s, &graph);
-        if (graph) cudaGraphDestroy(graph);
-        cudaGetLastError();
-        throw;
-    }
-    GLI_CUDA(cudaStreamEndCapture(s, &graph));
-    e->launches = launch_count() - l0;
+    auto capture = [&](bool trusted, StageTimer* tm, cudaGraphExec_t* exec, long long* launches) {
+        const long long l0 = launch_count();
+        GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t graph = nullptr;
+        try {
+            StageTimer untimed(false, s);
+            EvalSizes sz = sized;
+            enqueue_eval(a, mode, e->status.p, tm ? *tm : untimed, sz, s, e->plan.get(), trusted);
+        } catch (...) {
+            cudaStreamEndCapture(s, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            throw;
+        }
+        GLI_CUDA(cudaStreamEndCapture(s, &graph));
+        *launches = launch_count() - l0;
+        const cudaError_t ie = cudaGraphInstantiate(exec, graph, 0);
+        cudaGraphDestroy(graph);
+        GLI_CUDA(ie);
+    };
+    capture(false, e->timer.get(), &e->exec, &e->launches);
     e->paths = t_enq_paths;
-    const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
-    cudaGraphDestroy(graph);
-    GLI_CUDA(ie);
+    // the product form (its gather checks every class against the kept plan)
+    // has a trusted variant
+    EvalSizes szb = sized;
+    if (mode == PLAN_BOUNDED) {
+        szb.nku = a.t->nkeys;
+        szb.nP = std::min(a.t->nkeys * (a.t->nkeys + 1) / 2, a.m);
+    }
+    if (product_pays((double)szb.nP, (double)szb.nku, a.m)) {
+        if (timed) e->timer_trust = std::make_unique<StageTimer>(true, s, true);
+        capture(true, e->timer_trust.get(), &e->exec_trust, &e->launches_trust);
+    }
     t_graphs.push_front(std::move(e));
     while (t_graphs.size() > kGraphEntries) t_graphs.pop_back();
     return t_graphs.front().get();
@@ -2285,10 +2355,11 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     // (stage timing replays graphs of its own, whose stage marks are nodes)
     GraphEntry* e = graphs && (bounded || sized_plan_fits(t.nkeys)) ? find_graph(a, ctx.device, t_timing) : nullptr;
     if (!e && graphs && bounded) e = capture_graph(a, tp, ctx.device, s, PLAN_BOUNDED, EvalSizes{}, t_timing);
-    t_graph_timer = e ? e->timer.get() : nullptr;
+    const bool trust = e && e->exec_trust && e->planned;
+    t_graph_timer = e ? (trust ? e->timer_trust.get() : e->timer.get()) : nullptr;
     if (e) {
-        GLI_CUDA(cudaGraphLaunch(e->exec, s));
-        add_launches(e->launches);
+        GLI_CUDA(cudaGraphLaunch(trust ? e->exec_trust : e->exec, s));
+        add_launches(trust ? e->launches_trust : e->launches);
         t_paths = e->paths;
         GLI_CUDA(cudaMemcpyAsync(h_status, e->status.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
         *sized = e;
@@ -2365,6 +2436,7 @@ void sparse_values_device(int kind, const double* h_coeffs, i64 nb, const GridDe
         GLI_CUDA(cudaStreamSynchronize(s));
     }
     check_status(kind, m, *h, *tp, timer, stats);
+    if (!h->cnt.overflow) graph_replayed(sized);
 }
 
 // Stream-ordered evaluations: queued without a host wait, their status read
@@ -2432,6 +2504,7 @@ static void finish_pending(PendingEval& e) {
     }
     StageTimer timer(false, e.s);
     check_status(e.kind, e.m, *e.h_status, *e.tp, timer, nullptr);
+    graph_replayed(e.sized);
 }
 
 void sparse_values_wait(i64 ticket) {
@@ -2587,6 +2660,7 @@ static void sparse_values_pinned(int kind, const double* h_coeffs, i64 nb, const
             drop_graph(sized[0]);  // the list outgrew its graph's sizes: once more, exactly
         }
         check_status(kind, m, *hs, *tp, timer, nullptr);
+        if (!hs->cnt.overflow) graph_replayed(sized[0]);
         return;
     }
     t_copy_streams.ensure(ctx.device);
@@ -2635,6 +2709,7 @@ static void sparse_values_pinned(int kind, const double* h_coeffs, i64 nb, const
             GLI_CUDA(cudaStreamSynchronize(s));
         }
         check_status(kind, n, hs[c], *tp, timer, nullptr);
+        if (!hs[c].cnt.overflow) graph_replayed(sized[c]);
     }
 }
 
@@ -2680,6 +2755,7 @@ void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc
         GLI_CUDA(cudaStreamSynchronize(s));
         if (redo_if_overflow()) return;
         check_status(kind, m, *hs, *tp, timer, nullptr);
+        graph_replayed(sized);
         host_copy(h_out, pin_val, (size_t)m * sizeof(double));
         return;
     }
@@ -2701,6 +2777,7 @@ void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc
     GLI_CUDA(cudaEventSynchronize(ev[0]));  // the status copy came before the values
     if (redo_if_overflow()) return;
     check_status(kind, m, *hs, *tp, timer, nullptr);
+    graph_replayed(sized);
     for (i64 c = 0; c < chunks; ++c) {
         const i64 b = c * per, n = std::min(m, b + per) - b;
         GLI_CUDA(cudaEventSynchronize(ev[c]));
