@@ -1399,8 +1399,12 @@ struct PlanStore {
     DevMem<PlanCounts> saved_cnt;
     DevMem<int> valid;
     DevMem<uint2> pd;  // the ERI pair descriptors, when the decode uses them
-    void alloc(i64 nk, i64 words, i64 capA, i64 capP, i64 tile_ints, i64 pairs) {
+    // the (pair, key) products of a product-form stage C, kept with the graph
+    // so that a class gather launched apart from it can read them
+    DevMem<double> Q;
+    void alloc(i64 nk, i64 words, i64 capA, i64 capP, i64 tile_ints, i64 pairs, i64 q_entries) {
         if (pairs > 0) pd.alloc((size_t)pairs);
+        if (q_entries > 0) Q.alloc((size_t)q_entries);
         ids.alloc((size_t)(2 * nk));
         pairPre.alloc((size_t)words);
         keyOf.alloc((size_t)nk);
@@ -1714,6 +1718,36 @@ enum PlanMode { PLAN_BOUNDED = 0, PLAN_EXACT = 1, PLAN_SIZED = 2 };
 // key spaces that the sized plan's single-block plan kernel holds
 static bool sized_plan_fits(i64 nk) { return nk <= PLAN_SMALL_KEYS && (nk * nk + 31) / 32 <= 8 * 1024; }
 
+// What a plan-checking class gather needs, for a gather launched apart from
+// the graph of its stages (the pipelined host-buffer path gathers the class
+// list range by range as it arrives): all of it lives with the graph (its
+// kept plan, its products Q, its status block).
+struct GatherLaunch {
+    const double* Q = nullptr;
+    int parts = 0;
+    i64 part_stride = 0;
+    ClassDecode dec;
+    const uint64_t* kid = nullptr;
+    int nk = 0;
+    const uint32_t* bits = nullptr;
+    const uint64_t* pre = nullptr;
+    int ldq = 0;
+    PlanCounts* cnt = nullptr;
+};
+
+// the plan-checking gather of classes idx[0, m) into out[0, m)
+static void launch_gather(const GatherLaunch& gl, const int64_t* idx, i64 m, double* out, int num_sms,
+                          cudaStream_t s) {
+    if (m <= 0) return;
+    const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)num_sms * 8);
+    if (gl.dec.pd)
+        launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, gl.Q, gl.parts, gl.part_stride, gl.dec, idx, m,
+                      gl.kid, gl.nk, gl.bits, gl.pre, gl.ldq, gl.cnt, out);
+    else
+        launch_kernel(k_gather_q_plan<false>, dim3(gq), dim3(256), 0, s, gl.Q, gl.parts, gl.part_stride, gl.dec, idx,
+                      m, gl.kid, gl.nk, gl.bits, gl.pre, gl.ldq, gl.cnt, out);
+}
+
 // the u split of the stage-C product: 64-column tiles (the product's grid is
 // small, and wider tiles cost it parallelism: ERIDA 129^3 73 us with 80
 // columns, 66 us with 64).  A grid under a wave (four blocks per SM; about half
@@ -1752,7 +1786,8 @@ struct StageBufs {
     DevBuf<unsigned> tickets;
     int q_parts = 0, u_chunk = 0;
     i64 tail = 0;
-    void alloc(const EvalArgs& a, const EvalSizes& sz, bool tc_a, bool product, cudaStream_t s) {
+    void alloc(const EvalArgs& a, const EvalSizes& sz, bool tc_a, bool product, cudaStream_t s,
+               const PlanStore* keep = nullptr) {
         const LatticeTables& t = *a.t;
         const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
         if (sz.nA * (i64)U * U > ((i64)1 << 31))
@@ -1761,7 +1796,11 @@ struct StageBufs {
         H2.alloc(sz.nP * (i64)Up, s);
         if (product) {
             q_parts = product_split(sz.nP, sz.nku, U, a.m, a.num_sms, &u_chunk);
-            Q.alloc(q_parts * sz.nP * sz.nku, s);
+            const i64 q = q_parts * sz.nP * sz.nku;
+            if (keep && keep->Q.p && keep->Q.n >= (size_t)q)
+                Q.borrow(keep->Q.p, q, s);  // a graph's own products, kept between its replays
+            else
+                Q.alloc(q, s);
         }
         tail = tc_a ? 0 : stage_a_tail(sz.nA, nS, U, a.num_sms);
         if (tail) {
@@ -1777,9 +1816,11 @@ struct StageBufs {
 // otherwise).
 // trusted: a replay that launches neither the mark pass nor the plan (the
 // plan kept in pstore stands; k_restore_plan): for evaluations whose class
-// gather checks every class (product form, kept plan).
+// gather checks every class (product form, kept plan).  split (trusted
+// only): the class gather is not launched; *split receives its arguments.
 static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, StageTimer& timer, EvalSizes& sz,
-                         cudaStream_t s, PlanStore* pstore = nullptr, bool trusted = false) {
+                         cudaStream_t s, PlanStore* pstore = nullptr, bool trusted = false,
+                         GatherLaunch* split = nullptr) {
     const bool bounded = mode == PLAN_BOUNDED;
     const LatticeTables& t = *a.t;
     const i64 nk = t.nkeys, m = a.m;
@@ -1835,6 +1876,8 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     const bool fused = pstore && mode != PLAN_EXACT && product_pays((double)sz.nP, (double)sz.nku, m);
     if (trusted && !(fused && pstore->pd.p == dec.pd))
         fail(GLI_ERR_INTERNAL, "a trusted replay needs a kept plan and the product form");
+    if (split && !(trusted && pstore->Q.p))
+        fail(GLI_ERR_INTERNAL, "a gather launched apart needs a trusted replay with kept products");
     // packed key triple per class, written by the decode pass and read by the
     // gather (decoding a class twice, in the mark pass and again in the gather,
     // measured slower than re-reading its 8 bytes: ERI 7^3 stage C 52 against
@@ -1886,7 +1929,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     auto stage_bufs = [&]() {
         const bool tc = a.mixed && sz.nA * (i64)nS >= tc_a_outputs();
         const bool prod = product_pays((double)sz.nP, (double)sz.nku, m) || (bounded && m >= 65536);
-        sb.alloc(a, sz, tc, prod, s);
+        sb.alloc(a, sz, tc, prod, s, pstore);
     };
     if (known) stage_bufs();
 
@@ -2093,20 +2136,30 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up, (int)nku,
                                   u_chunk, ps, Q.p, &st->products},
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
-        const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
-        // (fused: the plan's own pair bitmap, since this replay's stays empty
-        // when the mark pass skipped)
-        const uint32_t* saved = fused ? (const uint32_t*)pstore->saved_bits.p : nullptr;
         t_enq_paths |= (fused ? 2 : 1) << 2;  // the class gather that ran
-        if (fused && dec.pd)
-            launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p, (int)nk,
-                          saved, pairPre.p, (int)nku, cnt, a.out);
-        else if (fused)
-            launch_kernel(k_gather_q_plan<false>, dim3(gq), dim3(256), 0, s, Q.p, P, ps, dec, a.idx, m, ids.p,
-                          (int)nk, saved, pairPre.p, (int)nku, cnt, a.out);
-        else
+        if (fused) {
+            // (the plan's own pair bitmap: this replay's stays empty when the
+            // mark pass skipped)
+            GatherLaunch gl;
+            gl.Q = Q.p;
+            gl.parts = P;
+            gl.part_stride = ps;
+            gl.dec = dec;
+            gl.kid = ids.p;
+            gl.nk = (int)nk;
+            gl.bits = pstore->saved_bits.p;
+            gl.pre = pairPre.p;
+            gl.ldq = (int)nku;
+            gl.cnt = cnt;
+            if (split)
+                *split = gl;
+            else
+                launch_gather(gl, a.idx, m, a.out, a.num_sms, s);
+        } else {
+            const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
             launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
                           pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
+        }
     }
     if (undecided || !product_host) {
         const i64 want = (m + 7) / 8;
@@ -2144,6 +2197,11 @@ struct GraphEntry {
     cudaGraphExec_t exec_trust = nullptr;
     long long launches_trust = 0;
     bool planned = false;
+    // the trusted variant without its class gather, and the gather's launch
+    // (the pipelined host-buffer path gathers range by range)
+    cudaGraphExec_t exec_stages = nullptr;
+    long long launches_stages = 0;
+    GatherLaunch gather;
     PlanMode mode = PLAN_BOUNDED;
     EvalSizes sz;            // the sizes a PLAN_SIZED graph was captured with
     std::unique_ptr<PlanStore> plan;  // the graph's plan, kept between replays
@@ -2156,6 +2214,7 @@ struct GraphEntry {
     ~GraphEntry() {
         if (exec) cudaGraphExecDestroy(exec);
         if (exec_trust) cudaGraphExecDestroy(exec_trust);
+        if (exec_stages) cudaGraphExecDestroy(exec_stages);
     }
 };
 
@@ -2232,24 +2291,37 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageAOp<80>, true>();
     dmma_prepare<StageBOp<true>, true>();
     dmma_prepare<StageBOp<false>, true>();
-    {
-        // the plan kept between replays, with room for the sized counts or the
-        // bounds of a bounded plan
-        const i64 nk = a.t->nkeys, words = (nk * nk + 31) / 32;
-        const i64 capA = mode == PLAN_SIZED ? sized.nA : nk;
-        const i64 capP = mode == PLAN_SIZED ? sized.nP : std::min(nk * (nk + 1) / 2, a.m);
-        e->plan = std::make_unique<PlanStore>();
-        e->plan->alloc(nk, words, capA, capP, PairTiles::ints(capA, capP, 64, true),
-                       pair_desc_applies(a.d) ? (i64)a.d.N2 : 0);
+    // the sizes of the plan: the sized counts, or the bounds of a bounded plan
+    const i64 nk = a.t->nkeys;
+    EvalSizes szb = sized;
+    if (mode == PLAN_BOUNDED) {
+        szb.nA = nk;
+        szb.nku = nk;
+        szb.nP = std::min(nk * (nk + 1) / 2, a.m);
     }
-    auto capture = [&](bool trusted, StageTimer* tm, cudaGraphExec_t* exec, long long* launches) {
+    // the product form (its gather checks every class against the kept plan)
+    // has trusted variants, and keeps its products with the graph
+    const bool product = product_pays((double)szb.nP, (double)szb.nku, a.m);
+    {
+        const i64 words = (nk * nk + 31) / 32;
+        i64 q_entries = 0;
+        if (product) {
+            int u_chunk = 0;
+            q_entries = product_split(szb.nP, szb.nku, (int)a.t->U, a.m, a.num_sms, &u_chunk) * szb.nP * szb.nku;
+        }
+        e->plan = std::make_unique<PlanStore>();
+        e->plan->alloc(nk, words, szb.nA, szb.nP, PairTiles::ints(szb.nA, szb.nP, 64, true),
+                       pair_desc_applies(a.d) ? (i64)a.d.N2 : 0, q_entries);
+    }
+    auto capture = [&](bool trusted, StageTimer* tm, cudaGraphExec_t* exec, long long* launches,
+                       GatherLaunch* split) {
         const long long l0 = launch_count();
         GLI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         cudaGraph_t graph = nullptr;
         try {
             StageTimer untimed(false, s);
             EvalSizes sz = sized;
-            enqueue_eval(a, mode, e->status.p, tm ? *tm : untimed, sz, s, e->plan.get(), trusted);
+            enqueue_eval(a, mode, e->status.p, tm ? *tm : untimed, sz, s, e->plan.get(), trusted, split);
         } catch (...) {
             cudaStreamEndCapture(s, &graph);
             if (graph) cudaGraphDestroy(graph);
@@ -2262,18 +2334,13 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
         cudaGraphDestroy(graph);
         GLI_CUDA(ie);
     };
-    capture(false, e->timer.get(), &e->exec, &e->launches);
+    capture(false, e->timer.get(), &e->exec, &e->launches, nullptr);
     e->paths = t_enq_paths;
-    // the product form (its gather checks every class against the kept plan)
-    // has a trusted variant
-    EvalSizes szb = sized;
-    if (mode == PLAN_BOUNDED) {
-        szb.nku = a.t->nkeys;
-        szb.nP = std::min(a.t->nkeys * (a.t->nkeys + 1) / 2, a.m);
-    }
-    if (product_pays((double)szb.nP, (double)szb.nku, a.m)) {
+    if (product) {
         if (timed) e->timer_trust = std::make_unique<StageTimer>(true, s, true);
-        capture(true, e->timer_trust.get(), &e->exec_trust, &e->launches_trust);
+        capture(true, e->timer_trust.get(), &e->exec_trust, &e->launches_trust, nullptr);
+        // the stages alone, for the pipelined host-buffer path
+        if (!timed) capture(true, nullptr, &e->exec_stages, &e->launches_stages, &e->gather);
     }
     t_graphs.push_front(std::move(e));
     while (t_graphs.size() > kGraphEntries) t_graphs.pop_back();
@@ -2299,16 +2366,11 @@ struct PinnedBuf {
     }
 };
 
-// Queues one evaluation on stream s and an asynchronous copy of its status
-// block into h_status (pinned); the caller synchronises and checks it.
-// *sized receives the graph that was replayed (null otherwise): when its
-// status reports an overflow (a sized plan outgrown, or a class outside a
-// reused plan), the caller drops it and calls again, which plans anew.
-static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
-                                  const int64_t* d_indices, i64 m, double tol, int form, double* d_out, cudaStream_t s,
-                                  EvalStatus* h_status, std::shared_ptr<const LatticeTables>& tp, StageTimer& timer,
-                                  const GraphEntry** sized) {
-    *sized = nullptr;
+// The arguments of one evaluation: checks, the (cached) tables of its form and
+// the class decoder of its grid.  tp keeps the tables alive.
+static EvalArgs eval_args(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* d_indices,
+                          i64 m, double tol, int form, double* d_out, cudaStream_t s,
+                          std::shared_ptr<const LatticeTables>& tp, StageTimer& timer) {
     if (form != FORM_FP64 && form != FORM_MIXED)
         fail(GLI_ERR_ARGUMENT, "form %d is not a sparse evaluation form (0 = FP64, 1 = mixed)", form);
     if (!(tol >= 0)) fail(GLI_ERR_ARGUMENT, "tol must be non-negative");
@@ -2350,6 +2412,22 @@ static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, cons
     a.m = m;
     a.out = d_out;
     a.num_sms = ctx.num_sms;
+    return a;
+}
+
+// Queues one evaluation on stream s and an asynchronous copy of its status
+// block into h_status (pinned); the caller synchronises and checks it.
+// *sized receives the graph that was replayed (null otherwise): when its
+// status reports an overflow (a sized plan outgrown, or a class outside a
+// reused plan), the caller drops it and calls again, which plans anew.
+static void sparse_values_enqueue(int kind, const double* h_coeffs, i64 nb, const GridDesc& g,
+                                  const int64_t* d_indices, i64 m, double tol, int form, double* d_out, cudaStream_t s,
+                                  EvalStatus* h_status, std::shared_ptr<const LatticeTables>& tp, StageTimer& timer,
+                                  const GraphEntry** sized) {
+    *sized = nullptr;
+    const Context& ctx = context();
+    EvalArgs a = eval_args(kind, h_coeffs, nb, g, d_indices, m, tol, form, d_out, s, tp, timer);
+    const LatticeTables& t = *tp;
     const bool bounded = t.nkeys <= BOUNDED_KEYS;
     const bool graphs = g_graphs_enabled;
     // (stage timing replays graphs of its own, whose stage marks are nodes)
@@ -2627,90 +2705,121 @@ struct CopyStreams {
     }
 };
 static thread_local CopyStreams t_copy_streams;
-static thread_local PinnedBuf t_pin_status_chunks;
 
 // Page-locked class list and value arrays: the copies go straight between them
-// and the device buffers (no staging).  A list of a million classes or more is
-// evaluated in PINNED_CHUNKS contiguous ranges so that the copies overlap the
-// evaluations: the class list streams in on one copy stream, each range is
-// evaluated as soon as its part has arrived, and its values stream out on a
-// second copy stream (the two directions run concurrently) while the next
-// range is evaluated.  Each range is an evaluation of its own (its own plan
-// and sized graph); its values agree with one evaluation of the whole list
-// within the FP64 parity bar.
-constexpr i64 PINNED_CHUNKS = 4;
+// and the device buffers (no staging).  Once a list's graph has completed a
+// replay (its plan is kept and valid), a list of a million classes or more is
+// pipelined: the stages, which need only the kept plan, run while the class
+// list streams in on one copy stream in PIPE_CHUNKS ranges; each range is
+// gathered as soon as it has arrived (the plan-checking gather), and its values
+// stream out on a second copy stream while later ranges arrive.  The stages run
+// once for the whole list, so the values equal those of the other paths.  A
+// list that no longer fits the kept plan (rewritten since: a class of it fails
+// the gather's check) is evaluated again, whole and exactly.  Before that (the
+// first calls for a list) and for smaller lists, the list is copied in,
+// evaluated and copied out.
+constexpr i64 PIPE_CHUNKS = 8;
+
+struct PipeEvents {  // the pipeline's events, created once per thread and device
+    int device = -1;
+    cudaEvent_t start = nullptr, in[PIPE_CHUNKS] = {}, gathered[PIPE_CHUNKS] = {};
+    void ensure(int dev) {
+        if (dev == device) return;
+        release();
+        GLI_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+        for (i64 c = 0; c < PIPE_CHUNKS; ++c) {
+            GLI_CUDA(cudaEventCreateWithFlags(&in[c], cudaEventDisableTiming));
+            GLI_CUDA(cudaEventCreateWithFlags(&gathered[c], cudaEventDisableTiming));
+        }
+        device = dev;
+    }
+    void release() {
+        if (start) cudaEventDestroy(start);
+        for (i64 c = 0; c < PIPE_CHUNKS; ++c) {
+            if (in[c]) cudaEventDestroy(in[c]);
+            if (gathered[c]) cudaEventDestroy(gathered[c]);
+            in[c] = gathered[c] = nullptr;
+        }
+        start = nullptr;
+        device = -1;
+    }
+    ~PipeEvents() { release(); }
+};
+static thread_local PipeEvents t_pipe_events;
+
 static void sparse_values_pinned(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices,
                                  i64 m, double tol, int form, double* h_out, cudaStream_t s) {
     const Context& ctx = context();
     t_host_call.ensure(ctx.device, m);
-    const i64 chunks = m >= ((i64)1 << 20) ? PINNED_CHUNKS : 1, per = (m + chunks - 1) / chunks;
-    EvalStatus* hs = (EvalStatus*)t_pin_status_chunks.get(chunks * sizeof(EvalStatus));
+    EvalStatus* hs = (EvalStatus*)t_pin_status.get(sizeof(EvalStatus));
     std::shared_ptr<const LatticeTables> tp;
-    StageTimer timer(t_timing && chunks == 1, s);
-    std::vector<const GraphEntry*> sized(chunks, nullptr);
+    StageTimer timer(t_timing, s);
     int64_t* d_idx = t_host_call.idx->p;
     double* d_val = t_host_call.val->p;
-    if (chunks == 1) {
-        GLI_CUDA(cudaMemcpyAsync(d_idx, h_indices, (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-        for (int attempt = 0; attempt < 2; ++attempt) {
-            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx, m, tol, form, d_val, s, hs, tp, timer, &sized[0]);
+    GraphEntry* e = nullptr;
+    if (!t_timing && g_graphs_enabled && m >= ((i64)1 << 20)) {
+        const EvalArgs a = eval_args(kind, h_coeffs, nb, g, d_idx, m, tol, form, d_val, s, tp, timer);
+        e = find_graph(a, ctx.device, false);
+        if (e && !(e->planned && e->exec_stages)) e = nullptr;
+    }
+    if (e) {
+        t_copy_streams.ensure(ctx.device);
+        t_pipe_events.ensure(ctx.device);
+        cudaStream_t s_in = t_copy_streams.in, s_out = t_copy_streams.out;
+        PipeEvents& ev = t_pipe_events;
+        const i64 per = (m + PIPE_CHUNKS - 1) / PIPE_CHUNKS;
+        // the copy streams start after the work already queued on s
+        GLI_CUDA(cudaEventRecord(ev.start, s));
+        GLI_CUDA(cudaStreamWaitEvent(s_in, ev.start, 0));
+        GLI_CUDA(cudaStreamWaitEvent(s_out, ev.start, 0));
+        GLI_CUDA(cudaGraphLaunch(e->exec_stages, s));
+        add_launches(e->launches_stages);
+        for (i64 c = 0; c < PIPE_CHUNKS; ++c) {
+            const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
+            if (n > 0)
+                GLI_CUDA(cudaMemcpyAsync(d_idx + b, h_indices + b, (size_t)n * sizeof(int64_t),
+                                         cudaMemcpyHostToDevice, s_in));
+            GLI_CUDA(cudaEventRecord(ev.in[c], s_in));
+        }
+        for (i64 c = 0; c < PIPE_CHUNKS; ++c) {
+            const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
+            GLI_CUDA(cudaStreamWaitEvent(s, ev.in[c], 0));
+            launch_gather(e->gather, d_idx + b, n, d_val + b, ctx.num_sms, s);
+            GLI_CUDA(cudaEventRecord(ev.gathered[c], s));
+            GLI_CUDA(cudaStreamWaitEvent(s_out, ev.gathered[c], 0));
+            if (n > 0)
+                GLI_CUDA(cudaMemcpyAsync(h_out + b, d_val + b, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                                         s_out));
+        }
+        GLI_CUDA(cudaMemcpyAsync(hs, e->status.p, sizeof(EvalStatus), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s_out));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        t_paths = e->paths;
+        t_graph_timer = nullptr;
+        if (hs->cnt.overflow) {
+            // a class outside the kept plan: the list (already in device
+            // memory) once more, whole, with a new plan
+            drop_graph(e);
+            const GraphEntry* sized = nullptr;
+            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx, m, tol, form, d_val, s, hs, tp, timer, &sized);
             GLI_CUDA(cudaMemcpyAsync(h_out, d_val, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
             GLI_CUDA(cudaStreamSynchronize(s));
-            if (!hs->cnt.overflow) break;
-            drop_graph(sized[0]);  // the list outgrew its graph's sizes: once more, exactly
+            if (hs->cnt.overflow) fail(GLI_ERR_INTERNAL, "a new plan overflowed");
         }
         check_status(kind, m, *hs, *tp, timer, nullptr);
-        if (!hs->cnt.overflow) graph_replayed(sized[0]);
         return;
     }
-    t_copy_streams.ensure(ctx.device);
-    cudaStream_t s_in = t_copy_streams.in, s_out = t_copy_streams.out;
-    std::vector<cudaEvent_t> ev(2 * chunks + 1, nullptr);
-    struct Release {
-        std::vector<cudaEvent_t>& e;
-        ~Release() {
-            for (cudaEvent_t x : e)
-                if (x) cudaEventDestroy(x);
-        }
-    } release{ev};
-    for (auto& e : ev) GLI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    // the copy streams start after the work already queued on s
-    GLI_CUDA(cudaEventRecord(ev[2 * chunks], s));
-    GLI_CUDA(cudaStreamWaitEvent(s_in, ev[2 * chunks], 0));
-    GLI_CUDA(cudaStreamWaitEvent(s_out, ev[2 * chunks], 0));
-    for (i64 c = 0; c < chunks; ++c) {
-        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
-        if (n > 0)
-            GLI_CUDA(cudaMemcpyAsync(d_idx + b, h_indices + b, (size_t)n * sizeof(int64_t), cudaMemcpyHostToDevice,
-                                     s_in));
-        GLI_CUDA(cudaEventRecord(ev[c], s_in));
+    const GraphEntry* sized = nullptr;
+    GLI_CUDA(cudaMemcpyAsync(d_idx, h_indices, (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx, m, tol, form, d_val, s, hs, tp, timer, &sized);
+        GLI_CUDA(cudaMemcpyAsync(h_out, d_val, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GLI_CUDA(cudaStreamSynchronize(s));
+        if (!hs->cnt.overflow) break;
+        drop_graph(sized);  // the list outgrew its graph's sizes: once more, exactly
     }
-    for (i64 c = 0; c < chunks; ++c) {
-        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
-        GLI_CUDA(cudaStreamWaitEvent(s, ev[c], 0));
-        if (n > 0)
-            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx + b, n, tol, form, d_val + b, s, hs + c, tp, timer,
-                                  &sized[c]);
-        GLI_CUDA(cudaEventRecord(ev[chunks + c], s));
-        GLI_CUDA(cudaStreamWaitEvent(s_out, ev[chunks + c], 0));
-        if (n > 0)
-            GLI_CUDA(cudaMemcpyAsync(h_out + b, d_val + b, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s_out));
-    }
-    GLI_CUDA(cudaStreamSynchronize(s_out));
-    GLI_CUDA(cudaStreamSynchronize(s));
-    for (i64 c = 0; c < chunks; ++c) {
-        const i64 b = c * per, n = std::max<i64>(0, std::min(m, b + per) - b);
-        if (n <= 0) continue;
-        if (hs[c].cnt.overflow) {  // this range outgrew its graph's sizes: once more, exactly
-            drop_graph(sized[c]);
-            sparse_values_enqueue(kind, h_coeffs, nb, g, d_idx + b, n, tol, form, d_val + b, s, hs + c, tp, timer,
-                                  &sized[c]);
-            GLI_CUDA(cudaMemcpyAsync(h_out + b, d_val + b, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
-            GLI_CUDA(cudaStreamSynchronize(s));
-        }
-        check_status(kind, n, hs[c], *tp, timer, nullptr);
-        if (!hs[c].cnt.overflow) graph_replayed(sized[c]);
-    }
+    check_status(kind, m, *hs, *tp, timer, nullptr);
+    if (!hs->cnt.overflow) graph_replayed(sized);
 }
 
 void sparse_values_host(int kind, const double* h_coeffs, i64 nb, const GridDesc& g, const int64_t* h_indices, i64 m,

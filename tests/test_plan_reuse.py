@@ -145,3 +145,40 @@ def test_stream_ordered_evaluations(gli):
     t = queue(outs[1])
     assert L.gli_b200_sparse_values_wait(t) == 0, L.gli_b200_last_error_message().decode()
     assert_parity(outs[1].cpu().numpy(), refs[2], what="queued evaluation after the repair")
+
+
+def test_pinned_host_lists_pipeline(gli):
+    # gli_b200_sparse_values with page-locked host arrays: after the exact call
+    # and one replay, calls stream the list in ranges, gathering each as it
+    # arrives behind the stages of the kept plan; a list rewritten in place
+    # with classes outside that plan is evaluated again whole
+    import torch
+
+    from gausslectronitegrate_b200 import _abi
+    from gausslectronitegrate_b200 import workloads as W
+    full = gli.compute_sparse_eri_gausslet_integrals(g10(), W.ERI6_SPARSE, 1e-16)
+    m = full.indices.size // 2
+    halves = [full.indices[:m], full.indices[m:2 * m]]
+    refs = [full.values[:m], full.values[m:2 * m]]
+    idx = torch.from_numpy(halves[0].copy()).pin_memory()
+    out = torch.empty(m, dtype=torch.float64).pin_memory()
+    gd, keep = gli._parse_coeffs(np.ascontiguousarray(g10()), "")
+    L = gli.lib()
+
+    def run():
+        out.fill_(float("nan"))
+        return L.gli_b200_sparse_values(_abi.GLI_KIND_ERI, C.byref(gd), C.byref(gli._grid_struct(W.ERI6_SPARSE)),
+                                        C.cast(idx.data_ptr(), _abi.lptr), m, 1e-16, _abi.GLI_FORM_FP64,
+                                        C.cast(out.data_ptr(), _abi.dptr))
+
+    for k in range(5):
+        assert run() == 0, L.gli_b200_last_error_message().decode()
+        assert_parity(out.numpy(), refs[0], what=f"pinned first half, call {k}")
+    perm = np.random.default_rng(9).permutation(m)
+    idx.copy_(torch.from_numpy(halves[0][perm]))
+    assert run() == 0, L.gli_b200_last_error_message().decode()
+    assert_parity(out.numpy(), refs[0][perm], what="pinned first half permuted")
+    idx.copy_(torch.from_numpy(halves[1]))
+    for k in range(4):
+        assert run() == 0, L.gli_b200_last_error_message().decode()
+        assert_parity(out.numpy(), refs[1], what=f"pinned second half, call {k}")
