@@ -181,12 +181,13 @@ __global__ void k_dense_points(DenseGrid D, short4* __restrict__ pt) {
     pt[n] = make_short4((short)p[0], (short)p[1], (short)p[2], 0);
 }
 
-// slab i of the (i j k l) tensor, S[(j N + k) N + l] = V[i j k l], from the key
-// table (range L) of a complete list: 32-bit index arithmetic (N^3 < 2^32),
-// the points from a table, 32-bit axis keys, one entry per thread
+// slab i of the (i j k l) tensor, S[(j N + k) N + l] = V[i j k l], its first
+// `total` entries (rows j < total / N^2), from the key table (range L) of a
+// complete list: 32-bit index arithmetic (N^3 < 2^32), the points from a
+// table, 32-bit axis keys, one entry per thread
 __global__ void __launch_bounds__(256) k_fill_slab_keyed(const short4* __restrict__ pt, uint32_t N, int L, short4 pi,
-                                                         const double* __restrict__ table, double* __restrict__ S) {
-    const uint32_t total = N * N * N;
+                                                         const double* __restrict__ table, uint32_t total,
+                                                         double* __restrict__ S) {
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
         const uint32_t row = e / N, l = e - row * N, j = row / N, k = row - j * N;
         const short4 pj = pt[j], pk = pt[k], pl = pt[l];
@@ -213,6 +214,7 @@ struct KeyedSlabOp {
     double* C;            // N^2 x M row-major
     short4 pi;
     int N, L, M;
+    int rows;  // rows (j k) computed: j < rows / N
     struct Block {
         int mvalid, nvalid, nk;
         int m0;
@@ -224,7 +226,7 @@ struct KeyedSlabOp {
     struct BState {};
     __device__ bool begin(Block& b) const {
         b.m0 = blockIdx.x * DM_BM;
-        b.mvalid = min(DM_BM, N * N - b.m0);
+        b.mvalid = min(DM_BM, rows - b.m0);
         b.nvalid = min(BN, M);
         b.nk = (N + DM_BK - 1) / DM_BK;
         return b.mvalid > 0;
@@ -553,6 +555,14 @@ void apply_eri_device(const GridDesc& g, const int64_t* d_idx, const double* d_v
 
 // E[p,q,r,s] = sum V[i j k l] B[i p] B[j q] B[k r] B[l s] (chemists' order).
 // kind 1: V = ERI tensor; kind 0: V[i i j j] = ERIDA matrix (Khatri-Rao form).
+// W[j][i] = W[i][j] for j > i (blocks of `mm` doubles of an n x n array of blocks)
+__global__ void k_mirror_pairs(double* __restrict__ W, i64 n, i64 mm) {
+    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < n * n * mm; e += (i64)gridDim.x * blockDim.x) {
+        const i64 blk = e / mm, r = e - blk * mm, i = blk / n, j = blk - i * n;
+        if (j > i) W[e] = W[(j * n + i) * mm + r];
+    }
+}
+
 void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const double* d_val, i64 m,
                     const double* d_basis, i64 M, double* d_out, cudaStream_t s) {
     const SymGrid G = sym_of(g);
@@ -627,38 +637,46 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
             bx = bcomp.p;
         }
     }
-    const i64 Nx2 = Nx * Nx, per_i = Nx2 * Nx;
-    DevBuf<double> A1(Nx2 * M, s), A2(Nx * M * M, s), A3(Nx * M * M * M, s), S;
+    // V[i j k l] = V[j i k l]: the two first contractions run over the pairs
+    // j <= i only, W[i][j] = B^T V[i j] B (M x M), and W[j][i] = W[i][j] is
+    // copied; then A3[i] = B^T W[i] and E = B^T A3.  The generated entries and
+    // the dominant first contraction are halved.
+    const i64 Nx2 = Nx * Nx, MM = M * M;
+    DevBuf<double> A1(Nx2 * M, s), W(Nx2 * MM, s), A3(Nx * MM * M, s), S;
     // the first contraction with its slab computed as the GEMM stages it (at
     // most 32 orbitals), or from a filled slab
     const bool fused = slab32 && M <= 32;
-    if (!fused) S.alloc(per_i, s);
+    if (!fused) S.alloc(Nx2 * Nx, s);
     for (i64 i = 0; i < Nx; ++i) {
+        const i64 rows = (i + 1) * Nx;  // (j k) with j <= i
         if (fused) {
-            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, bx, A1.p, hpt[i], (int)Nx, (int)G.L, (int)M},
-                        dim3((unsigned)((Nx2 + DM_BM - 1) / DM_BM)), s);
+            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, bx, A1.p, hpt[i], (int)Nx, (int)G.L, (int)M, (int)rows},
+                        dim3((unsigned)((rows + DM_BM - 1) / DM_BM)), s);
         } else {
             if (slab32)
-                k_fill_slab_keyed<<<grid_for(per_i), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p, S.p);
+                k_fill_slab_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p,
+                                                                      (uint32_t)(rows * Nx), S.p);
             else if (kt.ok)
-                k_fill_eri_rows_keyed<<<grid_for(per_i), 256, 0, s>>>(D, kt.t.p, G.L, i * N, N, S.p);
+                k_fill_eri_rows_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(D, kt.t.p, G.L, i * N, i + 1, S.p);
             else
-                k_fill_eri_rows<<<grid_for(per_i), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, N, S.p);
+                k_fill_eri_rows<<<grid_for(rows * Nx), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, i + 1, S.p);
             GLI_CHECK_LAUNCH();
             // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-            dgemm((int)Nx2, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false,
+            dgemm((int)rows, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false,
                   s);
         }
-        // A2[j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j)
-        dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, A2.p, M * M, M, 1,
-              (int)Nx, false, s);
-        // A3[i][q][(r s)] = sum_j B[j][q] A2[j][(r s)]
-        dgemm((int)M, (int)(M * M), (int)Nx, MatView{bx, 0, 1, M}, MatView{A2.p, 0, M * M, 1},
-              A3.p + i * M * M * M, 0, M * M, 1, 1, false, s);
+        // W[i][j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j <= i)
+        dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, W.p + i * Nx * MM, MM, M, 1,
+              (int)(i + 1), false, s);
     }
+    k_mirror_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, MM);
+    GLI_CHECK_LAUNCH();
+    // A3[i][q][(r s)] = sum_j B[j][q] W[i][j][(r s)]   (batch i)
+    dgemm((int)M, (int)MM, (int)Nx, MatView{bx, 0, 1, M}, MatView{W.p, Nx * MM, MM, 1}, A3.p, MM * M, MM, 1,
+          (int)Nx, false, s);
     // E[p][(q r s)] = sum_i B[i][p] A3[i][(q r s)]
-    dgemm((int)M, (int)(M * M * M), (int)Nx, MatView{bx, 0, 1, M}, MatView{A3.p, 0, M * M * M, 1}, d_out, 0,
-          M * M * M, 1, 1, false, s);
+    dgemm((int)M, (int)(MM * M), (int)Nx, MatView{bx, 0, 1, M}, MatView{A3.p, 0, MM * M, 1}, d_out, 0, MM * M, 1, 1,
+          false, s);
 }
 
 }  // namespace gli

@@ -354,6 +354,21 @@ def test_project_eri(gli):
     assert np.max(np.abs(s.project(basis) - project_factored(dense, basis))) <= 1e-12
 
 
+def test_project_eri_wide_basis_and_zero_rows(gli):
+    # more than 32 columns (the slab filled, then contracted) and a basis with
+    # zero rows (the contraction over the nonzero rows only); the first two
+    # contractions run over the pairs j <= i of the (i j) symmetry
+    s = gli.compute_sparse_eri_gausslet_integrals(g10(), sym_grid(3), 1e-10)
+    dense = s.fill_tensor(sym_grid(3))
+    rng = np.random.default_rng(21)
+    basis = rng.normal(size=(27, 36))
+    basis[[0, 5, 13, 26]] = 0.0
+    got = s.project(basis)
+    ref = project_factored(dense, basis)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref)) * 27 ** 2
+    assert np.max(np.abs(got - got.transpose(1, 0, 2, 3))) <= 1e-13 * np.max(np.abs(ref))
+
+
 def test_eri_keyed_fill_equals_oracle_fill(gli):
     # a complete class list: dense entries come from the key-triple table; the
     # oracle canonicalises every entry and looks it up -- same class values in,
