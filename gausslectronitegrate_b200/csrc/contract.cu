@@ -1035,18 +1035,17 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
 // classes (the mark pass skipped): each class is decoded here from its index
 // (through the pair descriptors where PD, else class_keys) and checked against
 // the plan -- its (A, B) pair set in the plan's pair bitmap and its third key
-// a used key (kid[k2 + 1] > kid[k2]), which the marks of the list that made
-// the plan guarantee for every class of that list.  A class outside the plan
+// a used key (bit 31 of kk[k2]), which the marks of the list that made the
+// plan guarantee for every class of that list.  A class outside the plan
 // (the list was rewritten in place since) or outside the tensor sets the
 // overflow flag, and the host evaluates the list again with a new plan.  This
 // saves the mark pass's read of the indices and the write and re-read of the
 // packed keys (24 bytes per class).
 template <bool PD>
-__global__ void __launch_bounds__(256, 8) k_gather_q_plan(const double* __restrict__ Q, int parts, i64 part_stride,
+__global__ void __launch_bounds__(256, PD ? 8 : 6) k_gather_q_plan(const double* __restrict__ Q, int parts, i64 part_stride,
                                                         ClassDecode dec, const int64_t* __restrict__ idx, i64 m,
-                                                        const uint64_t* __restrict__ kid, int nk,
-                                                        const uint32_t* __restrict__ pairBits,
-                                                        const uint64_t* __restrict__ pairPre, int ldq,
+                                                        const uint32_t* __restrict__ kk, int nk,
+                                                        const uint2* __restrict__ bitpre, int ldq,
                                                         PlanCounts* __restrict__ cnt, double* __restrict__ out) {
     if (cnt->overflow) return;
     const bool vec = ((uintptr_t)idx & 15) == 0 && ((uintptr_t)out & 15) == 0;
@@ -1099,16 +1098,16 @@ __global__ void __launch_bounds__(256, 8) k_gather_q_plan(const double* __restri
                 const i64 slot = (i64)s1 * nk + s0;
                 if (slot != last_slot) {
                     last_slot = slot;
-                    const i64 w = slot >> 5;
-                    const uint32_t b = __ldg(&pairBits[w]), bit = (uint32_t)(slot & 31);
-                    last_pid = (b >> bit) & 1u ? (i64)__ldg(&pairPre[w]) + __popc(b & ((1u << bit) - 1u)) : -1;
+                    const uint2 bp = __ldg(&bitpre[slot >> 5]);  // (bits, pairs before the word)
+                    const uint32_t bit = (uint32_t)(slot & 31);
+                    last_pid = (bp.x >> bit) & 1u ? (i64)bp.y + __popc(bp.x & ((1u << bit) - 1u)) : -1;
                 }
-                const uint64_t k0 = __ldg(&kid[s2]), k1 = __ldg(&kid[s2 + 1]);
-                if (last_pid < 0 || k1 == k0) {
+                const uint32_t k0 = __ldg(&kk[s2]);  // key id, bit 31: a key the list uses
+                if (last_pid < 0 || !(k0 >> 31)) {
                     miss = true;
                     continue;
                 }
-                q[h][v] = last_pid * ldq + (i64)k0;
+                q[h][v] = last_pid * ldq + (i64)(k0 & 0x7fffffffu);
             }
         }
         double acc[G][4];
@@ -1387,6 +1386,11 @@ struct PlanReuse {
     uint32_t* saved_bits = nullptr;
     PlanCounts* saved_cnt = nullptr;
     int* valid = nullptr;  // null: no reuse (bounded plans)
+    // the plan in the form the plan-checking gather reads: per pair-bitmap
+    // word its bits and the pairs before it, per key its id with bit 31 set
+    // when the list uses it (one load each instead of two)
+    uint2* bitpre = nullptr;
+    uint32_t* kk = nullptr;
     // set: the replay did not mark its classes (the mark pass skipped them and
     // k_gather_q_plan checks each against the plan), so a valid saved plan is
     // restored without the comparison
@@ -1398,6 +1402,8 @@ struct PlanStore {
     DevMem<uint32_t> saved_used, saved_bits;
     DevMem<PlanCounts> saved_cnt;
     DevMem<int> valid;
+    DevMem<uint2> bitpre;
+    DevMem<uint32_t> kk;
     DevMem<uint2> pd;  // the ERI pair descriptors, when the decode uses them
     // the (pair, key) products of a product-form stage C, kept with the graph
     // so that a class gather launched apart from it can read them
@@ -1415,11 +1421,23 @@ struct PlanStore {
         tiles.alloc((size_t)tile_ints);
         saved_used.alloc((size_t)(2 * nk));
         saved_bits.alloc((size_t)words);
+        bitpre.alloc((size_t)words);
+        kk.alloc((size_t)nk);
         saved_cnt.alloc(1);
         valid.alloc(1);
         GLI_CUDA(cudaMemset(valid.p, 0, sizeof(int)));
     }
-    PlanReuse reuse(bool trust) { return PlanReuse{saved_used.p, saved_bits.p, saved_cnt.p, valid.p, trust ? 1 : 0}; }
+    PlanReuse reuse(bool trust) {
+        PlanReuse r;
+        r.saved_used = saved_used.p;
+        r.saved_bits = saved_bits.p;
+        r.saved_cnt = saved_cnt.p;
+        r.valid = valid.p;
+        r.bitpre = bitpre.p;
+        r.kk = kk.p;
+        r.trust = trust ? 1 : 0;
+        return r;
+    }
 };
 
 // Bounded plans (at most 256 keys: 512 key flags, 2,048 pair-bitmap words):
@@ -1535,7 +1553,11 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
     if (reuse.valid) {
         // save what this plan was made from, for the next replay's check
         for (i64 i = threadIdx.x; i < 2 * nk; i += blockDim.x) reuse.saved_used[i] = used[i];
-        for (i64 w = threadIdx.x; w < words; w += blockDim.x) reuse.saved_bits[w] = s_bits[w];
+        for (i64 w = threadIdx.x; w < words; w += blockDim.x) {
+            reuse.saved_bits[w] = s_bits[w];
+            reuse.bitpre[w] = make_uint2(s_bits[w], s_pre[w]);
+        }
+        if (k < nk) reuse.kk[k] = ex | (f ? 0x80000000u : 0u);
         if (threadIdx.x == 0) {
             PlanCounts c;
             c.key_total = key_total;
@@ -1727,10 +1749,9 @@ struct GatherLaunch {
     int parts = 0;
     i64 part_stride = 0;
     ClassDecode dec;
-    const uint64_t* kid = nullptr;
+    const uint32_t* kk = nullptr;
     int nk = 0;
-    const uint32_t* bits = nullptr;
-    const uint64_t* pre = nullptr;
+    const uint2* bitpre = nullptr;
     int ldq = 0;
     PlanCounts* cnt = nullptr;
 };
@@ -1742,10 +1763,10 @@ static void launch_gather(const GatherLaunch& gl, const int64_t* idx, i64 m, dou
     const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)num_sms * 8);
     if (gl.dec.pd)
         launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, gl.Q, gl.parts, gl.part_stride, gl.dec, idx, m,
-                      gl.kid, gl.nk, gl.bits, gl.pre, gl.ldq, gl.cnt, out);
+                      gl.kk, gl.nk, gl.bitpre, gl.ldq, gl.cnt, out);
     else
         launch_kernel(k_gather_q_plan<false>, dim3(gq), dim3(256), 0, s, gl.Q, gl.parts, gl.part_stride, gl.dec, idx,
-                      m, gl.kid, gl.nk, gl.bits, gl.pre, gl.ldq, gl.cnt, out);
+                      m, gl.kk, gl.nk, gl.bitpre, gl.ldq, gl.cnt, out);
 }
 
 // the u split of the stage-C product: 64-column tiles (the product's grid is
@@ -2138,17 +2159,16 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                     dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         t_enq_paths |= (fused ? 2 : 1) << 2;  // the class gather that ran
         if (fused) {
-            // (the plan's own pair bitmap: this replay's stays empty when the
-            // mark pass skipped)
+            // (the kept plan's packed lookups: this replay's pair bitmap stays
+            // empty when the mark pass skipped)
             GatherLaunch gl;
             gl.Q = Q.p;
             gl.parts = P;
             gl.part_stride = ps;
             gl.dec = dec;
-            gl.kid = ids.p;
+            gl.kk = pstore->kk.p;
             gl.nk = (int)nk;
-            gl.bits = pstore->saved_bits.p;
-            gl.pre = pairPre.p;
+            gl.bitpre = pstore->bitpre.p;
             gl.ldq = (int)nku;
             gl.cnt = cnt;
             if (split)
