@@ -445,21 +445,51 @@ static unsigned grid_for(i64 work, int per_block = 256) {
     return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
-// number of canonical ERI classes of a symmetric grid (enumerated once per extent)
-static i64 canonical_eri_count(const GridDesc& g, i64 e, cudaStream_t s) {
+// The canonical ERI class list of a symmetric grid of extent e (the
+// enumeration, sorted), kept on the device once made: a list is the complete
+// canonical list exactly when it equals this one.  Lists above
+// ENUM_KEEP_CLASSES are not kept (their count is): the per-class orbit test
+// decides for them.
+constexpr i64 ENUM_KEEP_CLASSES = (i64)1 << 27;  // 1 GB of indices
+struct CanonicalList {
+    i64 count = 0;
+    int64_t* d = nullptr;  // null: not kept
+};
+static CanonicalList canonical_eri_list(const GridDesc& g, i64 e, cudaStream_t s) {
     static std::mutex mu;
-    static std::map<i64, i64> cache;
+    static std::map<std::pair<int, i64>, CanonicalList> cache;  // (device, extent)
+    int dev = 0;
+    GLI_CUDA(cudaGetDevice(&dev));
     {
         std::lock_guard<std::mutex> lk(mu);
-        auto it = cache.find(e);
+        auto it = cache.find({dev, e});
         if (it != cache.end()) return it->second;
     }
     int64_t* d = nullptr;
-    const i64 n = enumerate_device(1, g, &d, s);
-    if (d) GLI_CUDA(cudaFreeAsync(d, s));
+    CanonicalList c;
+    c.count = enumerate_device(1, g, &d, s);
+    if (d && c.count <= ENUM_KEEP_CLASSES) {
+        c.d = d;  // kept for the process (one list per device and extent)
+    } else if (d) {
+        GLI_CUDA(cudaFreeAsync(d, s));
+    }
     std::lock_guard<std::mutex> lk(mu);
-    cache[e] = n;
-    return n;
+    auto it = cache.find({dev, e});
+    if (it != cache.end()) {  // another thread made it meanwhile
+        if (c.d) GLI_CUDA(cudaFreeAsync(c.d, s));
+        return it->second;
+    }
+    cache[{dev, e}] = c;
+    return c;
+}
+
+// bad = 1 where the list differs from the canonical list
+__global__ void k_equal_lists(const int64_t* __restrict__ a, const int64_t* __restrict__ b, i64 m,
+                              int* __restrict__ bad) {
+    bool differ = false;
+    for (i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x; n < m; n += (i64)gridDim.x * blockDim.x)
+        differ = differ || a[n] != b[n];
+    if (differ) atomicOr(bad, 1);
 }
 
 // Key table of a complete ERI class list, or an empty buffer when the list is
@@ -477,10 +507,14 @@ static void build_key_table(const SymGrid& G, const GridDesc& g, const int64_t* 
     const i64 nk = L * (L + 1) / 2 * (2 * L - 1);
     const i64 slots = nk * (nk + 1) * (nk + 2) / 6;
     if (slots > ((i64)1 << 29)) return;  // above 4 GB: keep the lookups
-    if (canonical_eri_count(g, G.e, s) != m) return;
+    const CanonicalList canon = canonical_eri_list(g, G.e, s);
+    if (canon.count != m) return;
     DevBuf<int> bad(1, s);
     bad.zero();
-    k_check_complete<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(G, d_idx, m, bad.p);
+    if (canon.d)
+        k_equal_lists<<<grid_for(m), 256, 0, s>>>(d_idx, canon.d, m, bad.p);
+    else
+        k_check_complete<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(G, d_idx, m, bad.p);
     GLI_CHECK_LAUNCH();
     int h = 0;
     GLI_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
