@@ -201,10 +201,14 @@ __global__ void __launch_bounds__(256) k_fill_slab_keyed(const short4* __restric
     }
 }
 
-// A1[(j k)][s] = sum_l V[i j k l] B[l][s] for slab i of a complete list, the
-// slab never written out: each A element is computed from the key table as the
-// tile is staged (K-major A tiles: a thread keeps its row (j, k) and walks l),
-// B (the basis, at most 32 columns) read row-major.
+// A1[(j k)][s] = sum_l U[k][l] B[l][s] for slab i of a complete list, where U
+// is the upper triangle (l >= k) of the symmetric V[i j k .] with its diagonal
+// halved, so that B^T V[i j] B = Y + Y^T for Y = B^T A1[j]: half of the
+// entries are generated.  The slab is never written out: each A element is
+// computed from the key table as the tile is staged (K-major A tiles: a
+// thread keeps its row (j, k) and walks l), B (the basis, at most 32 columns)
+// read row-major.  A row tile (rows of one j) starts its K loop at the chunk
+// of its smallest k, the elements below each row's k staged as zeros.
 struct KeyedSlabOp {
     static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
     static constexpr int BN = 32;
@@ -217,19 +221,26 @@ struct KeyedSlabOp {
     int rows;  // rows (j k) computed: j < rows / N
     struct Block {
         int mvalid, nvalid, nk;
-        int m0;
+        int m0, kc0;
     };
     struct AState {
         int d[3], s[3], k[3];  // pi - pj, pi + pj, pk per axis of this thread's row
+        int kr;                // the row's k
         bool ok;
     };
     struct BState {};
+    // row tiles never straddle two j: tile t holds rows (j, k0 .. k0 + 63) of
+    // j = t / tpj, k0 = 64 (t % tpj), tpj = ceil(N / 64) tiles per j
     __device__ bool begin(Block& b) const {
-        b.m0 = blockIdx.x * DM_BM;
-        b.mvalid = min(DM_BM, rows - b.m0);
+        const int tpj = (N + DM_BM - 1) / DM_BM, j = blockIdx.x / tpj;
+        const int k0 = (blockIdx.x - j * tpj) * DM_BM;
+        b.m0 = j * N + k0;
+        b.mvalid = min(DM_BM, N - k0);
+        if (b.m0 >= rows || b.mvalid <= 0) return false;
+        b.kc0 = k0 / DM_BK;  // l >= k >= k0: the chunks below are zero
         b.nvalid = min(BN, M);
-        b.nk = (N + DM_BK - 1) / DM_BK;
-        return b.mvalid > 0;
+        b.nk = (N + DM_BK - 1) / DM_BK - b.kc0;
+        return true;
     }
     __device__ void a_init(const Block& b, AState& st) const {
         const int r = dm_kmajor_row(threadIdx.x);
@@ -239,13 +250,14 @@ struct KeyedSlabOp {
         st.d[0] = pi.x - pj.x, st.d[1] = pi.y - pj.y, st.d[2] = pi.z - pj.z;
         st.s[0] = pi.x + pj.x, st.s[1] = pi.y + pj.y, st.s[2] = pi.z + pj.z;
         st.k[0] = pk.x, st.k[1] = pk.y, st.k[2] = pk.z;
+        st.kr = k;
     }
     __device__ void a_issue(const Block& b, AState& st, int kc, double* tile) const {
         const int r = dm_kmajor_row(threadIdx.x);
 #pragma unroll
         for (int q = 0; q < DM_ELEMS; ++q) {
-            const int kq = dm_kmajor_k(threadIdx.x, q), l = kc * DM_BK + kq;
-            const bool v = st.ok && l < N;
+            const int kq = dm_kmajor_k(threadIdx.x, q), l = (b.kc0 + kc) * DM_BK + kq;
+            const bool v = st.ok && l < N && l >= st.kr;
             const double* src = table;
             if (v) {
                 const short4 pl = pt[l];
@@ -260,11 +272,19 @@ struct KeyedSlabOp {
             dm_cp8(tile + dm_kmajor_at(r, kq), src, v);
         }
     }
+    // the diagonal element of the row, halved once it has landed
+    static constexpr bool A_LANDED = true;
+    __device__ void a_landed(const Block& b, AState& st, int kc, double* tile) const {
+        const int r = dm_kmajor_row(threadIdx.x), kq = st.kr - (b.kc0 + kc) * DM_BK;
+        if (!st.ok || kq < 0 || kq >= DM_BK || ((kq - (threadIdx.x >> 6)) & 1)) return;  // not this thread's element
+        tile[dm_kmajor_at(r, kq)] *= 0.5;
+    }
     __device__ void b_init(const Block&, BState&) const {}
     __device__ void b_issue(const Block& b, BState&, int kc, double* tile) const {
 #pragma unroll
         for (int q = 0; q < BN * DM_BK / DM_THREADS; ++q) {
-            const int n = dm_rowmajor_row(threadIdx.x, q), kq = dm_rowmajor_k(threadIdx.x), l = kc * DM_BK + kq;
+            const int n = dm_rowmajor_row(threadIdx.x, q), kq = dm_rowmajor_k(threadIdx.x);
+            const int l = (b.kc0 + kc) * DM_BK + kq;
             const bool v = n < b.nvalid && l < N;
             dm_cp8(tile + dm_rowmajor_at(n, kq), v ? basis + (i64)l * M + n : basis, v);
         }
@@ -597,6 +617,26 @@ __global__ void k_mirror_pairs(double* __restrict__ W, i64 n, i64 mm) {
     }
 }
 
+// W[i][j] = Y + Y^T for the M x M blocks Y of the pairs j <= i (each entry
+// pair (r, s), (s, r) by one thread), and W[j][i] = W[i][j]
+__global__ void k_symmetrize_pairs(double* __restrict__ W, i64 n, int M) {
+    const i64 mm = (i64)M * M;
+    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < n * n * mm; e += (i64)gridDim.x * blockDim.x) {
+        const i64 blk = e / mm, rs = e - blk * mm, i = blk / n, j = blk - i * n;
+        const int r = (int)(rs / M), c = (int)(rs - (i64)r * M);
+        if (j > i || c < r) continue;
+        double* y = W + blk * mm;
+        const double v = y[(i64)r * M + c] + y[(i64)c * M + r];
+        y[(i64)r * M + c] = v;
+        y[(i64)c * M + r] = v;
+        if (j < i) {
+            double* t = W + (j * n + i) * mm;
+            t[(i64)r * M + c] = v;
+            t[(i64)c * M + r] = v;
+        }
+    }
+}
+
 void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const double* d_val, i64 m,
                     const double* d_basis, i64 M, double* d_out, cudaStream_t s) {
     const SymGrid G = sym_of(g);
@@ -684,8 +724,9 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     for (i64 i = 0; i < Nx; ++i) {
         const i64 rows = (i + 1) * Nx;  // (j k) with j <= i
         if (fused) {
+            const i64 tpj = (Nx + DM_BM - 1) / DM_BM;  // row tiles per j
             dmma_launch(KeyedSlabOp{pt.p, kt.t.p, bx, A1.p, hpt[i], (int)Nx, (int)G.L, (int)M, (int)rows},
-                        dim3((unsigned)((rows + DM_BM - 1) / DM_BM)), s);
+                        dim3((unsigned)((i + 1) * tpj)), s);
         } else {
             if (slab32)
                 k_fill_slab_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p,
@@ -703,7 +744,10 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
         dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, W.p + i * Nx * MM, MM, M, 1,
               (int)(i + 1), false, s);
     }
-    k_mirror_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, MM);
+    if (fused)  // the fused slabs gave Y = B^T U B: W = Y + Y^T, then the mirror
+        k_symmetrize_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, (int)M);
+    else
+        k_mirror_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, MM);
     GLI_CHECK_LAUNCH();
     // A3[i][q][(r s)] = sum_j B[j][q] W[i][j][(r s)]   (batch i)
     dgemm((int)M, (int)MM, (int)Nx, MatView{bx, 0, 1, M}, MatView{W.p, Nx * MM, MM, 1}, A3.p, MM * M, MM, 1,

@@ -120,6 +120,19 @@ __device__ __forceinline__ double dm_frag(const double* s, int row0, int k0, int
 //   void b_issue(const Block&, BState&, int kc, double* tile)   (chunks issued in order)
 //   void store(const Block&, int m, int n, double v_n, double v_n1)   C[m][n], C[m][n+1]
 //
+// Op::a_landed(const Block&, AState&, int kc, double* tile) (optional, when
+// the Op declares A_LANDED): called by each thread once its own copies of
+// chunk kc have landed and before the block's barrier, to adjust the elements
+// it copied (in place, in shared memory)
+template <class Op, class = void>
+struct dm_a_landed {
+    static constexpr bool value = false;
+};
+template <class Op>
+struct dm_a_landed<Op, std::void_t<decltype(Op::A_LANDED)>> {
+    static constexpr bool value = Op::A_LANDED;
+};
+
 // The k loop of one block; FULL: every m8n8 tile of the warp's quadrant holds
 // data, so the MMAs run unpredicated (a runtime predicate per MMA costs about
 // a fifth of the tensor-pipe throughput).
@@ -132,6 +145,7 @@ __device__ __forceinline__ void dm_mainloop(const Op& op, const typename Op::Blo
     const int nk = blk.nk;
     for (int kc = 0; kc < nk; ++kc) {
         dm_wait<NS - 2>();  // chunk kc has landed (this thread's copies)
+        if constexpr (dm_a_landed<Op>::value) op.a_landed(blk, as, kc, smem + (kc % NS) * STAGE);
         __syncthreads();    // ... everyone's; and chunk kc - 1 is consumed
         const int nx = kc + NS - 1;
         if (nx < nk) {
