@@ -44,11 +44,6 @@ T* host_alloc(i64 count) {
     return (T*)p;
 }
 
-template <class T>
-void to_device(DevBuf<T>& d, const T* h, i64 n, cudaStream_t s) {
-    d.alloc(n, s);
-    if (n) GLI_CUDA(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
-}
 
 // Large device -> host copies into pageable memory (dense kinetic and nuclear
 // matrices, dense tensors: up to GBs) go through two page-locked staging
@@ -112,6 +107,42 @@ void to_host(T* h, const T* d, i64 n, cudaStream_t s) {
             GLI_CUDA(cudaEventSynchronize(t_staged.ev[p & 1]));
             parallel_memcpy((char*)h + off, t_staged.pin[p & 1], len);
         }
+    }
+}
+
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes a = {};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Host -> device copies of long arrays in pageable memory (class lists and
+// values of the reference-facing calls: tens of MB) go through the same two
+// page-locked staging buffers: the host copy of one chunk, split over a few
+// threads, overlaps the DMA of the previous one.  Returns with the last DMAs
+// queued on s (the buffers are not rewritten before their events complete).
+template <class T>
+void to_device(DevBuf<T>& d, const T* h, i64 n, cudaStream_t s) {
+    d.alloc(n, s);
+    const size_t bytes = (size_t)n * sizeof(T);
+    constexpr size_t kChunk = (size_t)16 << 20;
+    if (bytes < kChunk || host_pinned(h)) {
+        if (n) GLI_CUDA(cudaMemcpyAsync(d.p, h, bytes, cudaMemcpyHostToDevice, s));
+        return;
+    }
+    t_staged.ensure();
+    for (int k = 0; k < 2; ++k) GLI_CUDA(cudaEventSynchronize(t_staged.ev[k]));  // earlier uses of the buffers
+    const size_t chunks = (bytes + kChunk - 1) / kChunk;
+    for (size_t c = 0; c < chunks; ++c) {
+        const size_t off = c * kChunk, len = std::min(kChunk, bytes - off);
+        const int k = (int)(c & 1);
+        if (c >= 2) GLI_CUDA(cudaEventSynchronize(t_staged.ev[k]));  // the buffer's previous DMA is done
+        parallel_memcpy(t_staged.pin[k], (const char*)h + off, len);
+        GLI_CUDA(cudaMemcpyAsync((char*)d.p + off, t_staged.pin[k], len, cudaMemcpyHostToDevice, s));
+        GLI_CUDA(cudaEventRecord(t_staged.ev[k], s));
     }
 }
 
