@@ -2232,6 +2232,9 @@ struct GraphEntry {
     int paths = 0;           // tensor-core stages of the captured evaluation
     DevMem<EvalStatus> status;
     ~GraphEntry() {
+        // (an entry may be evicted or dropped while a queued replay of it --
+        // a stream-ordered call not yet waited for -- is still running)
+        cudaDeviceSynchronize();
         if (exec) cudaGraphExecDestroy(exec);
         if (exec_trust) cudaGraphExecDestroy(exec_trust);
         if (exec_stages) cudaGraphExecDestroy(exec_stages);

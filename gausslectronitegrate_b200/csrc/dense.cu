@@ -617,23 +617,23 @@ __global__ void k_mirror_pairs(double* __restrict__ W, i64 n, i64 mm) {
     }
 }
 
-// W[i][j] = Y + Y^T for the M x M blocks Y of the pairs j <= i (each entry
-// pair (r, s), (s, r) by one thread), and W[j][i] = W[i][j]
-__global__ void k_symmetrize_pairs(double* __restrict__ W, i64 n, int M) {
+// W[i][j] = Y + Y^T for the M x M blocks Y (M <= 32) of the pairs j <= i, and
+// W[j][i] = W[i][j]: one block per pair (blockIdx.y = i, blockIdx.x = j), Y
+// read once into shared memory, the sums written row by row (coalesced)
+__global__ void __launch_bounds__(256) k_symmetrize_pairs(double* __restrict__ W, i64 n, int M) {
+    __shared__ double y[32 * 33];
+    const i64 i = blockIdx.y, j = blockIdx.x;
+    if (j > i) return;
     const i64 mm = (i64)M * M;
-    for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < n * n * mm; e += (i64)gridDim.x * blockDim.x) {
-        const i64 blk = e / mm, rs = e - blk * mm, i = blk / n, j = blk - i * n;
-        const int r = (int)(rs / M), c = (int)(rs - (i64)r * M);
-        if (j > i || c < r) continue;
-        double* y = W + blk * mm;
-        const double v = y[(i64)r * M + c] + y[(i64)c * M + r];
-        y[(i64)r * M + c] = v;
-        y[(i64)c * M + r] = v;
-        if (j < i) {
-            double* t = W + (j * n + i) * mm;
-            t[(i64)r * M + c] = v;
-            t[(i64)c * M + r] = v;
-        }
+    double* blk = W + (i * n + j) * mm;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) y[(e / M) * 33 + e % M] = blk[e];
+    __syncthreads();
+    double* mir = W + (j * n + i) * mm;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+        const int r = e / M, c = e - r * M;
+        const double v = y[r * 33 + c] + y[c * 33 + r];
+        blk[e] = v;
+        if (j < i) mir[e] = v;
     }
 }
 
@@ -745,7 +745,7 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
               (int)(i + 1), false, s);
     }
     if (fused)  // the fused slabs gave Y = B^T U B: W = Y + Y^T, then the mirror
-        k_symmetrize_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, (int)M);
+        k_symmetrize_pairs<<<dim3((unsigned)Nx, (unsigned)Nx), 256, 0, s>>>(W.p, Nx, (int)M);
     else
         k_mirror_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, MM);
     GLI_CHECK_LAUNCH();
