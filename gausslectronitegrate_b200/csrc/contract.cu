@@ -1772,16 +1772,15 @@ static void launch_gather(const GatherLaunch& gl, const int64_t* idx, i64 m, dou
 // the u split of the stage-C product: 64-column tiles (the product's grid is
 // small, and wider tiles cost it parallelism: ERIDA 129^3 73 us with 80
 // columns, 66 us with 64).  A grid under a wave (four blocks per SM; about half
-// the column tiles are active after the A-key shift) splits u in up to three
-// where the classes are few beside the product (each class then sums the
-// slices: ERIDA 129^3 has 366,145 classes and 1.08 million products, 45 us
-// against 47 with two slices; ERI 7^3's 3.57 million classes would pay more in
-// the gather than the split saves).  Returns the slices; *u_chunk their length.
-static int product_split(i64 nP, i64 nku, int U, i64 m, int num_sms, int* u_chunk) {
+// the column tiles are active after the A-key shift) splits u over up to four
+// blocks of a cluster, which sum their partial tiles in distributed shared
+// memory, so Q holds one product per (pair, key).  (Summing slices of Q in the
+// gather instead made ERI 7^3's 3.57 million classes read several values
+// each.)  Returns the blocks per tile; *u_chunk their length of u.
+static int product_split(i64 nP, i64 nku, int U, int num_sms, int* u_chunk) {
     const i64 mt = (nP + DM_BM - 1) / DM_BM, nt = (nku + DM_BN - 1) / DM_BN;
     *u_chunk = U;
-    int P = std::min(3, split_count(mt * ((nt + 1) / 2), U, DM_BK, 4 * (i64)num_sms, u_chunk));
-    if (2 * m > nP * nku) P = 1;
+    const int P = std::min(4, split_count(mt * ((nt + 1) / 2), U, DM_BK, 4 * (i64)num_sms, u_chunk));
     *u_chunk = ((U + P - 1) / P + DM_BK - 1) / DM_BK * DM_BK;
     return (U + *u_chunk - 1) / *u_chunk;
 }
@@ -1816,8 +1815,8 @@ struct StageBufs {
         H.alloc(sz.nA * (i64)nS, s);
         H2.alloc(sz.nP * (i64)Up, s);
         if (product) {
-            q_parts = product_split(sz.nP, sz.nku, U, a.m, a.num_sms, &u_chunk);
-            const i64 q = q_parts * sz.nP * sz.nku;
+            q_parts = product_split(sz.nP, sz.nku, U, a.num_sms, &u_chunk);
+            const i64 q = sz.nP * sz.nku;
             if (keep && keep->Q.p && keep->Q.n >= (size_t)q)
                 Q.borrow(keep->Q.p, q, s);  // a graph's own products, kept between its replays
             else
@@ -2154,16 +2153,17 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         const i64 ps = nP * nku;
         const DevBuf<double>& Q = sb.Q;
         if (P < 1 || !Q.p) fail(GLI_ERR_INTERNAL, "stage C product without its buffer");
-        dmma_launch(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up, (int)nku,
-                                  u_chunk, ps, Q.p, &st->products},
-                    dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
+        // (a split sums its parts inside a cluster of the P blocks of a tile)
+        dmma_launch_cluster(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up,
+                                          (int)nku, u_chunk, 0, Q.p, &st->products},
+                            dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
         t_enq_paths |= (fused ? 2 : 1) << 2;  // the class gather that ran
         if (fused) {
             // (the kept plan's packed lookups: this replay's pair bitmap stays
             // empty when the mark pass skipped)
             GatherLaunch gl;
             gl.Q = Q.p;
-            gl.parts = P;
+            gl.parts = 1;
             gl.part_stride = ps;
             gl.dec = dec;
             gl.kk = pstore->kk.p;
@@ -2177,7 +2177,7 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                 launch_gather(gl, a.idx, m, a.out, a.num_sms, s);
         } else {
             const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
-            launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, P, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
+            launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, 1, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
                           pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
         }
     }
@@ -2310,6 +2310,7 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
     dmma_prepare<StageBOp<true>>();
     dmma_prepare<StageBOp<false>>();
     dmma_prepare<ProductOp<64>>();
+    dmma_prepare<ProductOp<64>, true>();
     dmma_prepare<StageAOp<64>, true>();
     dmma_prepare<StageAOp<80>, true>();
     dmma_prepare<StageBOp<true>, true>();
@@ -2330,7 +2331,7 @@ static GraphEntry* capture_graph(const EvalArgs& a, const std::shared_ptr<const 
         i64 q_entries = 0;
         if (product) {
             int u_chunk = 0;
-            q_entries = product_split(szb.nP, szb.nku, (int)a.t->U, a.m, a.num_sms, &u_chunk) * szb.nP * szb.nku;
+            q_entries = szb.nP * szb.nku;
         }
         e->plan = std::make_unique<PlanStore>();
         e->plan->alloc(nk, words, szb.nA, szb.nP, PairTiles::ints(szb.nA, szb.nP, 64, true),
