@@ -424,10 +424,13 @@ def run_ours(args):
         ms4 = (C.c_float * 4)()
         sz3 = (_abi.glong * 3)()
         L.gli_b200_last_stage_times(ms4, sz3)
+        ms2 = (C.c_float * 2)()
+        L.gli_b200_last_stage_c_times(ms2)
         L.gli_b200_set_timing(0)
         plan4 = (_abi.glong * 4)()
         L.gli_b200_last_plan(plan4)
         stage[name] = {"tables": float(ms4[0]), "A": float(ms4[1]), "B": float(ms4[2]), "C": float(ms4[3]),
+                       "C_product": float(ms2[0]), "C_class": float(ms2[1]),
                        "sizes": (int(sz3[0]), int(sz3[1]), int(sz3[2])), "plan": tuple(int(x) for x in plan4)}
     nA, nP, U = stage[chosen]["sizes"]
     peak = C.c_double()
@@ -474,9 +477,13 @@ def run_ours(args):
             cpu = {"value": None, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {ex}"}
     st = stage[chosen]
-    dom = max(("A", "B", "C"), key=lambda k: st[k])
+    # the dominant kernel: stage A, stage B, or one of stage C's two kernels
+    # (its product GEMM, and the class gather or per-class dots after it)
+    dom = max(("A", "B", "C_product", "C_class"), key=lambda k: st[k])
     roof = roofline(paths[chosen], dom, st, st["plan"], U, m, peak.value)
-    roof["traffic"] = measured_traffic(f"{args.workload}:{dom}{':tc' if roof['bound'] == 'hbm' and dom in 'AB' else ''}")
+    # (measured DRAM bytes per launch are keyed by stage; "C" is the class gather)
+    tkey = {"C_class": "C"}.get(dom, dom) + (":tc" if roof["bound"] == "hbm" and dom in ("A", "B") else "")
+    roof["traffic"] = measured_traffic(f"{args.workload}:{tkey}")
     line = {
         "metric": METRIC, "value": main["value"], "unit": "classes/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": main["ms_per_step"], "higher_is_better": True,
@@ -500,7 +507,8 @@ def run_ours(args):
                                        "B": "s8 tcgen05" if v[1] else "f64 dmma",
                                        "C": ("f64 product gemm + " + GATHERS[v[2]]) if v[2] else "f64 per-class dots"}
                                    for k, v in paths.items()},
-                   "stage_ms": {k: {s_: v[s_] for s_ in ("tables", "A", "B", "C")} for k, v in stage.items()},
+                   "stage_ms": {k: {s_: v[s_] for s_ in ("tables", "A", "B", "C", "C_product", "C_class")}
+                                for k, v in stage.items()},
                    "stage_sizes": {k: {"keys_A": v["sizes"][0], "key_pairs": v["sizes"][1], "lattice_U": v["sizes"][2]}
                                    for k, v in stage.items()},
                    "wall_s_timed_region": main["wall_s"]},
@@ -874,44 +882,41 @@ def lattice_nS(U):
 
 
 def roofline(paths, dom, st, plan, U, m, fp64_peak):
-    """Roofline entry of the dominant stage (from the library's stage events).
-    FP64 stages (the FP64 tensor-core GEMM k_dmma, or the per-class dots of
-    stage C): the stage's algorithmic FP64 FLOPs against the measured FP64 peak
-    (gli_b200_measure_fp64_peak: the faster of the FMA and m8n8k4 MMA probes).
-    Tensor-core stages of the mixed form: the sliced work is bound by the bytes
-    it must move (int8 slices read, FP64 results written) against the measured
-    HBM bandwidth.  paths = the library's per-stage report of the step
+    """Roofline entry of the dominant kernel (from the library's stage events:
+    stage A, stage B, or one of stage C's two kernels, C_product and C_class).
+    FP64 kernels (the FP64 tensor-core GEMM k_dmma, or the per-class dots of
+    stage C): the kernel's algorithmic FP64 FLOPs against the measured FP64
+    peak (gli_b200_measure_fp64_peak: the faster of the FMA and m8n8k4 MMA
+    probes).  Tensor-core stages of the mixed form: the sliced work is bound by
+    the bytes it must move (int8 slices read, FP64 results written) against the
+    measured HBM bandwidth.  paths = the library's per-stage report of the step
     (gli_b200_last_paths); plan = (nA, nP, used keys, stage C products): the
     (pair, key) products the product GEMM computed, 0 when stage C ran per
-    class (one length-U dot product per class).  A product-form stage C with
-    at least 8 classes per product is the class gather's HBM traffic (16 bytes
-    per class) against the measured HBM bandwidth."""
+    class (one length-U dot product per class).  The class gather after the
+    product GEMM moves 16 bytes per class (the class index in, its value out)
+    against the measured HBM bandwidth."""
     nA, nP, nku, product = plan
     ms = st[dom]
     nS = lattice_nS(U)
     kp = (U + 63) // 64 * 64
     on_tensor_cores = bool((dom == "A" and paths[0]) or (dom == "B" and paths[1]))
-    if dom == "C" and product and m >= 8 * product:
-        # the product GEMM is small beside the class gather (ERI 7^3: 207k
-        # products for 3.57 million classes): the stage moves 8 bytes of packed
-        # keys in and 8 bytes of value out per class, the gather's HBM traffic
-        ms = st[dom]
+    if dom == "C_class" and product:
         bytes_ = 16.0 * m
         achieved = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else None
         mp = measured_peaks()
         peak = mp["hbm_gbs"]
-        return {"bound": "hbm", "stage": dom, "kernel": f"{GATHERS[paths[2]]} (+ k_dmma<ProductOp> in the stage time)",
+        return {"bound": "hbm", "stage": "C", "kernel": GATHERS[paths[2]],
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved and peak else None,
                 "peak_source": peak_source(mp),
                 "algorithmic_bytes_per_launch": bytes_, "products": product, "traffic": None}
     if not on_tensor_cores:
         flops = {"A": 2.0 * nA * nS * U, "B": 2.0 * nP * U * U,
-                 "C": 2.0 * (product if product else m) * U}[dom]
-        kernel = {"A": "k_dmma<StageAOp>", "B": "k_dmma<StageBOp>",
-                  "C": "k_dmma<ProductOp> + k_gather_q" if product else "k_stage_c"}[dom]
+                 "C_product": 2.0 * product * U, "C_class": 2.0 * m * U}[dom]
+        kernel = {"A": "k_dmma<StageAOp>", "B": "k_dmma<StageBOp>", "C_product": "k_dmma<ProductOp>",
+                  "C_class": "k_stage_c"}[dom]
         achieved = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
-        return {"bound": "fp64", "stage": dom, "kernel": kernel,
+        return {"bound": "fp64", "stage": dom[0], "kernel": kernel,
                 "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if achieved and fp64_peak else None,
                 "peak_source": "measured FP64 peak on this device (gli_b200_measure_fp64_peak: "

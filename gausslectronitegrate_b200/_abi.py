@@ -78,7 +78,8 @@ EXPORTS = [
     "gli_b200_last_error", "gli_b200_last_error_message", "gli_b200_device_count", "gli_b200_set_device",
     "gli_b200_version", "gli_b200_sparse_values_dev", "gli_b200_sparse_values_dev_async",
     "gli_b200_sparse_values_wait", "gli_b200_sparse_values", "gli_b200_enumerate_dev",
-    "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_last_plan",
+    "gli_b200_free_dev", "gli_b200_set_timing", "gli_b200_last_stage_times", "gli_b200_last_stage_c_times",
+    "gli_b200_last_plan",
     "gli_b200_last_paths", "gli_b200_last_screening", "gli_b200_clear_caches", "gli_b200_measure_fp64_peak",
     "gli_b200_kinetic_matrix_noalloc", "gli_b200_launch_count", "gli_b200_dgemm_sliced_dev",
     "gli_b200_nuclear_batch_dev", "gli_b200_nuclear_batch", "gli_b200_last_nuclear_batch", "gli_b200_autotune_report",
@@ -148,6 +149,7 @@ def load(path=LIB_PATH):
     L.gli_b200_free_dev.argtypes = [C.c_void_p, C.c_void_p]
     L.gli_b200_set_timing.argtypes = [C.c_int]
     L.gli_b200_last_stage_times.argtypes = [P(C.c_float), P(glong)]
+    L.gli_b200_last_stage_c_times.argtypes = [P(C.c_float)]
     L.gli_b200_last_plan.argtypes = [P(glong)]
     L.gli_b200_last_paths.argtypes = [P(C.c_int)]
     L.gli_b200_last_screening.argtypes = [P(C.c_double)]

@@ -332,6 +332,13 @@ int gli_b200_last_stage_times(float ms[4], glong sizes[3]) {
     return GLI_OK;
 }
 
+int gli_b200_last_stage_c_times(float ms[2]) {
+    const gli::ContractStats& st = gli::last_stats();
+    ms[0] = st.ms_c_product;
+    ms[1] = st.ms_c_class;
+    return GLI_OK;
+}
+
 int gli_b200_last_plan(glong out[4]) {
     const gli::ContractStats& st = gli::last_stats();
     out[0] = st.keys_a;

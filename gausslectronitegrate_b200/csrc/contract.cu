@@ -312,22 +312,25 @@ __device__ __forceinline__ uint64_t class_packed(const uint64_t* __restrict__ ke
 }
 
 // Sorted axis keys s0 <= s1 <= s2 of ERI class x through the pair
-// descriptors; (hi, da) carry the point pair (i, j) and its descriptor from
-// the previous class of the same thread (hi all ones: none), reused while the
-// remainder stays below N^2.  False for an index outside the tensor.
-__device__ __forceinline__ bool pd_class_keys(const ClassDecode& d, int64_t x, uint64_t& hi, uint2& da, int& s0,
+// descriptors; (base, da) carry the first index of the point pair (i, j) of
+// the previous class of the same thread (its quotient by N^2 times N^2;
+// PD_NO_BASE: none) and that pair's descriptor, reused while the remainder
+// stays below N^2.  False for an index outside the tensor.
+constexpr uint64_t PD_NO_BASE = (uint64_t)1 << 63;  // u - PD_NO_BASE >= 2^63 > N^2 for every index u < 2^63
+__device__ __forceinline__ bool pd_class_keys(const ClassDecode& d, int64_t x, uint64_t& base, uint2& da, int& s0,
                                               int& s1, int& s2) {
     if (x < 0) return false;
     const uint64_t u = (uint64_t)x, N2 = d.N2;
-    if (hi == ~(uint64_t)0 || u - hi * N2 >= N2) {
-        hi = div_est(u, N2, d.invN2);
+    if (u - base >= N2) {
+        const uint64_t hi = div_est(u, N2, d.invN2);
         if (hi >= N2) {
-            hi = ~(uint64_t)0;
+            base = PD_NO_BASE;
             return false;
         }
+        base = hi * N2;
         da = __ldg(&d.pd[hi]);
     }
-    const uint32_t lo = (uint32_t)u - (uint32_t)hi * (uint32_t)N2;
+    const uint32_t lo = (uint32_t)(u - base);
     const uint2 db = __ldg(&d.pd[lo]);
     const int L2m1 = 2 * (int)d.L - 1;
     const int k0 = pd_axis_key(da.x & 0xffffu, db.x & 0xffffu, L2m1);
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_
 #pragma unroll
             for (int v = 0; v < 4; ++v) c[v] = n0 + v < m ? __ldg(&idx[n0 + v]) : 0;
         }
-        uint64_t hi = ~(uint64_t)0;
+        uint64_t base = PD_NO_BASE;
         uint2 da = make_uint2(0, 0);
         int last_slot = -1;
         uint64_t kv[4];
@@ -390,7 +393,7 @@ __global__ void __launch_bounds__(256) k_mark_eri_pd(ClassDecode d, const int64_
             kv[v] = BAD_KEYS;
             if (n0 + v >= m) continue;
             int s0, s1, s2;
-            if (!pd_class_keys(d, c[v], hi, da, s0, s1, s2)) {
+            if (!pd_class_keys(d, c[v], base, da, s0, s1, s2)) {
                 atomicOr(bad, 1);
                 continue;
             }
@@ -881,7 +884,6 @@ struct ProductOp {
     const PlanCounts* cnt;
     i64 m;
     int choice, U, Up, ldq, u_chunk;
-    i64 part_stride;
     double* Q;
     unsigned long long* products;  // count of the products computed (one add per tile)
     struct Block {
@@ -906,7 +908,7 @@ struct ProductOp {
         b.u0 = blockIdx.z * u_chunk;
         b.u1 = min(U, b.u0 + u_chunk);
         b.nk = (b.u1 - b.u0 + DM_BK - 1) / DM_BK;
-        b.Q = Q + (i64)blockIdx.z * part_stride;
+        b.Q = Q;
         if (threadIdx.x == 0 && blockIdx.z == 0) atomicAdd(products, (unsigned long long)b.mvalid * b.nvalid);
         return b.nk > 0;
     }
@@ -953,8 +955,8 @@ struct ProductOp {
 };
 
 // val[n] = Q[pair(n)][kid(k3)], the class's (pair, key) found from its packed
-// keys, summed over the `parts` slices of Q in order (deterministic)
-__global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, int parts, i64 part_stride,
+// keys
+__global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, i64 nq,
                                                    const uint64_t* __restrict__ keys, ClassDecode dec,
                                                    const int64_t* __restrict__ idx, i64 m,
                                                    const uint64_t* __restrict__ kid, int nk,
@@ -1010,10 +1012,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 acc[h][v] = 0.0;
-                if (q[h][v] >= 0 && dcheck(q[h][v] < part_stride, 3, q[h][v])) {
-                    acc[h][v] = Q[q[h][v]];
-                    for (int z = 1; z < parts; ++z) acc[h][v] += Q[z * part_stride + q[h][v]];
-                }
+                if (q[h][v] >= 0 && dcheck(q[h][v] < nq, 3, q[h][v])) acc[h][v] = Q[q[h][v]];
             }
 #pragma unroll
         for (int h = 0; h < G; ++h) {
@@ -1042,7 +1041,7 @@ __global__ void __launch_bounds__(256) k_gather_q(const double* __restrict__ Q, 
 // saves the mark pass's read of the indices and the write and re-read of the
 // packed keys (24 bytes per class).
 template <bool PD>
-__global__ void __launch_bounds__(256, PD ? 8 : 6) k_gather_q_plan(const double* __restrict__ Q, int parts, i64 part_stride,
+__global__ void __launch_bounds__(256, PD ? 8 : 6) k_gather_q_plan(const double* __restrict__ Q, int nq,
                                                         ClassDecode dec, const int64_t* __restrict__ idx, i64 m,
                                                         const uint32_t* __restrict__ kk, int nk,
                                                         const uint2* __restrict__ bitpre, int ldq,
@@ -1069,20 +1068,20 @@ __global__ void __launch_bounds__(256, PD ? 8 : 6) k_gather_q_plan(const double*
                 for (int v = 0; v < 4; ++v) c[h][v] = n0 + v < m ? __ldg(&idx[n0 + v]) : 0;
             }
         }
-        i64 q[G][4];
+        int q[G][4];
 #pragma unroll
         for (int h = 0; h < G; ++h) {
             const i64 n0 = 4 * (g0 + h * stride);
-            uint64_t hi = ~(uint64_t)0;
+            uint64_t base = PD_NO_BASE;
             uint2 da = make_uint2(0, 0);
-            i64 last_slot = -1, last_pid = -1;
+            int last_slot = -1, last_pid = -1;
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 q[h][v] = -1;
                 if (n0 + v >= m) continue;
                 int s0, s1, s2;
                 if constexpr (PD) {
-                    if (!pd_class_keys(dec, c[h][v], hi, da, s0, s1, s2)) {
+                    if (!pd_class_keys(dec, c[h][v], base, da, s0, s1, s2)) {
                         miss = true;
                         continue;
                     }
@@ -1095,19 +1094,19 @@ __global__ void __launch_bounds__(256, PD ? 8 : 6) k_gather_q_plan(const double*
                     s0 = k[0], s1 = k[1], s2 = k[2];
                 }
                 if (!dcheck(s0 >= 0 && s2 < nk, 1, s2)) continue;
-                const i64 slot = (i64)s1 * nk + s0;
+                const int slot = s1 * nk + s0;
                 if (slot != last_slot) {
                     last_slot = slot;
                     const uint2 bp = __ldg(&bitpre[slot >> 5]);  // (bits, pairs before the word)
                     const uint32_t bit = (uint32_t)(slot & 31);
-                    last_pid = (bp.x >> bit) & 1u ? (i64)bp.y + __popc(bp.x & ((1u << bit) - 1u)) : -1;
+                    last_pid = (bp.x >> bit) & 1u ? (int)(bp.y + __popc(bp.x & ((1u << bit) - 1u))) : -1;
                 }
                 const uint32_t k0 = __ldg(&kk[s2]);  // key id, bit 31: a key the list uses
                 if (last_pid < 0 || !(k0 >> 31)) {
                     miss = true;
                     continue;
                 }
-                q[h][v] = last_pid * ldq + (i64)(k0 & 0x7fffffffu);
+                q[h][v] = last_pid * ldq + (int)(k0 & 0x7fffffffu);  // (Q has fewer than 2^31 entries)
             }
         }
         double acc[G][4];
@@ -1116,10 +1115,7 @@ __global__ void __launch_bounds__(256, PD ? 8 : 6) k_gather_q_plan(const double*
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 acc[h][v] = 0.0;
-                if (q[h][v] >= 0 && dcheck(q[h][v] < part_stride, 3, q[h][v])) {
-                    acc[h][v] = Q[q[h][v]];
-                    for (int z = 1; z < parts; ++z) acc[h][v] += Q[z * part_stride + q[h][v]];
-                }
+                if (q[h][v] >= 0 && dcheck(q[h][v] < nq, 3, q[h][v])) acc[h][v] = Q[q[h][v]];
             }
 #pragma unroll
         for (int h = 0; h < G; ++h) {
@@ -1746,8 +1742,7 @@ static bool sized_plan_fits(i64 nk) { return nk <= PLAN_SMALL_KEYS && (nk * nk +
 // kept plan, its products Q, its status block).
 struct GatherLaunch {
     const double* Q = nullptr;
-    int parts = 0;
-    i64 part_stride = 0;
+    i64 nq = 0;  // entries of Q
     ClassDecode dec;
     const uint32_t* kk = nullptr;
     int nk = 0;
@@ -1760,12 +1755,13 @@ struct GatherLaunch {
 static void launch_gather(const GatherLaunch& gl, const int64_t* idx, i64 m, double* out, int num_sms,
                           cudaStream_t s) {
     if (m <= 0) return;
+    if (gl.nq >= ((i64)1 << 31)) fail(GLI_ERR_INTERNAL, "class gather over %lld products", (long long)gl.nq);
     const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)num_sms * 8);
     if (gl.dec.pd)
-        launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, gl.Q, gl.parts, gl.part_stride, gl.dec, idx, m,
+        launch_kernel(k_gather_q_plan<true>, dim3(gq), dim3(256), 0, s, gl.Q, (int)gl.nq, gl.dec, idx, m,
                       gl.kk, gl.nk, gl.bitpre, gl.ldq, gl.cnt, out);
     else
-        launch_kernel(k_gather_q_plan<false>, dim3(gq), dim3(256), 0, s, gl.Q, gl.parts, gl.part_stride, gl.dec, idx,
+        launch_kernel(k_gather_q_plan<false>, dim3(gq), dim3(256), 0, s, gl.Q, (int)gl.nq, gl.dec, idx,
                       m, gl.kk, gl.nk, gl.bitpre, gl.ldq, gl.cnt, out);
 }
 
@@ -2155,16 +2151,16 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         if (P < 1 || !Q.p) fail(GLI_ERR_INTERNAL, "stage C product without its buffer");
         // (a split sums its parts inside a cluster of the P blocks of a tile)
         dmma_launch_cluster(ProductOp<64>{H2.p, t.W.p, keyOf.p, pairA.p, aKey.p, ids.p, cnt, m, c_prod, U, Up,
-                                          (int)nku, u_chunk, 0, Q.p, &st->products},
+                                          (int)nku, u_chunk, Q.p, &st->products},
                             dim3((unsigned)mt, (unsigned)nt, (unsigned)P), s);
+        timer.mark();  // (the class-level kernels of stage C start here)
         t_enq_paths |= (fused ? 2 : 1) << 2;  // the class gather that ran
         if (fused) {
             // (the kept plan's packed lookups: this replay's pair bitmap stays
             // empty when the mark pass skipped)
             GatherLaunch gl;
             gl.Q = Q.p;
-            gl.parts = 1;
-            gl.part_stride = ps;
+            gl.nq = ps;
             gl.dec = dec;
             gl.kk = pstore->kk.p;
             gl.nk = (int)nk;
@@ -2177,11 +2173,12 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                 launch_gather(gl, a.idx, m, a.out, a.num_sms, s);
         } else {
             const unsigned gq = (unsigned)std::min<i64>(((m + 3) / 4 + 255) / 256, (i64)a.num_sms * 8);
-            launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, 1, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
+            launch_kernel(k_gather_q, dim3(gq), dim3(256), 0, s, Q.p, ps, keys.p, dec, a.idx, m, ids.p, (int)nk,
                           pairBits.p, pairPre.p, (int)nku, cnt, c_prod, a.out);
         }
     }
     if (undecided || !product_host) {
+        if (!undecided) timer.mark();  // (no product GEMM: the class-level kernel starts stage C)
         const i64 want = (m + 7) / 8;
         const unsigned gc = (unsigned)(want < (i64)a.num_sms * 16 ? want : (i64)a.num_sms * 16);
         launch_kernel(k_stage_c, dim3(gc), dim3(256), 0, s, t.W.p, H2.p, keys.p, dec, a.idx, (int)nk, pairBits.p, pairPre.p, m, U, Up,
@@ -2515,7 +2512,9 @@ static void check_status(int kind, i64 m, const EvalStatus& h, const LatticeTabl
         const int b = t_graph_timer ? 0 : 2;
         st.ms_a = g.between(b, b + 1);
         st.ms_b = g.between(b + 1, b + 2);
-        st.ms_c = g.between(b + 2, b + 3);
+        st.ms_c = g.between(b + 2, b + 4);
+        st.ms_c_product = g.between(b + 2, b + 3);
+        st.ms_c_class = g.between(b + 3, b + 4);
     }
     t_last = st;
     if (stats) *stats = st;

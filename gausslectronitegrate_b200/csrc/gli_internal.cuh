@@ -167,6 +167,9 @@ struct ContractStats {
     double screen_tol = 0;    // the product threshold the tables were built with (mixed form: screened)
     double screen_bound = 0;  // bound on the change of a class value by that screening (grid units)
     float ms_tables = 0, ms_a = 0, ms_b = 0, ms_c = 0;
+    // stage C in two parts: the (pair, key) product GEMM (0 when stage C ran
+    // per class) and the class-level kernel (the gather, or the per-class dots)
+    float ms_c_product = 0, ms_c_class = 0;
 };
 
 // drops the calling thread's captured evaluations and every cached table set

@@ -429,6 +429,11 @@ int gli_b200_dgemm_sliced_dev(const double* d_A, glong lda, const double* d_B, g
 int gli_b200_kinetic_matrix_noalloc(const double* d_coeffs, glong num_coeffs,
 	const struct cartesian_grid_3d* grid, double* d_matrix, void* stream);
 int gli_b200_last_stage_times(float ms[4], glong sizes[3]);
+/* Stage C of the same evaluation in two parts (ms, filled under
+ * gli_b200_set_timing(1)): ms[0] the (pair, key) product GEMM (0 when stage C
+ * ran per class), ms[1] the class-level kernel that followed it (the class
+ * gather, or the per-class dot products).  No reference counterpart. */
+int gli_b200_last_stage_c_times(float ms[2]);
 
 /* Plan of the calling thread's last sparse evaluation: out[0] A keys, out[1]
  * (A, B) key pairs, out[2] distinct axis keys, out[3] the (pair, key) products

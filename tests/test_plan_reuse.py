@@ -182,3 +182,43 @@ def test_pinned_host_lists_pipeline(gli):
     for k in range(4):
         assert run() == 0, L.gli_b200_last_error_message().decode()
         assert_parity(out.numpy(), refs[1], what=f"pinned second half, call {k}")
+
+
+@pytest.mark.parametrize("case", ["eri7", "erida33"])
+def test_stage_times_split_stage_c(gli, case):
+    # with timing on, the stage times of graph replays are their own event
+    # marks; stage C is the product GEMM (ERI 7^3; at ERIDA 33^3 the device
+    # chooses the per-class dots) followed by the class-level kernel
+    import torch
+
+    from gausslectronitegrate_b200 import _abi
+    from gausslectronitegrate_b200 import workloads as W
+    kind, grid_of = CASES[case]
+    grid = grid_of(W)
+    L = gli.lib()
+    gs = gli._grid_struct(grid)
+    d_idx, m = C.c_void_p(), _abi.glong()
+    assert L.gli_b200_enumerate_dev(kind, C.byref(gs), C.byref(d_idx), C.byref(m), None) == 0
+    b = np.ascontiguousarray(g10())
+    d_out = torch.empty(m.value, dtype=torch.float64, device="cuda")
+    L.gli_b200_set_timing(1)
+    try:
+        for _ in range(3):
+            rc = L.gli_b200_sparse_values_dev(kind, b.ctypes.data_as(_abi.dptr), b.size, C.byref(gs),
+                                              d_idx, m.value, 1e-16, _abi.GLI_FORM_FP64,
+                                              C.c_void_p(d_out.data_ptr()), None)
+            assert rc == 0, L.gli_b200_last_error_message().decode()
+        ms4, sz3, ms2 = (C.c_float * 4)(), (_abi.glong * 3)(), (C.c_float * 2)()
+        L.gli_b200_last_stage_times(ms4, sz3)
+        L.gli_b200_last_stage_c_times(ms2)
+        plan = (_abi.glong * 4)()
+        L.gli_b200_last_plan(plan)
+    finally:
+        L.gli_b200_set_timing(0)
+        L.gli_b200_free_dev(d_idx, None)
+    assert all(ms4[k] > 0 for k in range(1, 4)), list(ms4)
+    assert ms2[1] > 0 and ms2[0] >= 0
+    # (a bounded plan that the host bounds leave undecided queues both stage-C
+    # paths: the product GEMM then launches and returns at once)
+    assert ms2[0] > 0 or plan[3] == 0, (list(ms2), list(plan))
+    assert abs(ms4[3] - (ms2[0] + ms2[1])) <= 1e-3 + 1e-3 * ms4[3], (list(ms4), list(ms2))
