@@ -234,6 +234,26 @@ struct PlanCounts {
     int64_t overflow;
 };
 
+// The counts of a trusted replay: those of the kept plan when it is valid,
+// else none and the overflow flag (the host then evaluates again, exactly)
+__device__ __forceinline__ void restore_counts(bool valid, const PlanCounts* __restrict__ saved,
+                                               PlanCounts* __restrict__ cnt) {
+    if (valid) {
+        const PlanCounts c = *saved;
+        cnt->key_total = c.key_total;
+        cnt->nku = c.nku;
+        cnt->nA = c.nA;
+        cnt->nP = c.nP;
+        cnt->overflow = 0;
+    } else {
+        cnt->key_total = 0;
+        cnt->nku = 0;
+        cnt->nA = 0;
+        cnt->nP = 0;
+        cnt->overflow = 1;
+    }
+}
+
 // Decodes every class once (its packed keys are kept for the later passes)
 // and marks the keys it uses (any role: usedKey; as A = k2: usedA) and its
 // (A, B) = (k2, k1) key pair (bit k2 * nk + k1 of pairBits).  Millions of
@@ -598,6 +618,13 @@ struct StageAOp {
     double* ws = nullptr;
     unsigned* tickets = nullptr;
     static constexpr bool TAIL_SPLIT = true;
+    // trusted replays (restore_valid non-null; 64- and 80-column tiles): the
+    // first block restores the kept plan's counts into cnt for the later
+    // kernels (k_restore_plan's work, one launch fewer), and every block reads
+    // the kept counts
+    const int* restore_valid = nullptr;
+    const PlanCounts* restore_from = nullptr;
+    PlanCounts* restore_to = nullptr;
     __device__ int split_half() const {
         return ws && (int)blockIdx.x >= nfull ? (int)((blockIdx.x - nfull) & 1) : -1;
     }
@@ -615,7 +642,15 @@ struct StageAOp {
         Off off[NB];  // aKey * Up of this thread's rows, -1 past nA
     };
     __device__ bool begin(Block& b) const {
-        const int nA = (int)cnt->nA;
+        const PlanCounts* c = cnt;
+        if (BN_ <= 80 && restore_valid) {
+            const bool valid = *restore_valid != 0;
+            if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0)
+                restore_counts(valid, restore_from, restore_to);
+            if (!valid) return false;
+            c = restore_from;
+        }
+        const int nA = (int)c->nA;
         b.n0 = blockIdx.y * BN;
         if (b.n0 >= nA) return false;  // grids are sized by a bound on nA
         const int half = split_half();
@@ -1574,20 +1609,7 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
 // checks every class against the kept plan (k_gather_q_plan).
 __global__ void k_restore_plan(PlanReuse reuse, PlanCounts* __restrict__ cnt) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (*reuse.valid) {
-        const PlanCounts c = *reuse.saved_cnt;
-        cnt->key_total = c.key_total;
-        cnt->nku = c.nku;
-        cnt->nA = c.nA;
-        cnt->nP = c.nP;
-        cnt->overflow = 0;
-    } else {
-        cnt->key_total = 0;
-        cnt->nku = 0;
-        cnt->nA = 0;
-        cnt->nP = 0;
-        cnt->overflow = 1;
-    }
+    restore_counts(*reuse.valid != 0, reuse.saved_cnt, cnt);
 }
 
 // G sliced once per table set (cached with the tables); the build synchronises
@@ -1966,8 +1988,13 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
                           lb ? 1 : 0, fused ? (const int*)pstore->valid.p : (const int*)nullptr);
         }
     }
+    // (a trusted replay whose stage A runs on the FP64 tensor-core GEMM in 64-
+    // or 80-column tiles restores the kept counts in that kernel; the
+    // 144-column tiles have no registers to spare for it)
+    const bool restore_in_a = plan_small && trusted && !(a.mixed && sz.nA * (i64)nS >= tc_a_outputs()) &&
+                              !(sz.nA > 128 && sz.nA <= 144);
     if (plan_small && trusted) {
-        launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), cnt);
+        if (!restore_in_a) launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), cnt);
         tiles.built = true;
     } else if (plan_small) {
         launch_kernel(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
@@ -2014,6 +2041,8 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     // the mixed form runs a stage on the tensor cores when it is large enough for
     // them to pay off; smaller stages (latency-bound either way) stay FP64
     const bool tc_a = a.mixed && nA * (i64)nS >= tc_a_outputs();
+    if (restore_in_a && (tc_a || (nA > 128 && nA <= 144)))
+        fail(GLI_ERR_INTERNAL, "trusted replay: stage A changed path after the plan");
     const bool tc_b = stage_b_sliced(a.mixed, nA, nP, U);
     DevBuf<double>& H2 = sb.H2;
     t_enq_paths = (tc_a ? 1 : 0) | (tc_b ? 2 : 0);
@@ -2043,6 +2072,16 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         int t_chunk = U;
         const int P = bn == 144 ? 1 : split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
         const dim3 grid(mb, nb, (unsigned)P);
+        if (restore_in_a && (mb == 0 || nb == 0))  // (no stage-A block would restore the counts)
+            launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), cnt);
+        auto restoring = [&](auto op) {
+            if (restore_in_a && mb > 0 && nb > 0) {
+                op.restore_valid = pstore->valid.p;
+                op.restore_from = pstore->saved_cnt.p;
+                op.restore_to = cnt;
+            }
+            return op;
+        };
         if (bn == 144) {
             // one 144-column tile; a last wave under half full split in K
             // (stage_a_tail)
@@ -2057,9 +2096,11 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
             dmma_launch(op, g, s);
         } else if (bn == 80) {
             // a split sums its parts inside a cluster of the P blocks of a tile
-            dmma_launch_cluster(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}, grid, s);
+            dmma_launch_cluster(restoring(StageAOp<80>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}),
+                                grid, s);
         } else {
-            dmma_launch_cluster(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}, grid, s);
+            dmma_launch_cluster(restoring(StageAOp<64>{t.W.p, t.T.p, t.S.p, aKey.p, cnt, nS, U, Up, t_chunk, 0, H.p}),
+                                grid, s);
         }
     }
     timer.mark();
