@@ -209,19 +209,26 @@ __global__ void __launch_bounds__(256) k_fill_slab_keyed(const short4* __restric
 // thread keeps its row (j, k) and walks l), B (the basis, at most 32 columns)
 // read row-major.  A row tile (rows of one j) starts its K loop at the chunk
 // of its smallest k, the elements below each row's k staged as zeros.
+//
+// One launch covers the pairs g0 <= g < g1 of the packed order
+// g = i (i + 1) / 2 + j (j <= i), several slabs at once: slab by slab, the
+// launches of the small slabs (a few tiles) left most of the GPU idle and
+// every launch ended on a partial wave.  Rows of pair g are
+// A1[(g - g0) N + k].
 struct KeyedSlabOp {
     static constexpr bool A_KMAJOR = true, B_KMAJOR = false;
     static constexpr int BN = 32;
     const short4* pt;  // points of the grid
     const double* table;
     const double* basis;  // N x M row-major
-    double* C;            // N^2 x M row-major
-    short4 pi;
+    double* C;            // (g1 - g0) N x M row-major
     int N, L, M;
-    int rows;  // rows (j k) computed: j < rows / N
+    int g0, g1;  // packed pairs (i, j <= i) of this launch
     struct Block {
         int mvalid, nvalid, nk;
         int m0, kc0;
+        int j, k0;
+        short4 pi;
     };
     struct AState {
         int d[3], s[3], k[3];  // pi - pj, pi + pj, pk per axis of this thread's row
@@ -229,15 +236,23 @@ struct KeyedSlabOp {
         bool ok;
     };
     struct BState {};
-    // row tiles never straddle two j: tile t holds rows (j, k0 .. k0 + 63) of
-    // j = t / tpj, k0 = 64 (t % tpj), tpj = ceil(N / 64) tiles per j
+    // row tiles never straddle two pairs: tile t holds rows (k0 .. k0 + 63) of
+    // pair g = g0 + t / tpj, k0 = 64 (t % tpj), tpj = ceil(N / 64) tiles per pair
     __device__ bool begin(Block& b) const {
-        const int tpj = (N + DM_BM - 1) / DM_BM, j = blockIdx.x / tpj;
-        const int k0 = (blockIdx.x - j * tpj) * DM_BM;
-        b.m0 = j * N + k0;
-        b.mvalid = min(DM_BM, N - k0);
-        if (b.m0 >= rows || b.mvalid <= 0) return false;
-        b.kc0 = k0 / DM_BK;  // l >= k >= k0: the chunks below are zero
+        const int tpj = (N + DM_BM - 1) / DM_BM, t = (int)(blockIdx.x / tpj);
+        const int g = g0 + t;
+        if (g >= g1) return false;
+        // i = the largest integer with i (i + 1) / 2 <= g
+        int i = (int)((sqrt(8.0 * (double)g + 1.0) - 1.0) * 0.5);
+        while ((i64)(i + 1) * (i + 2) / 2 <= g) ++i;
+        while ((i64)i * (i + 1) / 2 > g) --i;
+        b.j = g - i * (i + 1) / 2;
+        b.pi = pt[i];
+        b.k0 = (blockIdx.x - t * tpj) * DM_BM;
+        b.m0 = t * N + b.k0;
+        b.mvalid = min(DM_BM, N - b.k0);
+        if (b.mvalid <= 0) return false;
+        b.kc0 = b.k0 / DM_BK;  // l >= k >= k0: the chunks below are zero
         b.nvalid = min(BN, M);
         b.nk = (N + DM_BK - 1) / DM_BK - b.kc0;
         return true;
@@ -245,8 +260,8 @@ struct KeyedSlabOp {
     __device__ void a_init(const Block& b, AState& st) const {
         const int r = dm_kmajor_row(threadIdx.x);
         st.ok = r < b.mvalid;
-        const int row = st.ok ? b.m0 + r : 0, j = row / N, k = row - j * N;
-        const short4 pj = pt[j], pk = pt[k];
+        const int k = st.ok ? b.k0 + r : 0;
+        const short4 pi = b.pi, pj = pt[b.j], pk = pt[k];
         st.d[0] = pi.x - pj.x, st.d[1] = pi.y - pj.y, st.d[2] = pi.z - pj.z;
         st.s[0] = pi.x + pj.x, st.s[1] = pi.y + pj.y, st.s[2] = pi.z + pj.z;
         st.k[0] = pk.x, st.k[1] = pk.y, st.k[2] = pk.z;
@@ -617,17 +632,20 @@ __global__ void k_mirror_pairs(double* __restrict__ W, i64 n, i64 mm) {
     }
 }
 
-// W[i][j] = Y + Y^T for the M x M blocks Y (M <= 32) of the pairs j <= i, and
-// W[j][i] = W[i][j]: one block per pair (blockIdx.y = i, blockIdx.x = j), Y
-// read once into shared memory, the sums written row by row (coalesced)
-__global__ void __launch_bounds__(256) k_symmetrize_pairs(double* __restrict__ W, i64 n, int M) {
+// W[i][j] = Y + Y^T for the M x M blocks Y (M <= 32) of the pairs j <= i
+// (packed: Y[i (i + 1) / 2 + j]), and W[j][i] = W[i][j]: one block per pair
+// (blockIdx.y = i, blockIdx.x = j), Y read once into shared memory, the sums
+// written row by row (coalesced)
+__global__ void __launch_bounds__(256) k_symmetrize_pairs(const double* __restrict__ Y, double* __restrict__ W, i64 n,
+                                                          int M) {
     __shared__ double y[32 * 33];
     const i64 i = blockIdx.y, j = blockIdx.x;
     if (j > i) return;
     const i64 mm = (i64)M * M;
-    double* blk = W + (i * n + j) * mm;
-    for (int e = threadIdx.x; e < M * M; e += blockDim.x) y[(e / M) * 33 + e % M] = blk[e];
+    const double* yg = Y + (i * (i + 1) / 2 + j) * mm;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) y[(e / M) * 33 + e % M] = yg[e];
     __syncthreads();
+    double* blk = W + (i * n + j) * mm;
     double* mir = W + (j * n + i) * mm;
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
         const int r = e / M, c = e - r * M;
@@ -716,39 +734,58 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     // copied; then A3[i] = B^T W[i] and E = B^T A3.  The generated entries and
     // the dominant first contraction are halved.
     const i64 Nx2 = Nx * Nx, MM = M * M;
-    DevBuf<double> A1(Nx2 * M, s), W(Nx2 * MM, s), A3(Nx * MM * M, s), S;
+    DevBuf<double> W(Nx2 * MM, s), A3(Nx * MM * M, s), S;
     // the first contraction with its slab computed as the GEMM stages it (at
     // most 32 orbitals), or from a filled slab
     const bool fused = slab32 && M <= 32;
-    if (!fused) S.alloc(Nx2 * Nx, s);
-    for (i64 i = 0; i < Nx; ++i) {
-        const i64 rows = (i + 1) * Nx;  // (j k) with j <= i
-        if (fused) {
-            const i64 tpj = (Nx + DM_BM - 1) / DM_BM;  // row tiles per j
-            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, bx, A1.p, hpt[i], (int)Nx, (int)G.L, (int)M, (int)rows},
-                        dim3((unsigned)((i + 1) * tpj)), s);
-        } else {
-            if (slab32)
-                k_fill_slab_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p,
-                                                                      (uint32_t)(rows * Nx), S.p);
-            else if (kt.ok)
-                k_fill_eri_rows_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(D, kt.t.p, G.L, i * N, i + 1, S.p);
-            else
-                k_fill_eri_rows<<<grid_for(rows * Nx), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, i + 1, S.p);
-            GLI_CHECK_LAUNCH();
-            // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-            dgemm((int)rows, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false,
-                  s);
+    if (fused) {
+        // The pairs (i, j <= i) in packed order g = i (i + 1) / 2 + j, as many
+        // slabs per launch as A1 holds (1 GB, at least one whole slab; at most
+        // 65,535 pairs, the batched GEMM's grid.z): the first contraction
+        // A1[g] = U[i j] B, then Y[g] = B^T A1[g], one batched GEMM per launch
+        // (the 216-point projection: two launches of each instead of 216).
+        const i64 pairs = Nx * (Nx + 1) / 2, tpj = (Nx + DM_BM - 1) / DM_BM;
+        const i64 cap = std::min<i64>(65535, std::max<i64>(Nx, ((i64)1 << 30) / (Nx * M * (i64)sizeof(double))));
+        const i64 launches = (pairs + cap - 1) / cap, per = (pairs + launches - 1) / launches;
+        if (pairs >= ((i64)1 << 31) || per * tpj >= ((i64)1 << 31) || per * Nx * M >= ((i64)1 << 31))
+            fail(GLI_ERR_LIMIT, "projection over %lld points exceeds the slab launch range", (long long)Nx);
+        DevBuf<double> A1(per * Nx * M, s), Y(pairs * MM, s);
+        for (i64 g0 = 0; g0 < pairs; g0 += per) {
+            const i64 g1 = std::min(pairs, g0 + per);
+            dmma_launch(KeyedSlabOp{pt.p, kt.t.p, bx, A1.p, (int)Nx, (int)G.L, (int)M, (int)g0, (int)g1},
+                        dim3((unsigned)((g1 - g0) * tpj)), s);
+            // Y[g] = B^T A1[g]   (batch g0 <= g < g1)
+            dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, Y.p + g0 * MM, MM, M, 1,
+                  (int)(g1 - g0), false, s);
         }
+        // W[i][j] = Y + Y^T, and the mirror W[j][i]
+        k_symmetrize_pairs<<<dim3((unsigned)Nx, (unsigned)Nx), 256, 0, s>>>(Y.p, W.p, Nx, (int)M);
+        GLI_CHECK_LAUNCH();
+    } else {
+        S.alloc(Nx2 * Nx, s);
+    }
+    DevBuf<double> A1;
+    if (!fused) A1.alloc(Nx2 * M, s);
+    for (i64 i = 0; !fused && i < Nx; ++i) {
+        const i64 rows = (i + 1) * Nx;  // (j k) with j <= i
+        if (slab32)
+            k_fill_slab_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p,
+                                                                  (uint32_t)(rows * Nx), S.p);
+        else if (kt.ok)
+            k_fill_eri_rows_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(D, kt.t.p, G.L, i * N, i + 1, S.p);
+        else
+            k_fill_eri_rows<<<grid_for(rows * Nx), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, i + 1, S.p);
+        GLI_CHECK_LAUNCH();
+        // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
+        dgemm((int)rows, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false, s);
         // W[i][j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j <= i)
         dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, W.p + i * Nx * MM, MM, M, 1,
               (int)(i + 1), false, s);
     }
-    if (fused)  // the fused slabs gave Y = B^T U B: W = Y + Y^T, then the mirror
-        k_symmetrize_pairs<<<dim3((unsigned)Nx, (unsigned)Nx), 256, 0, s>>>(W.p, Nx, (int)M);
-    else
+    if (!fused) {
         k_mirror_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, MM);
-    GLI_CHECK_LAUNCH();
+        GLI_CHECK_LAUNCH();
+    }
     // A3[i][q][(r s)] = sum_j B[j][q] W[i][j][(r s)]   (batch i)
     dgemm((int)M, (int)MM, (int)Nx, MatView{bx, 0, 1, M}, MatView{W.p, Nx * MM, MM, 1}, A3.p, MM * M, MM, 1,
           (int)Nx, false, s);
