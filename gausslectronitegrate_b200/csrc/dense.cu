@@ -15,8 +15,8 @@
 // semantics for arbitrary (also loaded or hand-made) sparse lists.  The
 // projections contract one tensor axis at a time (the factored form the
 // reference tests use as their check, test/test_eri_integrals.c:188-212)
-// instead of the O(N^4 M^4) atomic loop, slab by slab over the first index so
-// that the dense tensor is never held whole.
+// instead of the O(N^4 M^4) atomic loop, over slabs of the first index (or
+// batches of index pairs) so that the dense tensor is never held whole.
 //
 // Complete class lists.  When an ERI list holds every canonical class of its
 // grid (the count matches the enumeration, the indices increase strictly and
@@ -108,6 +108,11 @@ __global__ void k_fill_eri_rows(SymGrid G, DenseGrid D, const int64_t* __restric
 __host__ __device__ inline i64 tetra_index(i64 k1, i64 k2, i64 k3) {  // k1 <= k2 <= k3
     return k3 * (k3 + 1) * (k3 + 2) / 6 + k2 * (k2 + 1) / 2 + k1;
 }
+// the same in 32-bit arithmetic, for key tables of at most 2^29 slots (the
+// only ones built): then k3 (k3 + 1) (k3 + 2) <= 6 * 2^29 < 2^32
+__device__ __forceinline__ uint32_t tetra_index32(uint32_t k1, uint32_t k2, uint32_t k3) {
+    return k3 * (k3 + 1) * (k3 + 2) / 6u + k2 * (k2 + 1) / 2u + k1;
+}
 
 __device__ inline i64 eri_key_slot(const int p[4][3], i64 L) {
     i64 k[3];
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(256) k_fill_slab_keyed(const short4* __restric
         if (a > b) { const int t = a; a = b; b = t; }
         if (b > c) { const int t = b; b = c; c = t; }
         if (a > b) { const int t = a; a = b; b = t; }
-        S[e] = table[tetra_index(a, b, c)];
+        S[e] = table[tetra_index32(a, b, c)];
     }
 }
 
@@ -282,7 +287,7 @@ struct KeyedSlabOp {
                 if (a > c) { const int t = a; a = c; c = t; }
                 if (c > e) { const int t = c; c = e; e = t; }
                 if (a > c) { const int t = a; a = c; c = t; }
-                src = table + tetra_index(a, c, e);
+                src = table + tetra_index32(a, c, e);
             }
             dm_cp8(tile + dm_kmajor_at(r, kq), src, v);
         }
