@@ -254,6 +254,25 @@ __device__ __forceinline__ void restore_counts(bool valid, const PlanCounts* __r
     }
 }
 
+// an evaluation's status block: its counts and its flags
+struct EvalStatus {
+    PlanCounts cnt;
+    int bad;                      // a class index outside the tensor
+    int tc_err;                   // a tensor-core CTA gave up waiting
+    unsigned long long products;  // (pair, key) products that stage C's product GEMM computed
+};
+
+// The status block of a trusted replay, written whole by its first kernel
+// (such a replay queues no memset of the block): the restored counts, no
+// flags raised and no products counted yet
+__device__ __forceinline__ void restore_status(bool valid, const PlanCounts* __restrict__ saved,
+                                               EvalStatus* __restrict__ st) {
+    restore_counts(valid, saved, &st->cnt);
+    st->bad = 0;
+    st->tc_err = 0;
+    st->products = 0ull;
+}
+
 // Decodes every class once (its packed keys are kept for the later passes)
 // and marks the keys it uses (any role: usedKey; as A = k2: usedA) and its
 // (A, B) = (k2, k1) key pair (bit k2 * nk + k1 of pairBits).  Millions of
@@ -624,7 +643,7 @@ struct StageAOp {
     // the kept counts
     const int* restore_valid = nullptr;
     const PlanCounts* restore_from = nullptr;
-    PlanCounts* restore_to = nullptr;
+    EvalStatus* restore_to = nullptr;
     __device__ int split_half() const {
         return ws && (int)blockIdx.x >= nfull ? (int)((blockIdx.x - nfull) & 1) : -1;
     }
@@ -646,7 +665,7 @@ struct StageAOp {
         if (BN_ <= 80 && restore_valid) {
             const bool valid = *restore_valid != 0;
             if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0)
-                restore_counts(valid, restore_from, restore_to);
+                restore_status(valid, restore_from, restore_to);
             if (!valid) return false;
             c = restore_from;
         }
@@ -1607,9 +1626,9 @@ __global__ void __launch_bounds__(1024) k_plan_small(i64 nk, i64 capA, i64 capP,
 // valid plan be kept, an overflow (the host then evaluates anew).  Such a
 // replay launches neither the mark pass nor the plan kernel; its class gather
 // checks every class against the kept plan (k_gather_q_plan).
-__global__ void k_restore_plan(PlanReuse reuse, PlanCounts* __restrict__ cnt) {
+__global__ void k_restore_plan(PlanReuse reuse, EvalStatus* __restrict__ st) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    restore_counts(*reuse.valid != 0, reuse.saved_cnt, cnt);
+    restore_status(*reuse.valid != 0, reuse.saved_cnt, st);
 }
 
 // G sliced once per table set (cached with the tables); the build synchronises
@@ -1675,13 +1694,6 @@ struct StageTimer {
 };
 
 // status of one evaluation, read back by the host after the last kernel
-struct EvalStatus {
-    PlanCounts cnt;
-    int bad;                      // a class index outside the tensor
-    int tc_err;                   // a tensor-core CTA gave up waiting
-    unsigned long long products;  // (pair, key) products that stage C's product GEMM computed
-};
-
 struct EvalArgs {
     bool mixed = false;
     const LatticeTables* t = nullptr;
@@ -1863,7 +1875,12 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     const LatticeTables& t = *a.t;
     const i64 nk = t.nkeys, m = a.m;
     const int U = (int)t.U, Up = (int)t.Up, nS = (int)t.nS;
-    GLI_CUDA(cudaMemsetAsync(st, 0, sizeof(EvalStatus), s));
+    // A trusted replay of a small plan starts with the kernel that restores
+    // the kept plan, which writes the whole status block (k_restore_plan, or
+    // stage A's first block): no memset node ahead of it
+    const bool restores = trusted && (bounded || mode == PLAN_SIZED) && (nk * nk + 31) / 32 <= 8 * 1024 &&
+                          nk <= PLAN_SMALL_KEYS;
+    if (!restores) GLI_CUDA(cudaMemsetAsync(st, 0, sizeof(EvalStatus), s));
     PlanCounts* cnt = &st->cnt;
     if (bounded) {
         sz.nku = nk;
@@ -1993,8 +2010,9 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
     // 144-column tiles have no registers to spare for it)
     const bool restore_in_a = plan_small && trusted && !(a.mixed && sz.nA * (i64)nS >= tc_a_outputs()) &&
                               !(sz.nA > 128 && sz.nA <= 144);
+    if (restores != (plan_small && trusted)) fail(GLI_ERR_INTERNAL, "trusted replay without its restoring kernel");
     if (plan_small && trusted) {
-        if (!restore_in_a) launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), cnt);
+        if (!restore_in_a) launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), st);
         tiles.built = true;
     } else if (plan_small) {
         launch_kernel(k_plan_small, dim3(1), dim3(1024), 0, s, nk, sz.nA, sz.nP, used.p, ids.p, keyOf.p, aId.p, aKey.p, words,
@@ -2073,12 +2091,12 @@ static void enqueue_eval(const EvalArgs& a, PlanMode mode, EvalStatus* st, Stage
         const int P = bn == 144 ? 1 : split_count((i64)mb * nb, U, DM_BK, DM_SPLIT_TARGET * a.num_sms, &t_chunk);
         const dim3 grid(mb, nb, (unsigned)P);
         if (restore_in_a && (mb == 0 || nb == 0))  // (no stage-A block would restore the counts)
-            launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), cnt);
+            launch_kernel(k_restore_plan, dim3(1), dim3(32), 0, s, pstore->reuse(true), st);
         auto restoring = [&](auto op) {
             if (restore_in_a && mb > 0 && nb > 0) {
                 op.restore_valid = pstore->valid.p;
                 op.restore_from = pstore->saved_cnt.p;
-                op.restore_to = cnt;
+                op.restore_to = st;
             }
             return op;
         };
