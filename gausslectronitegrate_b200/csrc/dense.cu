@@ -739,16 +739,17 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
     // copied; then A3[i] = B^T W[i] and E = B^T A3.  The generated entries and
     // the dominant first contraction are halved.
     const i64 Nx2 = Nx * Nx, MM = M * M;
-    DevBuf<double> W(Nx2 * MM, s), A3(Nx * MM * M, s), S;
+    DevBuf<double> W(Nx2 * MM, s), A3(Nx * MM * M, s);
     // the first contraction with its slab computed as the GEMM stages it (at
     // most 32 orbitals), or from a filled slab
     const bool fused = slab32 && M <= 32;
     if (fused) {
-        // The pairs (i, j <= i) in packed order g = i (i + 1) / 2 + j, as many
-        // slabs per launch as A1 holds (1 GB, at least one whole slab; at most
-        // 65,535 pairs, the batched GEMM's grid.z): the first contraction
-        // A1[g] = U[i j] B, then Y[g] = B^T A1[g], one batched GEMM per launch
-        // (the 216-point projection: two launches of each instead of 216).
+        // The pairs (i, j <= i) in packed order g = i (i + 1) / 2 + j, split
+        // evenly over launches of as many pairs as a 1 GB A1 holds (at least
+        // Nx, at most 65,535: the batched GEMM's grid.z): the first
+        // contraction A1[g] = U[i j] B, then Y[g] = B^T A1[g], one batched GEMM
+        // per launch (the 216-point projection: two launches of each instead
+        // of one per slab).
         const i64 pairs = Nx * (Nx + 1) / 2, tpj = (Nx + DM_BM - 1) / DM_BM;
         const i64 cap = std::min<i64>(65535, std::max<i64>(Nx, ((i64)1 << 30) / (Nx * M * (i64)sizeof(double))));
         const i64 launches = (pairs + cap - 1) / cap, per = (pairs + launches - 1) / launches;
@@ -767,27 +768,25 @@ void project_device(int kind, const GridDesc& g, const int64_t* d_idx, const dou
         k_symmetrize_pairs<<<dim3((unsigned)Nx, (unsigned)Nx), 256, 0, s>>>(Y.p, W.p, Nx, (int)M);
         GLI_CHECK_LAUNCH();
     } else {
-        S.alloc(Nx2 * Nx, s);
-    }
-    DevBuf<double> A1;
-    if (!fused) A1.alloc(Nx2 * M, s);
-    for (i64 i = 0; !fused && i < Nx; ++i) {
-        const i64 rows = (i + 1) * Nx;  // (j k) with j <= i
-        if (slab32)
-            k_fill_slab_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p,
-                                                                  (uint32_t)(rows * Nx), S.p);
-        else if (kt.ok)
-            k_fill_eri_rows_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(D, kt.t.p, G.L, i * N, i + 1, S.p);
-        else
-            k_fill_eri_rows<<<grid_for(rows * Nx), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, i + 1, S.p);
-        GLI_CHECK_LAUNCH();
-        // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
-        dgemm((int)rows, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false, s);
-        // W[i][j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j <= i)
-        dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, W.p + i * Nx * MM, MM, M, 1,
-              (int)(i + 1), false, s);
-    }
-    if (!fused) {
+        // slab by slab: S = V[i j k l] for j <= i filled, then contracted
+        DevBuf<double> A1(Nx2 * M, s), S(Nx2 * Nx, s);
+        for (i64 i = 0; i < Nx; ++i) {
+            const i64 rows = (i + 1) * Nx;  // (j k) with j <= i
+            if (slab32)
+                k_fill_slab_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(pt.p, (uint32_t)Nx, (int)G.L, hpt[i], kt.t.p,
+                                                                      (uint32_t)(rows * Nx), S.p);
+            else if (kt.ok)
+                k_fill_eri_rows_keyed<<<grid_for(rows * Nx), 256, 0, s>>>(D, kt.t.p, G.L, i * N, i + 1, S.p);
+            else
+                k_fill_eri_rows<<<grid_for(rows * Nx), 256, 0, s>>>(G, D, d_idx, d_val, m, i * N, i + 1, S.p);
+            GLI_CHECK_LAUNCH();
+            // A1[(j k)][s] = sum_l S[(j k)][l] B[l][s]
+            dgemm((int)rows, (int)M, (int)Nx, MatView{S.p, 0, Nx, 1}, MatView{bx, 0, M, 1}, A1.p, 0, M, 1, 1, false,
+                  s);
+            // W[i][j][r][s] = sum_k B[k][r] A1[j][k][s]   (batch j <= i)
+            dgemm((int)M, (int)M, (int)Nx, MatView{bx, 0, 1, M}, MatView{A1.p, Nx * M, M, 1}, W.p + i * Nx * MM, MM,
+                  M, 1, (int)(i + 1), false, s);
+        }
         k_mirror_pairs<<<grid_for(Nx2 * MM), 256, 0, s>>>(W.p, Nx, MM);
         GLI_CHECK_LAUNCH();
     }
