@@ -117,6 +117,24 @@ def dist_env():
     return ws, rank, local
 
 
+def host_threads():
+    """Host cores this process may run on (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def use_all_host_threads():
+    """Makes the reference core's OpenMP runtime use every host core this
+    process may run on, whatever OMP_NUM_THREADS the launcher set (torchrun
+    sets 1 per rank; the reference arm runs on rank 0 alone).  Call before
+    the reference library is loaded; returns the thread count."""
+    n = host_threads()
+    os.environ["OMP_NUM_THREADS"] = str(n)
+    return n
+
+
 class Clocks:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -183,8 +201,9 @@ def cpu_reference_rate(b, spec, idx, tol, min_seconds=8.0):
 def cpu_baseline_subprocess(gpu_values_path, workload):
     """Times the reference core in a fresh process (no torch, so its OpenMP
     runtime is the only one loaded); compares its values with the GPU's."""
+    env = dict(os.environ, OMP_NUM_THREADS=str(host_threads()))
     r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-baseline-json", gpu_values_path,
-                        "--workload", workload], capture_output=True, text=True, timeout=600)
+                        "--workload", workload], capture_output=True, text=True, timeout=600, env=env)
     if r.returncode != 0:
         raise RuntimeError(f"CPU baseline process failed: {r.stderr.strip()[-300:]}")
     return json.loads(r.stdout.strip().splitlines()[-1])
@@ -201,7 +220,8 @@ def cpu_baseline_main(gpu_values_path):
     pos = np.searchsorted(idx, sidx)
     errs = {f"max_abs_err_ha_gpu_{k}_vs_reference": float(np.max(np.abs(vals - gpu[k][pos])) / SPACING)
             for k in ("fp64", "mixed") if gpu[k].shape == idx.shape}
-    print(json.dumps({"value": rate, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
+    print(json.dumps({"value": rate, "unit": "classes/s", "cores": int(os.environ.get("OMP_NUM_THREADS", "0")) or
+                      host_threads(), "kind": "reference",
                       "sample": sample, **errs}))
     return 0
 
@@ -210,8 +230,7 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    cores = os.cpu_count()
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    cores = use_all_host_threads()
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     from ref_binding import RefLib
     r = RefLib()
@@ -474,7 +493,7 @@ def run_ours(args):
             cpu = cpu_baseline_subprocess(tmp, args.workload)
             os.unlink(tmp)
         except Exception as ex:  # the reference core must be prebuilt (make -C oracle ref)
-            cpu = {"value": None, "unit": "classes/s", "cores": os.cpu_count(), "kind": "reference",
+            cpu = {"value": None, "unit": "classes/s", "cores": host_threads(), "kind": "reference",
                    "sample": f"unavailable: {ex}"}
     st = stage[chosen]
     # the dominant kernel: stage A, stage B, or one of stage C's two kernels
